@@ -1,0 +1,305 @@
+#!/usr/bin/env python
+"""Benchmark of the Mittet fictitious-wave FDTD forward solve on B200.
+
+One bench "step" is one shot-solve of the workload: the full time loop
+(Nt leapfrog steps of the (2,4) Yee + CPML stencil with source injection and
+receiver sampling) plus the f_to_d transform (receiver spectra and, for the
+default workload, the full-volume f_to_d of Ex/Ey/Ez at 4 frequencies).
+
+Default workload (N=1): 256x256x192 cells, dx 25 m, 16-cell CPML, seeded
+log-normal model + resistive body, one Ex dipole, Nt 6000, 256 receivers,
+FP32 fields with FP64 DFT accumulators.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  `value` is whole-job Gcell/s with inputs
+resident in HBM; `e2e` is the same metric through the C ABI with host
+buffers (H2D of the model and D2H of every spectrum inside the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        import tempfile
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if "Active" in r[5 + q] and "Not" not in r[5 + q]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def stencil_bytes(wl, esz):
+    """Algorithmic bytes of one E-phase launch (the dominant kernel):
+    read Ex Ey Ez Hx Hy Hz and the model word, write Ex Ey Ez (10 words per cell),
+    + the FP32 ring write of Ex Ey Ez when the full-volume DFT is on,
+    + 2 psi read + 2 psi write per cell of each E slab group."""
+    cp = wl.cp
+    n = cp.nx * cp.ny * cp.nz
+    b = 10 * esz * n
+    if wl.volume_dft:
+        b += len(wl.volume_dft) * esz * n
+    nc = cp.ncpml
+    # E slab widths of the ncver0027 ranges: (ncpml-1) cells each side
+    w = [2 * (nc - 1)] * 3
+    slab_cells = w[0] * cp.ny * cp.nz + w[1] * cp.nx * cp.nz + w[2] * cp.nx * cp.ny
+    b += 4 * esz * slab_cells
+    return b * len(wl.shots)
+
+
+def run_cpu_baseline(wl, budget_s=20.0):
+    """Oracle (FP64 CPU restatement, all host threads) on a bounded sample of the
+    workload: a few time steps of the same grid.  Returns (Gcell/s, sample text, threads)."""
+    from oracle import oracle as O
+    cp = wl.cp
+    p = O.Params(nx=cp.nx, ny=cp.ny, nz=cp.nz, dx=cp.dx, dy=cp.dy, dz=cp.dz, dt=cp.dt, ncpml=cp.ncpml,
+                 cmax=cp.cmax, omega0=cp.omega0)
+    mu = np.full(wl.sigma.shape, cp.mu0)
+    src = wl.shots[0].points
+    sec = O.time_oracle_steps(p, wl.sigma, mu, src, wl.wavelet, 1, 4)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    g = cp.nx * cp.ny * cp.nz / sec / 1e9
+    return g, f"oracle FP64, {cp.nx}x{cp.ny}x{cp.nz} grid, 3 time steps (difference of 1- and 4-step runs)", threads
+
+
+def run_reference(args, wl):
+    """--impl reference: the reference's own satan_i C kernels (oracle/_ref) on
+    the host cores, same grid, W+K segments of a few time steps each."""
+    from oracle import oracle as O
+    cp = wl.cp
+    threads = os.cpu_count() or 1
+    seg = args.ref_seg_steps
+    cx, cy, cz = wl.shots[0].points[0][:3]
+    times = O.time_satan_reference(cp.nx, cp.ny, cp.nz, cp.dx, cp.dy, cp.dz, cp.ncpml, cp.omega0, wl.sigma,
+                                   seg, args.warmup + args.steps, (cx, cy, cz), 0, threads)
+    timed = times[args.warmup:]
+    t = float(np.sum(timed))
+    ncell = cp.nx * cp.ny * cp.nz
+    value = ncell * seg * args.steps / t / 1e9
+    sample = (f"satan_i e/h_field_cpml42 + e/hpml_abcs4 (gcc -O2 -fopenmp, {threads} threads), "
+              f"{cp.nx}x{cp.ny}x{cp.nz} grid, {seg} time steps per bench step")
+    return {
+        "metric": "Gcell/s", "value": value, "unit": "Gcell/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl.name, "nt_sample": seg, "note": "CPU reference, bounded sample"},
+        "shot_solves_per_s": value * 1e9 / (ncell * wl.nt),
+        "cpu_baseline": {"value": value, "unit": "Gcell/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain_gpu", choices=["plain_gpu", "batched", "plain_cpu"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--nt", type=int, default=0, help="override Nt (0 = workload default)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-seg-steps", type=int, default=4)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from mittet_main_b200 import workloads as W
+    from mittet_main_b200.capi import FP32, FP64
+    prec = FP64 if args.precision == "fp64" else FP32
+    mk = {"plain_gpu": W.plain_gpu, "batched": W.batched, "plain_cpu": W.plain_cpu}[args.workload]
+    kw = {"precision": prec}
+    if args.nt:
+        kw["nt"] = args.nt
+    wl = mk(**kw)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, wl)), flush=True)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    from dataclasses import replace
+    wl = replace(wl, cp=replace(wl.cp, device=dev))
+    # weak scaling: each rank solves its own shot(s) of the same model
+    solver = W.make_solver(wl)
+    nf = len(wl.omega)
+    nrec = len(wl.receivers)
+    out = torch.zeros((len(wl.shots), nrec, nf, 2), dtype=torch.float64, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        solver.forward_device(wl.nt, out, stream)
+    torch.cuda.synchronize()
+    launches0 = solver.launch_count()
+
+    sampler = ClockSampler(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        solver.forward_device(wl.nt, out, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    t_ms = e0.elapsed_time(e1)
+    t = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    cells = wl.cell_updates()
+    total_cells = cells * args.steps * world
+    value = total_cells / (t_ms / 1e3) / 1e9
+    gpu_launches = launches0 * args.steps
+
+    # per-kernel device times (CUDA events on the launching stream) for the roofline
+    kt = solver.time_kernels(min(64, wl.nt))
+    esz = 8 if prec == FP64 else 4
+    ebytes = stencil_bytes(wl, esz)
+    e_ms = kt["e_phase"]
+    achieved = ebytes / (e_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+
+    # end to end through the public C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        import ctypes
+        sig_host = np.ascontiguousarray(wl.sigma, dtype=np.float64)
+        h2d = sig_host.nbytes
+        d2h = len(wl.shots) * nrec * nf * 16
+        if wl.volume_dft:
+            d2h += len(wl.shots) * len(wl.volume_dft) * nf * wl.ncell * 16
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            solver.set_model(sig_host)
+            spec, _ = solver.forward(wl.nt)
+            if wl.volume_dft:
+                for s in range(len(wl.shots)):
+                    for c in wl.volume_dft:
+                        solver.volume_dft(s, "e" + c)
+        torch.cuda.synchronize()
+        te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=f"cuda:{dev}")
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te = float(te.item())
+        e2e = {"value": total_cells / te / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            g, sample, thr = run_cpu_baseline(wl)
+            cpu = {"value": g, "unit": "Gcell/s", "cores": thr, "kind": "port", "sample": sample}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Gcell/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": "Gcell/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == FP32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "nx": wl.cp.nx, "ny": wl.cp.ny, "nz": wl.cp.nz, "nt": wl.nt,
+                       "shots_per_gpu": len(wl.shots), "receivers": nrec, "freqs": nf,
+                       "volume_dft": wl.volume_dft or None, "fields": args.precision,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (fields > 126 MB)"},
+            "shot_solves_per_s": len(wl.shots) * args.steps * world / (t_ms / 1e3),
+            "gpu_launches": gpu_launches,
+            "kernel_ms": kt,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "e_phase_kernel",
+                         "alg_bytes_per_launch": ebytes, "peak_source": peak_kind},
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

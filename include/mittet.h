@@ -1,0 +1,209 @@
+/*
+ * mittet.h -- C ABI of the B200 Mittet fictitious-wave FDTD solver.
+ *
+ * One call of mittet_forward() replaces the reference's whole per-shot time
+ * loop and its f_to_d transform:
+ *
+ *   ncver0027/cpu_main.f90:99-143   do istep: read_source_3d, e_field_cpml4,
+ *                                    CPML_E4, h_field_cpml4, CPML_H4, output_EH_J
+ *   ncver0027/cpu_main.f90:182-185  f_to_d_e, f_to_d_h
+ *   satan_i/fwi3d_cpu_rec2rec_v1.4.c:48-59 (fwdpropagation loop + laplaceToFreq)
+ *
+ * and mittet_gradient() replaces the FWI gradient of
+ * satan_i/fwi3d_cpu_inv_fwi_v1.4.c:27-81 (residualE, sensitivity, conv_GdelE,
+ * calc_gamma), returning the gradient in the satan_i layout
+ * (double grad[nz][ny][nx], x fastest, zero in the CPML frame).
+ *
+ * Conventions
+ *   - Arrays are x fastest: index c = (k*ny + j)*nx + i with 0-based i,j,k;
+ *     this is Fortran sig(nx,ny,nz) column-major order and the satan_i
+ *     ijk = k*ix*iy + j*ix + i order.
+ *   - Source and receiver positions are 1-based (ix, iy, iz), exactly as the
+ *     Fortran driver and satan_i's model_env.dat give them.
+ *   - Complex outputs are interleaved (re, im) doubles (C99 double _Complex
+ *     layout, Fortran complex(kind(0d0))).
+ *   - Every call returns MITTET_OK (0) or a negative MITTET_ERR_* code;
+ *     mittet_last_error() gives the message of the calling thread's last error.
+ *   - The caller owns all host arrays; nothing is retained past a call.  A
+ *     handle owns its device memory (model, fields, accumulators), so the
+ *     model stays resident across calls.  A handle is not thread-safe; use one
+ *     handle per host thread.
+ */
+#ifndef MITTET_H
+#define MITTET_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define MITTET_OK 0
+#define MITTET_ERR_INVALID_ARG (-1)
+#define MITTET_ERR_CFL (-2)            /* dt above the (2,4) Taylor limit, cpu_set_condition.f90:279-286 */
+#define MITTET_ERR_OOM (-3)
+#define MITTET_ERR_DIVERGED (-4)       /* non-finite receiver samples */
+#define MITTET_ERR_DEVICE_TIMEOUT (-5) /* a bounded device wait gave up */
+#define MITTET_ERR_CUDA (-6)
+#define MITTET_ERR_STATE (-7)          /* call made before its inputs were set */
+
+/* ---- enums ---- */
+#define MITTET_FLAVOR_NCVER0027 0 /* Fortran ncver0027 ranges, profiles, c2 = -0.04167d0 */
+#define MITTET_FLAVOR_SATAN_I 1   /* C satan_i ranges, profiles (x * optToMax), c2 = -0.04167f */
+
+#define MITTET_FP32 0 /* FP32 fields, FP64 DFT accumulators */
+#define MITTET_FP64 1 /* FP64 everything */
+
+#define MITTET_EX 0
+#define MITTET_EY 1
+#define MITTET_EZ 2
+#define MITTET_HX 3
+#define MITTET_HY 4
+#define MITTET_HZ 5
+
+/* Magnetic source: F -= amp * s((n+1) dt) * dt / mu / (dx dy dz), added
+ * before the E half step (ncver0027/cpu_waveform.f90:46-50). */
+#define MITTET_SRC_MAGNETIC 0
+/* Electric source: F -= amp * (s(n dt) + s((n+1) dt))/2 * dt * 2 w0 / sigma / (dx dy dz),
+ * added after the E half step (satan_i/fwi3d_cpu_function_v1.4.c:526-527). */
+#define MITTET_SRC_ELECTRIC 1
+
+/* ---- configuration ---- */
+
+/* Grid: replaces the nx/ny/nz, dx/dy/dz and ncpml parameters of
+ * ncver0027/cpu_parameter_wafe.f90:25-28 (satan_i: model_env.dat fields 1-6, 14). */
+typedef struct {
+    int32_t nx, ny, nz;
+    double dx, dy, dz;
+    int32_t ncpml;
+} mittet_grid;
+
+/* Physics and scheme constants: replaces cpu_parameter_wafe.f90:30-40,117,123-132. */
+typedef struct {
+    double dt;        /* fictitious time step [s] */
+    double omega0;    /* 2 pi f0 [rad/s] */
+    double cmax;      /* fastest fictitious velocity sqrt(2 w0/(mu sigma_min)); sets the CPML sig_max */
+    double mu0;       /* permeability used where no mu volume is given */
+    double c1, c2;    /* (2,4) stencil weights (reference: 1.125, -0.04167) */
+    int32_t flavor;   /* MITTET_FLAVOR_* : index ranges and CPML profile formulae */
+    int32_t psi_hyx_typo; /* 1: psi_Hyx uses c1*Ez(i+1)-c2*Ez(i) as in cpu_cpml4.f90:400,413 */
+    int32_t e_sign, h_sign; /* +1; -1 gives the sign-flipped "bp" updates (cpu_eh_field_cpml42.f90:161-300) */
+    double cpml_nn, cpml_order, cpml_kappa_max, cpml_a_max, cpml_ma, cpml_rcoef, cpml_opt_to_max_x;
+    int32_t precision; /* MITTET_FP32 or MITTET_FP64 */
+    int32_t device;    /* CUDA device ordinal */
+    int32_t check_cfl; /* 1: reject dt above dx/cmax/sqrt(3)/1.16667 */
+} mittet_phys;
+
+/* One point source of one shot (a shot is one source position: the Fortran
+ * driver puts two Hz points in each shot, cpu_waveform.f90:46-50). */
+typedef struct {
+    int32_t shot;        /* 0-based shot index */
+    int32_t ix, iy, iz;  /* 1-based cell */
+    int32_t comp;        /* MITTET_EX .. MITTET_HZ */
+    int32_t kind;        /* MITTET_SRC_MAGNETIC or MITTET_SRC_ELECTRIC */
+    double amp;          /* multiplies the wavelet (1.0 in the reference) */
+} mittet_point_source;
+
+/* One receiver: point sample of one component after every step
+ * (ncver0027/cpu_output.f90:20-30; satan_i output() :772-777). */
+typedef struct {
+    int32_t ix, iy, iz; /* 1-based cell */
+    int32_t comp;       /* MITTET_EX .. MITTET_HZ */
+} mittet_receiver;
+
+typedef struct mittet_handle_s mittet_handle;
+
+/* Fill *phys with the reference constants of a flavour (dt, omega0 and cmax
+ * must still be set by the caller; dt can come from mittet_reference_dt). */
+int mittet_phys_defaults(int32_t flavor, mittet_phys *phys);
+
+/* dt by the reference rule of a flavour:
+ *   NCVER0027: 0.999 dx / cmax / sqrt(3) / 1.16667  (cpu_parameter_wafe.f90:117)
+ *   SATAN_I  : 1/cmax/sqrt(1/dx^2+1/dy^2+1/dz^2) * 6/7 * 0.999f (fwi3d_cpu_lattice_v1.4.c:38-39) */
+double mittet_reference_dt(int32_t flavor, const mittet_grid *grid, double cmax);
+
+/* Reference f_to_d frequency grid w_k = k * 2 pi / (nt dt), k = 0..nf-1
+ * (ncver0027/cpu_f_to_d_e.f90:134). */
+int mittet_freq_grid_ref(int32_t nt, double dt, int32_t nf, double *omega);
+
+/* Create a solver on phys->device.  Computes the CPML profiles
+ * (init_cpml, cpu_cpml4.f90:8-248 / cpmlabc.c:7-175) on the host. */
+int mittet_create(const mittet_grid *grid, const mittet_phys *phys, mittet_handle **out);
+void mittet_destroy(mittet_handle *h);
+
+/* Conductivity (and optionally permeability) volumes, nx*ny*nz doubles each,
+ * x fastest (Fortran sig/myu, cpu_parameter_wafe.f90:100-101).  mu may be NULL
+ * (phys->mu0 everywhere).  The model stays on the device until replaced. */
+int mittet_set_model(mittet_handle *h, const double *sigma, const double *mu);
+
+/* Shots and their point sources.  Shots share the model and receivers and
+ * run together in one batched launch per half step. */
+int mittet_set_sources(mittet_handle *h, int32_t nshot, int32_t npoint, const mittet_point_source *pts);
+
+/* Wavelet samples w[n] = s(n dt), n = 0..nt (nt+1 values). */
+int mittet_set_wavelet(mittet_handle *h, int32_t nt, const double *w);
+
+/* Receivers, the same for every shot. */
+int mittet_set_receivers(mittet_handle *h, int32_t nrec, const mittet_receiver *rec);
+
+/* Angular frequencies of the f_to_d transform.  h_factor = 1 multiplies the
+ * spectra of H receivers by sqrt(-2 w0/(i w)) (cpu_f_to_d_h.f90:146-148). */
+int mittet_set_freqs(mittet_handle *h, int32_t nf, const double *omega, int32_t h_factor);
+
+/* Full-volume f_to_d of the E components in comp_mask (bit c = MITTET_E*)
+ * at the handle's frequencies, accumulated on the fly (0 disables). */
+int mittet_set_volume_dft(mittet_handle *h, uint32_t comp_mask);
+
+/* Run nt steps for every shot.
+ *   rec_fd: [nshot][nrec][nf] complex (may be NULL)
+ *   rec_td: [nshot][nrec][nt] receiver traces (may be NULL)
+ * Trace sample n is taken after step n (t = (n+1) dt), as output_EH_J does. */
+int mittet_forward(mittet_handle *h, int32_t nt, double *rec_fd, double *rec_td);
+
+/* Full-volume spectra of the last forward: [nf][nz][ny][nx] complex. */
+int mittet_get_volume_dft(mittet_handle *h, int32_t shot, int32_t comp, double *out);
+
+/* Fields after the last forward: [6][nz][ny][nx] doubles (Ex Ey Ez Hx Hy Hz). */
+int mittet_get_fields(mittet_handle *h, int32_t shot, double *out);
+
+/* The reference's standalone f_to_d on host traces (cpu_f_to_d_e.f90:134-160,
+ * cpu_f_to_d_h.f90:141-167) evaluated on the GPU: x [ntrace][nt] real
+ * samples, out [ntrace][nf] complex.  h_factor as in mittet_set_freqs. */
+int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double omega0,
+                  const double *x, int32_t nf, const double *omega, int32_t h_factor, double *out);
+
+/* FWI gradient d(misfit)/d(sigma) for every shot of the handle.
+ *   obs: [nshot][nrec][nf] complex observed spectra (receivers and freqs of the handle)
+ *   misfit: 0.5 * sum |rec_fd - obs|^2 over shots, receivers, frequencies
+ *   grad: [nz][ny][nx] doubles, summed over shots, zero outside
+ *         [ncpml, n-ncpml) on every axis (satan_i calc_gamma,
+ *         fwi3d_cpu_function_v1.4.c:2351-2384).
+ * checkpoint_every: forward snapshots kept every that many steps (0 = 200). */
+int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t checkpoint_every,
+                    double *misfit, double *grad);
+
+/* Device-resident variants for callers that keep data on the GPU (the
+ * PyTorch front end).  Pointers are device pointers of the handle's device;
+ * stream is a cudaStream_t (NULL = the handle's stream). */
+int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu, int32_t is_fp64);
+int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *stream);
+
+/* Per-kernel timing (CUDA events on the handle's stream): restarts the last
+ * forward's shots from zero fields and runs nsteps steps (nsteps <= the last
+ * forward's nt) launching each kernel separately.  ms[0..5] receive the mean
+ * device time per launch of: magnetic inject, E phase, electric inject,
+ * H phase, sampling, volume-DFT flush (0 where a kernel did not run). */
+int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms);
+
+/* Number of kernels the last forward launched (for launch accounting). */
+int64_t mittet_last_launch_count(mittet_handle *h);
+
+/* Message of the calling thread's last error; returns its length. */
+int mittet_last_error(char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MITTET_H */

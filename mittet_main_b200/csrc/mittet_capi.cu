@@ -1,0 +1,954 @@
+// mittet_capi.cu -- the C ABI declared in include/mittet.h.
+//
+// A handle owns: the CPML profiles and ranges (host set-up), the resident
+// model (m = 2 w0 dt / sigma, optional dt/mu), the batched fields and compact
+// psi slabs of all shots, the receiver traces, and (optionally) the
+// full-volume DFT ring and accumulators.  mittet_forward() runs the time loop
+// as one CUDA graph of G steps replayed nt/G times, then the f_to_d
+// transform of the receiver traces.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mittet.h"
+#include "kernels.cuh"
+#include "setup_host.h"
+
+using namespace mittet;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) {                                                                     \
+            if (e_ == cudaErrorMemoryAllocation) {                                                   \
+                cudaGetLastError();                                                                  \
+                return fail(MITTET_ERR_OOM, "%s: %s", #call, cudaGetErrorString(e_));                \
+            }                                                                                        \
+            return fail(MITTET_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+        }                                                                                            \
+    } while (0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, b ? b : 16);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    template <typename T>
+    T *as() const { return (T *)p; }
+};
+
+DBox to_dbox(const Box &b) {
+    DBox d;
+    for (int a = 0; a < 3; a++) { d.lo[a] = b.lo[a]; d.hi[a] = b.hi[a]; }
+    return d;
+}
+DSlab to_dslab(const Slab &s) {
+    DSlab d;
+    d.nlo = s.nlo; d.nhi = s.nhi; d.flo = s.flo; d.fhi = s.fhi; d.width = s.width;
+    d.other = to_dbox(s.other);
+    return d;
+}
+
+}  // namespace
+
+struct mittet_handle_s {
+    mittet_grid g{};
+    mittet_phys ph{};
+    Setup su;
+    int px = 0;
+    long long plane = 0, fshot = 0;
+    bool fp64 = false;
+    size_t esz = 4;
+    cudaStream_t st = nullptr;
+
+    DevBuf prof, m, dtmu;
+    bool has_model = false, has_mu = false;
+    std::vector<double> sigma_h;  // host copy of the model (source scaling)
+    std::vector<double> mu_h;
+
+    int nshot = 0;
+    std::vector<mittet_point_source> pts;
+    DevBuf d_pts;
+    int npts = 0;
+    bool has_mag = false, has_ele = false;
+
+    int nt_wave = -1;
+    DevBuf wave;
+
+    int nrec = 0;
+    std::vector<mittet_receiver> recs;
+    DevBuf rec_off, rec_comp, rec_is_h;
+
+    std::vector<double> omega;
+    int hfac = 1;
+    DevBuf d_omega;
+
+    uint32_t vmask = 0;
+    int ring_k = 16;
+    DevBuf ring, acc, wtab;
+
+    DevBuf fields[6], psiE[3][2], psiH[3][2];
+    int alloc_shots = -1;
+    DevBuf traces, spectra, d_step, d_flag;
+    int last_nt = 0;
+    int64_t launches = 0;
+
+    // cached CUDA graph of G steps
+    cudaGraphExec_t gexec = nullptr;
+    int graph_steps = 0;
+    int graph_key_shots = -1;
+    long long graph_key = -1;
+};
+
+namespace {
+
+int set_device(mittet_handle *h) {
+    CK(cudaSetDevice(h->ph.device));
+    return MITTET_OK;
+}
+
+size_t psi_elems(const mittet_handle *h, const Slab &s, int axis) {
+    const size_t ny = h->g.ny, nz = h->g.nz, px = h->px;
+    if (axis == 0) return nz * ny * (size_t)s.width;
+    if (axis == 1) return nz * (size_t)s.width * px;
+    return (size_t)s.width * ny * px;
+}
+
+void drop_graph(mittet_handle *h) {
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+    h->graph_steps = 0;
+}
+
+int ensure_state(mittet_handle *h) {
+    const int ns = h->nshot;
+    if (h->alloc_shots != ns) {
+        drop_graph(h);
+        const size_t fbytes = (size_t)ns * h->fshot * h->esz;
+        for (int c = 0; c < 6; c++) CK(h->fields[c].ensure(fbytes));
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 2; w++) {
+                CK(h->psiE[a][w].ensure((size_t)ns * psi_elems(h, h->su.se[a], a) * h->esz));
+                CK(h->psiH[a][w].ensure((size_t)ns * psi_elems(h, h->su.sh[a], a) * h->esz));
+            }
+        h->alloc_shots = ns;
+    }
+    for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(h->fields[c].p, 0, (size_t)ns * h->fshot * h->esz, h->st));
+    for (int a = 0; a < 3; a++)
+        for (int w = 0; w < 2; w++) {
+            CK(cudaMemsetAsync(h->psiE[a][w].p, 0, (size_t)ns * psi_elems(h, h->su.se[a], a) * h->esz, h->st));
+            CK(cudaMemsetAsync(h->psiH[a][w].p, 0, (size_t)ns * psi_elems(h, h->su.sh[a], a) * h->esz, h->st));
+        }
+    return MITTET_OK;
+}
+
+template <typename T>
+PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
+    PhaseArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    for (int c = 0; c < 6; c++) a.f[c] = h->fields[c].as<T>();
+    for (int ax = 0; ax < 3; ax++)
+        for (int w = 0; w < 2; w++) a.psi[ax][w] = (e_phase ? h->psiE : h->psiH)[ax][w].as<T>();
+    a.m = h->m.as<T>();
+    a.dtmu = h->has_mu ? h->dtmu.as<T>() : nullptr;
+    a.dtmu0 = (T)(h->ph.dt / h->ph.mu0);
+    a.prof = h->prof.as<T>();
+    a.nmax = h->su.nmax;
+    a.nx = h->g.nx; a.ny = h->g.ny; a.nz = h->g.nz; a.px = h->px;
+    a.plane = h->plane; a.fshot = h->fshot;
+    for (int ax = 0; ax < 3; ax++) {
+        const Slab &s = e_phase ? h->su.se[ax] : h->su.sh[ax];
+        a.pshot[ax] = (long long)psi_elems(h, s, ax);
+        a.slab[ax] = to_dslab(s);
+        a.upd[ax] = to_dbox(h->su.upd[(e_phase ? 0 : 3) + ax]);
+    }
+    a.c1 = (T)h->ph.c1;
+    a.c2 = (T)h->ph.c2;
+    a.c2t = (T)(h->ph.psi_hyx_typo ? h->ph.c2 : h->ph.c1);
+    a.sgn = (T)(e_phase ? h->ph.e_sign : h->ph.h_sign);
+    a.zchunk = 16;
+    a.d_step = h->d_step.as<int>();
+    if (e_phase && h->vmask) {
+        a.ring = h->ring.as<T>();
+        a.ring_k = h->ring_k;
+        a.vmask = (int)h->vmask;
+        a.ring_comp = (long long)h->nshot * h->fshot;
+    }
+    return a;
+}
+
+constexpr int BX = 32, BY = 8;
+
+template <typename T>
+void launch_step(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha, const InjectArgs<T> &ia_m,
+                 const InjectArgs<T> &ia_e, const SampleArgs<T> &sa) {
+    const int nzc = (h->g.nz + ea.zchunk - 1) / ea.zchunk;
+    dim3 grid((h->g.nx + BX - 1) / BX, (h->g.ny + BY - 1) / BY, h->nshot * nzc);
+    dim3 block(BX, BY);
+    if (h->has_mag) { inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m); h->launches++; }
+    e_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ea);
+    h->launches++;
+    if (h->has_ele) { inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e); h->launches++; }
+    h_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ha);
+    h->launches++;
+    sample_kernel<T><<<1, 1024, 0, h->st>>>(sa);
+    h->launches++;
+}
+
+template <typename T>
+void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
+    const long long tot = (long long)h->nshot * h->fshot;
+    int blocks = (int)std::min<long long>((tot + 255) / 256, 148LL * 16);
+    volume_dft_kernel<T><<<blocks, 256, 0, h->st>>>(h->ring.as<T>(), tot, (int)h->vmask, h->nshot, h->fshot, cnt, n0,
+                                                    h->wtab.as<double2>(), (int)h->omega.size(),
+                                                    h->acc.as<double2>());
+    h->launches++;
+}
+
+template <typename T>
+int run_forward(mittet_handle *h, int nt) {
+    const int ns = h->nshot;
+    int rc = ensure_state(h);
+    if (rc) return rc;
+    CK(h->d_step.ensure(sizeof(int)));
+    CK(h->d_flag.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(h->d_step.p, 0, sizeof(int), h->st));
+    CK(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->st));
+    const size_t ntr = (size_t)ns * std::max(h->nrec, 1) * nt;
+    CK(h->traces.ensure(ntr * h->esz));
+    const int nf = (int)h->omega.size();
+    const bool vol = h->vmask && nf > 0;
+    if (vol) {
+        const size_t ring_b = (size_t)h->ring_k * 3 * ns * h->fshot * h->esz;
+        CK(h->ring.ensure(ring_b));
+        const size_t acc_b = (size_t)ns * 3 * nf * h->fshot * sizeof(double2);
+        CK(h->acc.ensure(acc_b));
+        CK(cudaMemsetAsync(h->acc.p, 0, acc_b, h->st));
+        // weights wt[n][f] = dt exp((i-1) sqrt(w0 w) n dt)
+        std::vector<double> wt((size_t)nt * nf * 2);
+        for (int n = 0; n < nt; n++)
+            for (int f = 0; f < nf; f++) {
+                const double xa = std::sqrt(h->ph.omega0 * h->omega[f]) * (double)n * h->ph.dt;
+                const double e = std::exp(-xa) * h->ph.dt;
+                wt[((size_t)n * nf + f) * 2] = e * std::cos(xa);
+                wt[((size_t)n * nf + f) * 2 + 1] = e * std::sin(xa);
+            }
+        CK(h->wtab.ensure(wt.size() * sizeof(double)));
+        CK(cudaMemcpyAsync(h->wtab.p, wt.data(), wt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    }
+
+    PhaseArgs<T> ea = phase_args<T>(h, true);
+    PhaseArgs<T> ha = phase_args<T>(h, false);
+    if (!vol) ea.ring_k = 0;
+    InjectArgs<T> ia;
+    memset(&ia, 0, sizeof(ia));
+    for (int c = 0; c < 6; c++) ia.f[c] = h->fields[c].as<T>();
+    ia.pts = h->d_pts.as<SrcPoint>();
+    ia.npts = h->npts;
+    ia.wave = h->wave.as<double>();
+    ia.d_step = h->d_step.as<int>();
+    if (vol) {
+        ia.ring = h->ring.as<T>();
+        ia.ring_k = h->ring_k;
+        ia.vmask = (int)h->vmask;
+        ia.ring_comp = (long long)ns * h->fshot;
+    }
+    InjectArgs<T> ia_m = ia, ia_e = ia;
+    ia_m.kind = 0;
+    ia_e.kind = 1;
+    SampleArgs<T> sa;
+    memset(&sa, 0, sizeof(sa));
+    for (int c = 0; c < 6; c++) sa.f[c] = h->fields[c].as<T>();
+    sa.rec_off = h->rec_off.as<long long>();
+    sa.rec_comp = h->rec_comp.as<int>();
+    sa.nrec = h->nrec;
+    sa.nshot = ns;
+    sa.fshot = h->fshot;
+    sa.traces = h->traces.as<T>();
+    sa.nt = nt;
+    sa.d_step = h->d_step.as<int>();
+
+    h->launches = 0;
+    // One graph holds G = ring_k steps (+ the volume flush when enabled).
+    const int G = h->ring_k;
+    const long long key = ((long long)nt << 20) ^ ((long long)ns << 4) ^ (vol ? 1 : 0) ^ ((long long)h->nrec << 40);
+    if (!h->gexec || h->graph_key != key) {
+        drop_graph(h);
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < G; s++) launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+        cudaError_t ec = cudaStreamEndCapture(h->st, &graph);
+        if (ec != cudaSuccess) return fail(MITTET_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
+        ec = cudaGraphInstantiate(&h->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ec != cudaSuccess) return fail(MITTET_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+        h->graph_key = key;
+        h->graph_steps = G;
+    }
+    h->launches = 0;
+    const long long per_step = (h->has_mag ? 1 : 0) + (h->has_ele ? 1 : 0) + 3;
+    int done = 0;
+    while (done + G <= nt) {
+        CK(cudaGraphLaunch(h->gexec, h->st));
+        h->launches += per_step * G;
+        if (vol) launch_volume_flush<T>(h, G, done);
+        done += G;
+    }
+    const int rem = nt - done;
+    for (int s = 0; s < rem; s++) {
+        launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+    }
+    if (rem > 0 && vol) launch_volume_flush<T>(h, rem, done);
+    CK(cudaGetLastError());
+
+    if (h->nrec > 0) {
+        finite_check_kernel<T><<<64, 256, 0, h->st>>>(h->traces.as<T>(), (long long)ns * h->nrec * nt,
+                                                      h->d_flag.as<int>());
+        h->launches++;
+        if (nf > 0) {
+            CK(h->spectra.ensure((size_t)ns * h->nrec * nf * sizeof(double2)));
+            trace_dft_kernel<T><<<nf, 256, 0, h->st>>>(h->traces.as<T>(), ns * h->nrec, nt, h->d_omega.as<double>(),
+                                                       nf, h->ph.dt, h->ph.omega0, h->rec_is_h.as<unsigned char>(),
+                                                       h->hfac, h->spectra.as<double2>());
+            h->launches++;
+        }
+    }
+    CK(cudaGetLastError());
+    h->last_nt = nt;
+    return MITTET_OK;
+}
+
+template <typename T>
+int time_kernels(mittet_handle *h, int nsteps, double *ms) {
+    int rc = ensure_state(h);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->d_step.p, 0, sizeof(int), h->st));
+    const int nt = h->last_nt;
+    const bool vol = h->vmask && !h->omega.empty();
+    PhaseArgs<T> ea = phase_args<T>(h, true);
+    PhaseArgs<T> ha = phase_args<T>(h, false);
+    if (!vol) ea.ring_k = 0;
+    InjectArgs<T> ia;
+    memset(&ia, 0, sizeof(ia));
+    for (int c = 0; c < 6; c++) ia.f[c] = h->fields[c].as<T>();
+    ia.pts = h->d_pts.as<SrcPoint>();
+    ia.npts = h->npts;
+    ia.wave = h->wave.as<double>();
+    ia.d_step = h->d_step.as<int>();
+    if (vol) {
+        ia.ring = h->ring.as<T>();
+        ia.ring_k = h->ring_k;
+        ia.vmask = (int)h->vmask;
+        ia.ring_comp = (long long)h->nshot * h->fshot;
+    }
+    InjectArgs<T> ia_m = ia, ia_e = ia;
+    ia_m.kind = 0;
+    ia_e.kind = 1;
+    SampleArgs<T> sa;
+    memset(&sa, 0, sizeof(sa));
+    for (int c = 0; c < 6; c++) sa.f[c] = h->fields[c].as<T>();
+    sa.rec_off = h->rec_off.as<long long>();
+    sa.rec_comp = h->rec_comp.as<int>();
+    sa.nrec = h->nrec;
+    sa.nshot = h->nshot;
+    sa.fshot = h->fshot;
+    sa.traces = h->traces.as<T>();
+    sa.nt = nt;
+    sa.d_step = h->d_step.as<int>();
+    const int nzc = (h->g.nz + ea.zchunk - 1) / ea.zchunk;
+    dim3 grid((h->g.nx + BX - 1) / BX, (h->g.ny + BY - 1) / BY, h->nshot * nzc);
+    dim3 block(BX, BY);
+    cudaEvent_t ev[12];
+    for (int q = 0; q < 12; q++) CK(cudaEventCreate(&ev[q]));
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    int cnt[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < nsteps; s++) {
+        CK(cudaEventRecord(ev[0], h->st));
+        if (h->has_mag) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m);
+        CK(cudaEventRecord(ev[1], h->st));
+        e_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ea);
+        CK(cudaEventRecord(ev[2], h->st));
+        if (h->has_ele) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e);
+        CK(cudaEventRecord(ev[3], h->st));
+        h_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ha);
+        CK(cudaEventRecord(ev[4], h->st));
+        sample_kernel<T><<<1, 1024, 0, h->st>>>(sa);  // also advances the step counter
+        CK(cudaEventRecord(ev[5], h->st));
+        const bool flush = vol && ((s + 1) % h->ring_k == 0);
+        if (flush) launch_volume_flush<T>(h, h->ring_k, s + 1 - h->ring_k);
+        CK(cudaEventRecord(ev[6], h->st));
+        CK(cudaGetLastError());
+        CK(cudaEventSynchronize(ev[6]));
+        float t;
+        const bool ran[6] = {h->has_mag, true, h->has_ele, true, true, flush};
+        for (int q = 0; q < 6; q++) {
+            if (!ran[q]) continue;
+            CK(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+            acc[q] += t;
+            cnt[q]++;
+        }
+    }
+    for (int q = 0; q < 12; q++) cudaEventDestroy(ev[q]);
+    for (int q = 0; q < 6; q++) ms[q] = cnt[q] ? acc[q] / cnt[q] : 0.0;
+    return MITTET_OK;
+}
+
+int validate_ready(mittet_handle *h, int nt) {
+    if (!h->has_model) return fail(MITTET_ERR_STATE, "mittet_set_model has not been called");
+    if (h->nshot <= 0) return fail(MITTET_ERR_STATE, "mittet_set_sources has not been called");
+    if (h->nt_wave < nt) return fail(MITTET_ERR_STATE, "wavelet has %d steps, forward asked for %d", h->nt_wave, nt);
+    if (nt <= 0) return fail(MITTET_ERR_INVALID_ARG, "nt must be positive");
+    return MITTET_OK;
+}
+
+// Upload the point sources with their per-point gain (depends on the model).
+int upload_sources(mittet_handle *h) {
+    if (!h->has_model || h->pts.empty()) return MITTET_OK;
+    std::vector<SrcPoint> dp(h->pts.size());
+    const double vol = h->g.dx * h->g.dy * h->g.dz;
+    h->has_mag = h->has_ele = false;
+    for (size_t q = 0; q < h->pts.size(); q++) {
+        const mittet_point_source &p = h->pts[q];
+        const long long cell = ((long long)(p.iz - 1) * h->g.ny + (p.iy - 1)) * h->px + (p.ix - 1);
+        const size_t c0 = ((size_t)(p.iz - 1) * h->g.ny + (p.iy - 1)) * h->g.nx + (p.ix - 1);
+        dp[q].off = (long long)p.shot * h->fshot + cell;
+        dp[q].comp = p.comp;
+        dp[q].kind = p.kind;
+        if (p.kind == MITTET_SRC_MAGNETIC) {
+            const double mu = h->mu_h.empty() ? h->ph.mu0 : h->mu_h[c0];
+            dp[q].g = p.amp * h->ph.dt / mu / vol;
+            h->has_mag = true;
+        } else {
+            dp[q].g = p.amp * h->ph.dt * 2.0 * h->ph.omega0 / h->sigma_h[c0] / vol;
+            h->has_ele = true;
+        }
+    }
+    CK(h->d_pts.ensure(dp.size() * sizeof(SrcPoint)));
+    CK(cudaMemcpyAsync(h->d_pts.p, dp.data(), dp.size() * sizeof(SrcPoint), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->npts = (int)dp.size();
+    drop_graph(h);
+    return MITTET_OK;
+}
+
+template <typename T>
+__global__ void model_kernel(const double *__restrict__ sig, const double *__restrict__ mu, int nx, int ny, int nz,
+                             int px, double two_w0_dt, double dt, T *__restrict__ m, T *__restrict__ dtmu) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % nx);
+        const long long r = e / nx;
+        const long long o = r * px + i;
+        m[o] = (T)(two_w0_dt / sig[e]);
+        if (mu) dtmu[o] = (T)(dt / mu[e]);
+    }
+}
+
+template <typename T>
+__global__ void model_kernel_dev(const T *__restrict__ sig, const T *__restrict__ mu, int nx, int ny, int nz, int px,
+                                 double two_w0_dt, double dt, T *__restrict__ m, T *__restrict__ dtmu) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % nx);
+        const long long r = e / nx;
+        const long long o = r * px + i;
+        m[o] = (T)(two_w0_dt / (double)sig[e]);
+        if (mu) dtmu[o] = (T)(dt / (double)mu[e]);
+    }
+}
+
+}  // namespace
+
+// ======================================================================= API
+
+extern "C" {
+
+int mittet_last_error(char *buf, size_t len) {
+    if (buf && len) {
+        strncpy(buf, g_err.c_str(), len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)g_err.size();
+}
+
+int mittet_phys_defaults(int32_t flavor, mittet_phys *p) {
+    if (!p) return fail(MITTET_ERR_INVALID_ARG, "null phys");
+    memset(p, 0, sizeof(*p));
+    p->flavor = flavor;
+    p->c1 = 1.125;
+    p->e_sign = 1;
+    p->h_sign = 1;
+    p->precision = MITTET_FP32;
+    p->check_cfl = 1;
+    if (flavor == MITTET_FLAVOR_NCVER0027) {
+        // ncver0027/cpu_parameter_wafe.f90:30-32,40,84,123-132
+        p->c2 = -0.04167;
+        p->omega0 = 2.0 * 3.14159265358979 * 1.0;
+        p->mu0 = 1.2566370614e-6;
+        p->psi_hyx_typo = 1;
+        p->cpml_nn = 3.0; p->cpml_order = 0.0; p->cpml_kappa_max = 1.0; p->cpml_a_max = 0.2;
+        p->cpml_ma = 1.0; p->cpml_rcoef = 0.01; p->cpml_opt_to_max_x = 1.0;
+    } else if (flavor == MITTET_FLAVOR_SATAN_I) {
+        // satan_i/fwi3d_cpu_function_v1.4.c:1187, fwi3d_cpu_alloli1_v1.4.h:3, cpmlabc.c:12-23
+        p->c2 = (double)-0.04167f;
+        p->omega0 = 2.0 * M_PI;
+        p->mu0 = 12.5663706e-7;
+        p->psi_hyx_typo = 0;
+        p->cpml_nn = 3.0; p->cpml_order = 0.0; p->cpml_kappa_max = 1.0; p->cpml_a_max = (double)0.2f;
+        p->cpml_ma = 1.0; p->cpml_rcoef = (double)0.01f; p->cpml_opt_to_max_x = 10.0;
+    } else {
+        return fail(MITTET_ERR_INVALID_ARG, "unknown flavor %d", flavor);
+    }
+    return MITTET_OK;
+}
+
+double mittet_reference_dt(int32_t flavor, const mittet_grid *g, double cmax) {
+    if (!g || cmax <= 0) return 0.0;
+    if (flavor == MITTET_FLAVOR_SATAN_I) {
+        const double courant = 1.0 / cmax / std::sqrt(1.0 / (g->dx * g->dx) + 1.0 / (g->dy * g->dy) + 1.0 / (g->dz * g->dz));
+        return courant * 6.0 / 7.0 * (double)0.999f;
+    }
+    return 0.999 * g->dx / cmax / std::sqrt(3.0) / 1.16667;
+}
+
+int mittet_freq_grid_ref(int32_t nt, double dt, int32_t nf, double *omega) {
+    if (nt <= 0 || dt <= 0 || nf < 0 || (!omega && nf)) return fail(MITTET_ERR_INVALID_ARG, "bad freq grid args");
+    const double om = 2.0 * 3.14159265358979 / (double)nt / dt;
+    for (int k = 0; k < nf; k++) omega[k] = om * k;
+    return MITTET_OK;
+}
+
+int mittet_create(const mittet_grid *g, const mittet_phys *ph, mittet_handle **out) {
+    if (!g || !ph || !out) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (g->nx < 8 || g->ny < 8 || g->nz < 8) return fail(MITTET_ERR_INVALID_ARG, "grid must be at least 8 cells per axis");
+    if (g->ncpml < 2 || 2 * g->ncpml + 4 > std::min(g->nx, std::min(g->ny, g->nz)))
+        return fail(MITTET_ERR_INVALID_ARG, "ncpml %d does not fit the grid", g->ncpml);
+    if (!(g->dx > 0 && g->dy > 0 && g->dz > 0)) return fail(MITTET_ERR_INVALID_ARG, "cell sizes must be positive");
+    if (!(ph->dt > 0 && ph->omega0 > 0 && ph->cmax > 0 && ph->mu0 > 0))
+        return fail(MITTET_ERR_INVALID_ARG, "dt, omega0, cmax and mu0 must be positive");
+    if (ph->flavor != MITTET_FLAVOR_NCVER0027 && ph->flavor != MITTET_FLAVOR_SATAN_I)
+        return fail(MITTET_ERR_INVALID_ARG, "unknown flavor %d", ph->flavor);
+    if (ph->precision != MITTET_FP32 && ph->precision != MITTET_FP64)
+        return fail(MITTET_ERR_INVALID_ARG, "precision must be MITTET_FP32 or MITTET_FP64");
+    if (ph->check_cfl) {
+        // Taylor (2,4) limit, ncver0027/cpu_set_condition.f90:279,285
+        const double dmin = std::min(g->dx, std::min(g->dy, g->dz));
+        const double taylor_dt = dmin / ph->cmax / std::sqrt(3.0) / 1.16667;
+        if (ph->dt > taylor_dt * (1.0 + 1e-12))
+            return fail(MITTET_ERR_CFL, "dt %.6e exceeds the (2,4) Taylor limit %.6e", ph->dt, taylor_dt);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(MITTET_ERR_CUDA, "no CUDA device available");
+    }
+    if (ph->device < 0 || ph->device >= ndev) return fail(MITTET_ERR_INVALID_ARG, "device %d out of range", ph->device);
+
+    mittet_handle *h = new mittet_handle();
+    h->g = *g;
+    h->ph = *ph;
+    h->fp64 = ph->precision == MITTET_FP64;
+    h->esz = h->fp64 ? 8 : 4;
+    h->px = (g->nx + 31) / 32 * 32;
+    h->plane = (long long)h->px * g->ny;
+    h->fshot = h->plane * g->nz;
+    CpmlConst cc{ph->cpml_nn, ph->cpml_order, ph->cpml_kappa_max, ph->cpml_a_max, ph->cpml_ma, ph->cpml_rcoef,
+                 ph->cpml_opt_to_max_x};
+    build_setup(ph->flavor, g->nx, g->ny, g->nz, g->dx, g->dy, g->dz, g->ncpml, ph->cmax, ph->dt, cc, h->su);
+    if (!ranges_in_bounds(h->su)) {
+        delete h;
+        return fail(MITTET_ERR_INVALID_ARG, "grid too small for the flavour's index ranges");
+    }
+    int rc = set_device(h);
+    if (rc) { delete h; return rc; }
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return fail(MITTET_ERR_CUDA, "stream creation failed");
+    }
+    // profiles in the field precision
+    const size_t np = h->su.prof.size();
+    cudaError_t e = h->prof.ensure(np * h->esz);
+    if (e == cudaSuccess) {
+        if (h->fp64) {
+            e = cudaMemcpy(h->prof.p, h->su.prof.data(), np * 8, cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> pf(np);
+            for (size_t q = 0; q < np; q++) pf[q] = (float)h->su.prof[q];
+            e = cudaMemcpy(h->prof.p, pf.data(), np * 4, cudaMemcpyHostToDevice);
+        }
+    }
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(h->st);
+        delete h;
+        return fail(e == cudaErrorMemoryAllocation ? MITTET_ERR_OOM : MITTET_ERR_CUDA, "profile upload: %s",
+                    cudaGetErrorString(e));
+    }
+    *out = h;
+    return MITTET_OK;
+}
+
+void mittet_destroy(mittet_handle *h) {
+    if (!h) return;
+    cudaSetDevice(h->ph.device);
+    drop_graph(h);
+    if (h->st) cudaStreamSynchronize(h->st);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+int mittet_set_model(mittet_handle *h, const double *sigma, const double *mu) {
+    if (!h || !sigma) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    for (size_t q = 0; q < n; q++)
+        if (!(sigma[q] > 0) || !std::isfinite(sigma[q]))
+            return fail(MITTET_ERR_INVALID_ARG, "sigma[%zu] = %g is not a positive finite conductivity", q, sigma[q]);
+    if (mu)
+        for (size_t q = 0; q < n; q++)
+            if (!(mu[q] > 0) || !std::isfinite(mu[q]))
+                return fail(MITTET_ERR_INVALID_ARG, "mu[%zu] = %g is not positive and finite", q, mu[q]);
+    h->sigma_h.assign(sigma, sigma + n);
+    if (mu) h->mu_h.assign(mu, mu + n); else h->mu_h.clear();
+    DevBuf ds, dm;
+    CK(ds.ensure(n * 8));
+    CK(cudaMemcpyAsync(ds.p, sigma, n * 8, cudaMemcpyHostToDevice, h->st));
+    if (mu) {
+        CK(dm.ensure(n * 8));
+        CK(cudaMemcpyAsync(dm.p, mu, n * 8, cudaMemcpyHostToDevice, h->st));
+    }
+    const size_t cb = (size_t)h->fshot * h->esz;
+    CK(h->m.ensure(cb));
+    CK(cudaMemsetAsync(h->m.p, 0, cb, h->st));
+    if (mu) {
+        CK(h->dtmu.ensure(cb));
+        CK(cudaMemsetAsync(h->dtmu.p, 0, cb, h->st));
+    }
+    const double k = 2.0 * h->ph.omega0 * h->ph.dt;
+    if (h->fp64)
+        model_kernel<double><<<1024, 256, 0, h->st>>>(ds.as<double>(), mu ? dm.as<double>() : nullptr, h->g.nx, h->g.ny,
+                                                      h->g.nz, h->px, k, h->ph.dt, h->m.as<double>(),
+                                                      mu ? h->dtmu.as<double>() : nullptr);
+    else
+        model_kernel<float><<<1024, 256, 0, h->st>>>(ds.as<double>(), mu ? dm.as<double>() : nullptr, h->g.nx, h->g.ny,
+                                                     h->g.nz, h->px, k, h->ph.dt, h->m.as<float>(),
+                                                     mu ? h->dtmu.as<float>() : nullptr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    h->has_model = true;
+    h->has_mu = mu != nullptr;
+    drop_graph(h);
+    return upload_sources(h);
+}
+
+int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu, int32_t is_fp64) {
+    if (!h || !sigma) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    // a host copy is kept for the electric source gains
+    h->sigma_h.resize(n);
+    if (is_fp64) {
+        CK(cudaMemcpy(h->sigma_h.data(), sigma, n * 8, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(n);
+        CK(cudaMemcpy(tmp.data(), sigma, n * 4, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < n; q++) h->sigma_h[q] = tmp[q];
+    }
+    for (size_t q = 0; q < n; q++)
+        if (!(h->sigma_h[q] > 0) || !std::isfinite(h->sigma_h[q]))
+            return fail(MITTET_ERR_INVALID_ARG, "sigma[%zu] is not a positive finite conductivity", q);
+    if (mu) {
+        h->mu_h.resize(n);
+        if (is_fp64) {
+            CK(cudaMemcpy(h->mu_h.data(), mu, n * 8, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> tmp(n);
+            CK(cudaMemcpy(tmp.data(), mu, n * 4, cudaMemcpyDeviceToHost));
+            for (size_t q = 0; q < n; q++) h->mu_h[q] = tmp[q];
+        }
+    } else {
+        h->mu_h.clear();
+    }
+    const size_t cb = (size_t)h->fshot * h->esz;
+    CK(h->m.ensure(cb));
+    CK(cudaMemsetAsync(h->m.p, 0, cb, h->st));
+    if (mu) {
+        CK(h->dtmu.ensure(cb));
+        CK(cudaMemsetAsync(h->dtmu.p, 0, cb, h->st));
+    }
+    const double k = 2.0 * h->ph.omega0 * h->ph.dt;
+    if (h->fp64 && is_fp64)
+        model_kernel_dev<double><<<1024, 256, 0, h->st>>>((const double *)sigma, (const double *)mu, h->g.nx, h->g.ny,
+                                                          h->g.nz, h->px, k, h->ph.dt, h->m.as<double>(),
+                                                          mu ? h->dtmu.as<double>() : nullptr);
+    else if (!h->fp64 && !is_fp64)
+        model_kernel_dev<float><<<1024, 256, 0, h->st>>>((const float *)sigma, (const float *)mu, h->g.nx, h->g.ny,
+                                                         h->g.nz, h->px, k, h->ph.dt, h->m.as<float>(),
+                                                         mu ? h->dtmu.as<float>() : nullptr);
+    else
+        return fail(MITTET_ERR_INVALID_ARG, "model dtype must match the handle precision");
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    h->has_model = true;
+    h->has_mu = mu != nullptr;
+    drop_graph(h);
+    return upload_sources(h);
+}
+
+int mittet_set_sources(mittet_handle *h, int32_t nshot, int32_t npoint, const mittet_point_source *pts) {
+    if (!h || nshot <= 0 || npoint <= 0 || !pts) return fail(MITTET_ERR_INVALID_ARG, "need at least one shot and point");
+    for (int q = 0; q < npoint; q++) {
+        const mittet_point_source &p = pts[q];
+        if (p.shot < 0 || p.shot >= nshot) return fail(MITTET_ERR_INVALID_ARG, "point %d: shot %d out of range", q, p.shot);
+        if (p.ix < 1 || p.ix > h->g.nx || p.iy < 1 || p.iy > h->g.ny || p.iz < 1 || p.iz > h->g.nz)
+            return fail(MITTET_ERR_INVALID_ARG, "point %d: position (%d,%d,%d) outside the grid", q, p.ix, p.iy, p.iz);
+        if (p.comp < 0 || p.comp > 5) return fail(MITTET_ERR_INVALID_ARG, "point %d: bad component", q);
+        if (p.kind != MITTET_SRC_MAGNETIC && p.kind != MITTET_SRC_ELECTRIC)
+            return fail(MITTET_ERR_INVALID_ARG, "point %d: bad kind", q);
+        if (!std::isfinite(p.amp)) return fail(MITTET_ERR_INVALID_ARG, "point %d: amplitude not finite", q);
+    }
+    int rc = set_device(h);
+    if (rc) return rc;
+    h->nshot = nshot;
+    h->pts.assign(pts, pts + npoint);
+    drop_graph(h);
+    return upload_sources(h);
+}
+
+int mittet_set_wavelet(mittet_handle *h, int32_t nt, const double *w) {
+    if (!h || nt <= 0 || !w) return fail(MITTET_ERR_INVALID_ARG, "bad wavelet");
+    for (int q = 0; q <= nt; q++)
+        if (!std::isfinite(w[q])) return fail(MITTET_ERR_INVALID_ARG, "wavelet sample %d not finite", q);
+    int rc = set_device(h);
+    if (rc) return rc;
+    CK(h->wave.ensure((size_t)(nt + 1) * 8));
+    CK(cudaMemcpy(h->wave.p, w, (size_t)(nt + 1) * 8, cudaMemcpyHostToDevice));
+    h->nt_wave = nt;
+    drop_graph(h);
+    return MITTET_OK;
+}
+
+int mittet_set_receivers(mittet_handle *h, int32_t nrec, const mittet_receiver *rec) {
+    if (!h || nrec < 0 || (nrec > 0 && !rec)) return fail(MITTET_ERR_INVALID_ARG, "bad receivers");
+    std::vector<long long> off(std::max(nrec, 1));
+    std::vector<int> comp(std::max(nrec, 1));
+    std::vector<unsigned char> ish(std::max(nrec, 1));
+    for (int r = 0; r < nrec; r++) {
+        const mittet_receiver &q = rec[r];
+        if (q.ix < 1 || q.ix > h->g.nx || q.iy < 1 || q.iy > h->g.ny || q.iz < 1 || q.iz > h->g.nz)
+            return fail(MITTET_ERR_INVALID_ARG, "receiver %d outside the grid", r);
+        if (q.comp < 0 || q.comp > 5) return fail(MITTET_ERR_INVALID_ARG, "receiver %d: bad component", r);
+        off[r] = ((long long)(q.iz - 1) * h->g.ny + (q.iy - 1)) * h->px + (q.ix - 1);
+        comp[r] = q.comp;
+        ish[r] = q.comp >= 3;
+    }
+    if (nrec * (long long)std::max(h->nshot, 1) > (1 << 24)) return fail(MITTET_ERR_INVALID_ARG, "too many receivers");
+    int rc = set_device(h);
+    if (rc) return rc;
+    CK(h->rec_off.ensure(off.size() * 8));
+    CK(h->rec_comp.ensure(comp.size() * 4));
+    CK(h->rec_is_h.ensure(ish.size()));
+    CK(cudaMemcpy(h->rec_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->rec_comp.p, comp.data(), comp.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->rec_is_h.p, ish.data(), ish.size(), cudaMemcpyHostToDevice));
+    h->nrec = nrec;
+    h->recs.assign(rec, rec + nrec);
+    drop_graph(h);
+    return MITTET_OK;
+}
+
+int mittet_set_freqs(mittet_handle *h, int32_t nf, const double *omega, int32_t h_factor) {
+    if (!h || nf < 0 || (nf > 0 && !omega)) return fail(MITTET_ERR_INVALID_ARG, "bad frequencies");
+    for (int f = 0; f < nf; f++)
+        if (!(omega[f] >= 0) || !std::isfinite(omega[f])) return fail(MITTET_ERR_INVALID_ARG, "omega[%d] invalid", f);
+    int rc = set_device(h);
+    if (rc) return rc;
+    h->omega.assign(omega, omega + nf);
+    h->hfac = h_factor ? 1 : 0;
+    CK(h->d_omega.ensure(std::max(nf, 1) * 8));
+    if (nf) CK(cudaMemcpy(h->d_omega.p, omega, nf * 8, cudaMemcpyHostToDevice));
+    drop_graph(h);
+    return MITTET_OK;
+}
+
+int mittet_set_volume_dft(mittet_handle *h, uint32_t comp_mask) {
+    if (!h || comp_mask > 7) return fail(MITTET_ERR_INVALID_ARG, "comp_mask must select Ex/Ey/Ez bits only");
+    if (comp_mask && h->omega.size() > 64) return fail(MITTET_ERR_INVALID_ARG, "volume DFT supports at most 64 frequencies");
+    h->vmask = comp_mask;
+    drop_graph(h);
+    return MITTET_OK;
+}
+
+int mittet_forward(mittet_handle *h, int32_t nt, double *rec_fd, double *rec_td) {
+    if (!h) return fail(MITTET_ERR_INVALID_ARG, "null handle");
+    int rc = validate_ready(h, nt);
+    if (rc) return rc;
+    if (h->vmask && h->omega.empty()) return fail(MITTET_ERR_STATE, "volume DFT needs mittet_set_freqs first");
+    rc = set_device(h);
+    if (rc) return rc;
+    rc = h->fp64 ? run_forward<double>(h, nt) : run_forward<float>(h, nt);
+    if (rc) return rc;
+    const int nf = (int)h->omega.size();
+    const size_t ntr = (size_t)h->nshot * h->nrec;
+    if (rec_fd && nf > 0 && ntr > 0)
+        CK(cudaMemcpyAsync(rec_fd, h->spectra.p, ntr * nf * sizeof(double2), cudaMemcpyDeviceToHost, h->st));
+    if (rec_td && ntr > 0) {
+        if (h->fp64) {
+            CK(cudaMemcpyAsync(rec_td, h->traces.p, ntr * nt * 8, cudaMemcpyDeviceToHost, h->st));
+        } else {
+            std::vector<float> tmp(ntr * nt);
+            CK(cudaMemcpyAsync(tmp.data(), h->traces.p, ntr * nt * 4, cudaMemcpyDeviceToHost, h->st));
+            CK(cudaStreamSynchronize(h->st));
+            for (size_t q = 0; q < tmp.size(); q++) rec_td[q] = tmp[q];
+        }
+    }
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (flag) return fail(MITTET_ERR_DIVERGED, "non-finite receiver samples (unstable time step or model)");
+    return MITTET_OK;
+}
+
+int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *stream) {
+    if (!h) return fail(MITTET_ERR_INVALID_ARG, "null handle");
+    int rc = validate_ready(h, nt);
+    if (rc) return rc;
+    rc = set_device(h);
+    if (rc) return rc;
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, user));
+        CK(cudaStreamWaitEvent(h->st, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    rc = h->fp64 ? run_forward<double>(h, nt) : run_forward<float>(h, nt);
+    if (rc) return rc;
+    const int nf = (int)h->omega.size();
+    const size_t ntr = (size_t)h->nshot * h->nrec;
+    if (rec_fd_dev && nf > 0 && ntr > 0)
+        CK(cudaMemcpyAsync(rec_fd_dev, h->spectra.p, ntr * nf * sizeof(double2), cudaMemcpyDeviceToDevice, h->st));
+    if (user) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, h->st));
+        CK(cudaStreamWaitEvent(user, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    return MITTET_OK;
+}
+
+int mittet_get_volume_dft(mittet_handle *h, int32_t shot, int32_t comp, double *out) {
+    if (!h || !out || shot < 0 || shot >= h->nshot || comp < 0 || comp > 2)
+        return fail(MITTET_ERR_INVALID_ARG, "bad volume DFT request");
+    if (!(h->vmask >> comp & 1) || !h->acc.p) return fail(MITTET_ERR_STATE, "component %d was not accumulated", comp);
+    int rc = set_device(h);
+    if (rc) return rc;
+    const int nf = (int)h->omega.size();
+    const double2 *base = h->acc.as<double2>() + (((size_t)shot * 3 + comp) * nf) * h->fshot;
+    // strip the row padding: [f][nz][ny][px] -> [f][nz][ny][nx]
+    CK(cudaMemcpy2DAsync(out, (size_t)h->g.nx * 16, base, (size_t)h->px * 16, (size_t)h->g.nx * 16,
+                         (size_t)nf * h->g.nz * h->g.ny, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return MITTET_OK;
+}
+
+int mittet_get_fields(mittet_handle *h, int32_t shot, double *out) {
+    if (!h || !out || shot < 0 || shot >= h->nshot || h->alloc_shots != h->nshot)
+        return fail(MITTET_ERR_INVALID_ARG, "bad field request");
+    int rc = set_device(h);
+    if (rc) return rc;
+    const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    for (int c = 0; c < 6; c++) {
+        const char *base = (const char *)h->fields[c].p + (size_t)shot * h->fshot * h->esz;
+        if (h->fp64) {
+            CK(cudaMemcpy2D(out + c * n, (size_t)h->g.nx * 8, base, (size_t)h->px * 8, (size_t)h->g.nx * 8,
+                            (size_t)h->g.nz * h->g.ny, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> tmp(n);
+            CK(cudaMemcpy2D(tmp.data(), (size_t)h->g.nx * 4, base, (size_t)h->px * 4, (size_t)h->g.nx * 4,
+                            (size_t)h->g.nz * h->g.ny, cudaMemcpyDeviceToHost));
+            for (size_t q = 0; q < n; q++) out[c * n + q] = tmp[q];
+        }
+    }
+    return MITTET_OK;
+}
+
+int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double omega0, const double *x, int32_t nf,
+                  const double *omega, int32_t h_factor, double *out) {
+    if (ntrace <= 0 || nt <= 0 || nf <= 0 || !x || !omega || !out || !(dt > 0) || !(omega0 > 0))
+        return fail(MITTET_ERR_INVALID_ARG, "bad f_to_d arguments");
+    CK(cudaSetDevice(device));
+    DevBuf dx_, dom, dout, dish;
+    CK(dx_.ensure((size_t)ntrace * nt * 8));
+    CK(dom.ensure((size_t)nf * 8));
+    CK(dout.ensure((size_t)ntrace * nf * 16));
+    std::vector<unsigned char> ish(ntrace, h_factor ? 1 : 0);
+    CK(dish.ensure(ntrace));
+    CK(cudaMemcpy(dx_.p, x, (size_t)ntrace * nt * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dom.p, omega, (size_t)nf * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dish.p, ish.data(), ntrace, cudaMemcpyHostToDevice));
+    trace_dft_kernel<double><<<nf, 256>>>(dx_.as<double>(), ntrace, nt, dom.as<double>(), nf, dt, omega0,
+                                          dish.as<unsigned char>(), h_factor ? 1 : 0, dout.as<double2>());
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(out, dout.p, (size_t)ntrace * nf * 16, cudaMemcpyDeviceToHost));
+    return MITTET_OK;
+}
+
+int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1; }
+
+int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms) {
+    if (!h || !ms || nsteps <= 0) return fail(MITTET_ERR_INVALID_ARG, "bad timing request");
+    if (h->last_nt < nsteps || h->alloc_shots != h->nshot)
+        return fail(MITTET_ERR_STATE, "run a forward of at least %d steps first", nsteps);
+    int rc = set_device(h);
+    if (rc) return rc;
+    rc = h->fp64 ? time_kernels<double>(h, nsteps, ms) : time_kernels<float>(h, nsteps, ms);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return MITTET_OK;
+}
+
+int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t checkpoint_every, double *misfit,
+                    double *grad) {
+    (void)nt; (void)obs; (void)checkpoint_every; (void)misfit; (void)grad;
+    if (!h) return fail(MITTET_ERR_INVALID_ARG, "null handle");
+    return fail(MITTET_ERR_STATE, "gradient is not available in this build");
+}
+
+}  // extern "C"

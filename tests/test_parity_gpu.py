@@ -1,0 +1,207 @@
+"""GPU parity of the forward path against the oracle and the reference's
+own satan_i kernels (golden fixtures).  Tolerances (rel-L2 over all
+receivers and frequencies of a component class):
+  FP64 fields: 1e-10    FP32 fields + FP64 DFT: 1e-4
+"""
+import os
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from mittet_main_b200 import workloads as W
+from mittet_main_b200.capi import FLAVOR_NCVER0027, FLAVOR_SATAN_I, FP32, FP64, SRC_ELECTRIC
+from mittet_main_b200.solver import ConstPara, MittetSolver, Shot, f_to_d
+from oracle import oracle as O
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+NAMES = ["ex", "ey", "ez", "hx", "hy", "hz"]
+TOL = {FP64: 1e-10, FP32: 1e-4}
+
+
+def oracle_params(cp: ConstPara) -> O.Params:
+    p = O.Params(nx=cp.nx, ny=cp.ny, nz=cp.nz, dx=cp.dx, dy=cp.dy, dz=cp.dz, dt=cp.dt, ncpml=cp.ncpml,
+                 cmax=cp.cmax, omega0=cp.omega0, flavor=cp.flavor, e_sign=cp.e_sign, h_sign=cp.h_sign)
+    if cp.flavor == FLAVOR_SATAN_I:
+        p.c2, p.psi_hyx_typo = O.C2_C, 0
+    return p
+
+
+def oracle_run(wl: W.Workload, cp=None, want_fields=False):
+    cp = cp or wl.cp
+    mu = wl.mu if wl.mu is not None else np.full(wl.sigma.shape, cp.mu0)
+    outs = []
+    for shot in wl.shots:
+        srcs = [(x, y, z, c, k, a) for (x, y, z, c, k, a) in shot.points]
+        outs.append(O.forward(oracle_params(cp), wl.sigma, mu, srcs, wl.wavelet, wl.receivers, wl.nt,
+                              want_fields=want_fields))
+    return outs
+
+
+def split_eh(wl, arr):
+    ise = np.array([r[3] in ("ex", "ey", "ez") for r in wl.receivers])
+    return arr[..., ise, :], arr[..., ~ise, :]
+
+
+def check_spectra(wl, got, ref_traces, tol):
+    """got: [nshot, nrec, nf]; ref_traces: list of [nrec, nt] oracle traces."""
+    for s, tr in enumerate(ref_traces):
+        ref = np.stack([O.dft(tr[r], wl.cp.dt, wl.cp.omega0, wl.omega, h_factor=wl.receivers[r][3].startswith("h"))
+                        for r in range(len(wl.receivers))])
+        ge, gh = split_eh(wl, got[s][None])
+        re_, rh = split_eh(wl, ref[None])
+        assert rel_l2(ge, re_) <= tol, f"E spectra rel-L2 {rel_l2(ge, re_):.3e}"
+        if rh.size:
+            assert rel_l2(gh, rh) <= tol, f"H spectra rel-L2 {rel_l2(gh, rh):.3e}"
+
+
+# ------------------------------------------------ pinned: reference satan_i
+@pytest.mark.parametrize("name", ["satan_ex", "satan_ey", "satan_ez"])
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_gpu_matches_reference_satan_kernels(golden_dir, name, prec):
+    g = dict(np.load(os.path.join(golden_dir, name + ".npz")))
+    ix, iy, iz = (int(v) for v in g["shape"])
+    d = float(g["d"])
+    cp = ConstPara(nx=ix, ny=iy, nz=iz, dx=d, dy=d, dz=d, ncpml=int(g["ncpml"]), dt=float(g["dt"]),
+                   cmax=float(g["cmax"]), omega0=float(g["omega0"]), mu0=O.MU0_C, flavor=FLAVOR_SATAN_I,
+                   precision=prec, check_cfl=False)
+    nt = int(g["nt"])
+    with MittetSolver(cp) as s:
+        s.set_model(g["sigma"])
+        src = [int(v) for v in g["src"]]
+        s.set_shots([Shot(points=[(src[0], src[1], src[2], NAMES[int(g["src_comp"])], SRC_ELECTRIC, 1.0)])])
+        s.set_wavelet(g["wavelet"])
+        s.set_receivers([(int(r[0]), int(r[1]), int(r[2]), NAMES[int(r[3])]) for r in g["receivers"]])
+        _, td = s.forward(nt, want_traces=True)
+        ref = g["traces"]
+        ise = np.array([int(r[3]) < 3 for r in g["receivers"]])
+        assert rel_l2(td[0][ise], ref[ise]) <= TOL[prec]
+        assert rel_l2(td[0][~ise], ref[~ise]) <= TOL[prec]
+        if "fields" in g:
+            F = s.fields(0)
+            for c in range(6):
+                assert rel_l2(F[c], g["fields"][c]) <= TOL[prec] * 10, NAMES[c]
+
+
+# ------------------------------------------------ ncver0027 flavour vs oracle
+@pytest.mark.parametrize("prec", [FP64, FP32])
+@pytest.mark.parametrize("magnetic", [False, True])
+def test_gpu_matches_oracle_ncver_small(prec, magnetic):
+    wl = W.small_case(nt=240, precision=prec, magnetic=magnetic)
+    ref = oracle_run(wl)
+    with W.make_solver(wl) as s:
+        spec, td = s.forward(wl.nt, want_traces=True)
+        assert rel_l2(td[0], ref[0]) <= TOL[prec]
+        check_spectra(wl, spec, ref, TOL[prec])
+
+
+def test_gpu_fp64_final_fields_match_oracle():
+    wl = W.small_case(n=(34, 30, 28), ncpml=7, nt=150, precision=FP64, magnetic=True)
+    tr, F = oracle_run(wl, want_fields=True)[0]
+    with W.make_solver(wl) as s:
+        s.forward(wl.nt)
+        G = s.fields(0)
+    for c in range(6):
+        assert rel_l2(G[c], F[c]) <= 1e-10, NAMES[c]
+
+
+def test_sign_flipped_bp_updates_match_oracle():
+    wl = W.small_case(nt=120, precision=FP64)
+    cp = replace(wl.cp, e_sign=-1, h_sign=-1, check_cfl=True)
+    wl2 = replace(wl, cp=cp)
+    ref = oracle_run(wl2)
+    with W.make_solver(wl2) as s:
+        _, td = s.forward(wl.nt, want_traces=True)
+    assert rel_l2(td[0], ref[0]) <= 1e-10
+
+
+def test_batched_shots_equal_single_shots():
+    wl = W.small_case(nt=150, precision=FP32)
+    pts2 = [(wl.cp.nx // 3, wl.cp.ny // 3, wl.cp.nz // 2, "ey", SRC_ELECTRIC, 0.5)]
+    wl2 = replace(wl, shots=[wl.shots[0], Shot(points=pts2), wl.shots[0]])
+    with W.make_solver(wl2) as s:
+        spec, td = s.forward(wl.nt, want_traces=True)
+    for k, shot in enumerate(wl2.shots):
+        with W.make_solver(replace(wl, shots=[shot])) as s1:
+            sp1, td1 = s1.forward(wl.nt, want_traces=True)
+        assert np.array_equal(td[k], td1[0])
+        assert np.array_equal(spec[k], sp1[0])
+
+
+def test_linearity_in_source_amplitude():
+    wl = W.small_case(nt=100, precision=FP32)
+    x, y, z, c, k, a = wl.shots[0].points[0]
+    wl2 = replace(wl, shots=[Shot(points=[(x, y, z, c, k, 2.0 * a)])])
+    with W.make_solver(wl) as s:
+        _, t1 = s.forward(wl.nt, want_traces=True)
+    with W.make_solver(wl2) as s:
+        _, t2 = s.forward(wl.nt, want_traces=True)
+    assert np.array_equal(2.0 * t1, t2)  # scaling by 2 is exact in binary floating point
+
+
+def test_volume_dft_matches_oracle_dft_of_traces():
+    wl = W.small_case(nt=200, precision=FP32)
+    cells = [(5, 6, 7), (wl.cp.nx // 2, wl.cp.ny // 2, wl.cp.nz // 2 - 2), (wl.cp.nx - 3, 4, wl.cp.nz - 5)]
+    rec = [(x, y, z, c) for (x, y, z) in cells for c in ("ex", "ey", "ez")]
+    wl2 = replace(wl, receivers=rec, volume_dft="xyz")
+    ref = oracle_run(wl2)[0]
+    with W.make_solver(wl2) as s:
+        s.forward(wl.nt)
+        vols = {c: s.volume_dft(0, c) for c in ("ex", "ey", "ez")}
+    got = np.stack([vols[c][:, z - 1, y - 1, x - 1] for (x, y, z, c) in rec])
+    want = np.stack([O.dft(ref[r], wl.cp.dt, wl.cp.omega0, wl.omega) for r in range(len(rec))])
+    assert rel_l2(got, want) <= 1e-4
+
+
+def test_volume_dft_with_ring_remainder():
+    # nt not a multiple of the 16-step ring exercises the partial flush
+    wl = W.small_case(nt=37, precision=FP64)
+    rec = [(wl.cp.nx // 2 + 1, wl.cp.ny // 2, wl.cp.nz // 2, "ex")]
+    wl2 = replace(wl, receivers=rec, volume_dft="x")
+    ref = oracle_run(wl2)[0]
+    with W.make_solver(wl2) as s:
+        s.forward(wl.nt)
+        v = s.volume_dft(0, "ex")
+    x, y, z, _ = rec[0]
+    assert rel_l2(v[:, z - 1, y - 1, x - 1], O.dft(ref[0], wl.cp.dt, wl.cp.omega0, wl.omega)) <= 1e-10
+
+
+def test_standalone_f_to_d_matches_oracle():
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(5, 700))
+    dt, w0 = 7.4e-4, 2 * 3.14159265358979
+    om = np.arange(1, 50) * 2 * np.pi / (700 * dt)
+    got = f_to_d(x, dt, w0, om)
+    ref = np.stack([O.dft(x[r], dt, w0, om) for r in range(5)])
+    assert rel_l2(got, ref) <= 1e-12
+    goth = f_to_d(x, dt, w0, om, h_factor=True)
+    refh = np.stack([O.dft(x[r], dt, w0, om, h_factor=True) for r in range(5)])
+    assert rel_l2(goth, refh) <= 1e-12
+
+
+def test_repeated_forward_is_deterministic():
+    wl = W.small_case(nt=64, precision=FP32)
+    with W.make_solver(wl) as s:
+        a, ta = s.forward(wl.nt, want_traces=True)
+        b, tb = s.forward(wl.nt, want_traces=True)
+    assert np.array_equal(ta, tb) and np.array_equal(a, b)
+
+
+def test_edge_source_and_receivers_at_grid_corners():
+    wl = W.small_case(nt=80, precision=FP64)
+    nx, ny, nz = wl.cp.nx, wl.cp.ny, wl.cp.nz
+    rec = [(1, 1, 1, "ez"), (nx, ny, nz, "hx"), (nx, 1, nz // 2, "ey"), (2, ny - 1, 3, "hz")]
+    wl2 = replace(wl, receivers=rec, shots=[Shot(points=[(3, 3, 3, "ez", SRC_ELECTRIC, 1.0)])])
+    ref = oracle_run(wl2)[0]
+    with W.make_solver(wl2) as s:
+        _, td = s.forward(wl.nt, want_traces=True)
+    assert rel_l2(td[0], ref) <= 1e-10
+
+
+def test_single_step():
+    wl = W.small_case(nt=1, precision=FP64)
+    ref = oracle_run(wl)[0]
+    with W.make_solver(wl) as s:
+        _, td = s.forward(1, want_traces=True)
+    assert np.allclose(td[0], ref, rtol=1e-12, atol=0)
