@@ -288,6 +288,7 @@ def main():
             "shot_solves_per_s": len(wl.shots) * args.steps * world / (t_ms / 1e3),
             "gpu_launches": gpu_launches,
             "kernel_ms": kt,
+            "stencil_variant": solver.tuned_variant(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "kernel": "e_phase_kernel",
                          "alg_bytes_per_launch": ebytes, "peak_source": peak_kind},

@@ -186,7 +186,9 @@ int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t che
 
 /* Device-resident variants for callers that keep data on the GPU (the
  * PyTorch front end).  Pointers are device pointers of the handle's device;
- * stream is a cudaStream_t (NULL = the handle's stream). */
+ * stream is the caller's cudaStream_t (NULL = the legacy default stream): the
+ * solve starts after the work already queued there and the stream waits for
+ * the solve, so events recorded on it bracket the whole solve. */
 int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu, int32_t is_fp64);
 int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *stream);
 
@@ -196,6 +198,10 @@ int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *
  * device time per launch of: magnetic inject, E phase, electric inject,
  * H phase, sampling, volume-DFT flush (0 where a kernel did not run). */
 int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms);
+
+/* Stencil variant the autotuner chose for the E and H phases at the last
+ * forward: {BX, BY, KZ} = thread tile in x, y and cells per thread in z. */
+int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
 
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);

@@ -103,6 +103,7 @@ SIGNATURES = {
     "mittet_set_model_device": (ctypes.c_int, [_VP, _VP, _VP, _I]),
     "mittet_forward_device": (ctypes.c_int, [_VP, _I, _VP, _VP]),
     "mittet_time_kernels": (ctypes.c_int, [_VP, _I, _P(_D)]),
+    "mittet_tuned_variant": (ctypes.c_int, [_VP, _P(_I), _P(_I)]),
     "mittet_last_launch_count": (ctypes.c_int64, [_VP]),
     "mittet_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
 }

@@ -15,10 +15,7 @@
 // plus dt/mu per cell only when a permeability volume is given.  CPML psi
 // variables exist only inside their slabs (compact [shot][...] boxes).
 //
-// Each thread owns one (i, j) column of a z-chunk and marches k upward,
-// keeping the four z-neighbours of the two fields differentiated along z in
-// registers; x/y neighbours come through the read-only L1 path (the fields
-// read in a phase are never written in that phase).
+// The two half-step kernels are in stencil.cuh.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -50,7 +47,6 @@ struct PhaseArgs {
     DSlab slab[3];          // slab groups of this phase (x, y, z)
     T c1, c2, c2t;          // stencil weights; c2t = c2 (psi_Hyx typo) or c1
     T sgn;                  // +1 / -1 ("bp" updates)
-    int zchunk;
     // full-volume DFT ring (E phase only): ring[slot][vcomp][shot][cell]
     T *ring;
     int ring_k;             // ring depth K (0 = no ring)
@@ -92,279 +88,11 @@ __device__ __forceinline__ T pv(const PhaseArgs<T> &a, int axis, int which, int 
     return ldg(a.prof + ((size_t)axis * 8 + which) * a.nmax + i);
 }
 
-// ------------------------------------------------------------------ E phase
-//
-// Ex = ca_x Ex + s cb_x (Dy(Hz)/kedy - Dz(Hy)/kedz)   with D backward (2,4):
-//   D(F)[v] = c1 (F[v] - F[v-1]) + c2 (F[v+1] - F[v-2])
-// ca = (1-h)/(1+h), cb = m/(1+h), h = esig * m / 2 on the component's axis.
-// CPML: psi = be psi + ce/d * D(F); the E field gets +-cb psi.
-template <typename T, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY) e_phase_kernel(PhaseArgs<T> a) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
-    const int shot = blockIdx.z / nzc;
-    const int k0 = (blockIdx.z % nzc) * a.zchunk;
-    const int k1 = min(k0 + a.zchunk, a.nz);
-    if (i >= a.nx || j >= a.ny) return;
+}  // namespace mittet
 
-    const long long sb = (long long)shot * a.fshot;
-    T *__restrict__ Ex = a.f[0] + sb;
-    T *__restrict__ Ey = a.f[1] + sb;
-    T *__restrict__ Ez = a.f[2] + sb;
-    const T *__restrict__ Hx = a.f[3] + sb;
-    const T *__restrict__ Hy = a.f[4] + sb;
-    const T *__restrict__ Hz = a.f[5] + sb;
-    const long long py = a.px, pz = a.plane;
-    const T c1 = a.c1, c2 = a.c2;
+#include "stencil.cuh"
 
-    // per-column profile values
-    const T esh_x = pv(a, 0, 0, i), esh_y = pv(a, 1, 0, j);
-    const T ik_x = pv(a, 0, 6, i), ik_y = pv(a, 1, 6, j);
-    const bool vx = (i >= 2) && (i + 1 < a.nx);
-    const bool vy = (j >= 2) && (j + 1 < a.ny);
-    const int lx = slab_local(a.slab[0], i);
-    const int ly = slab_local(a.slab[1], j);
-    const bool sx_col = lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1];
-    const bool sy_col = ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0];
-    const bool sz_col = i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
-                        j < a.slab[2].other.hi[1];
-    const T be_x = sx_col ? pv(a, 0, 2, i) : T(0), ced_x = sx_col ? pv(a, 0, 3, i) : T(0);
-    const T be_y = sy_col ? pv(a, 1, 2, j) : T(0), ced_y = sy_col ? pv(a, 1, 3, j) : T(0);
-
-    const int step = a.ring_k > 0 ? *a.d_step : 0;
-    const int slot = a.ring_k > 0 ? step % a.ring_k : 0;
-
-    // z window of Hx and Hy at (i, j): w[0..3] = F(k-2), F(k-1), F(k), F(k+1)
-    const long long col = (long long)j * py + i;
-    T wx[4], wy[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int kk = k0 - 2 + q;
-        const bool ok = kk >= 0 && kk < a.nz;
-        wx[q] = ok ? ldg(Hx + kk * pz + col) : T(0);
-        wy[q] = ok ? ldg(Hy + kk * pz + col) : T(0);
-    }
-
-    for (int k = k0; k < k1; ++k) {
-        const long long c = k * pz + col;
-        const bool vz = (k >= 2) && (k + 1 < a.nz);
-        const T hz = ldg(Hz + c);
-
-        T dyHz = T(0), dxHz = T(0), dxHy = T(0), dyHx = T(0), dzHy = T(0), dzHx = T(0);
-        if (vy) {
-            dyHz = c1 * (hz - ldg(Hz + c - py)) + c2 * (ldg(Hz + c + py) - ldg(Hz + c - 2 * py));
-            dyHx = c1 * (wx[2] - ldg(Hx + c - py)) + c2 * (ldg(Hx + c + py) - ldg(Hx + c - 2 * py));
-        }
-        if (vx) {
-            dxHz = c1 * (hz - ldg(Hz + c - 1)) + c2 * (ldg(Hz + c + 1) - ldg(Hz + c - 2));
-            dxHy = c1 * (wy[2] - ldg(Hy + c - 1)) + c2 * (ldg(Hy + c + 1) - ldg(Hy + c - 2));
-        }
-        if (vz) {
-            dzHy = c1 * (wy[2] - wy[1]) + c2 * (wy[3] - wy[0]);
-            dzHx = c1 * (wx[2] - wx[1]) + c2 * (wx[3] - wx[0]);
-        }
-
-        const T m = ldg(a.m + (long long)k * pz + col);
-        const T esh_z = pv(a, 2, 0, k);
-        const T ik_z = pv(a, 2, 6, k);
-        T ca_x = T(1), cb_x = m, ca_y = T(1), cb_y = m, ca_z = T(1), cb_z = m;
-        if (esh_x != T(0)) { const T h = esh_x * m; const T r = rcp(T(1) + h); ca_x = (T(1) - h) * r; cb_x = m * r; }
-        if (esh_y != T(0)) { const T h = esh_y * m; const T r = rcp(T(1) + h); ca_y = (T(1) - h) * r; cb_y = m * r; }
-        if (esh_z != T(0)) { const T h = esh_z * m; const T r = rcp(T(1) + h); ca_z = (T(1) - h) * r; cb_z = m * r; }
-
-        T ex = Ex[c], ey = Ey[c], ez = Ez[c];
-        if (in_box(a.upd[0], i, j, k)) ex = ca_x * ex + a.sgn * cb_x * (dyHz * ik_y - dzHy * ik_z);
-        if (in_box(a.upd[1], i, j, k)) ey = ca_y * ey + a.sgn * cb_y * (dzHx * ik_z - dxHz * ik_x);
-        if (in_box(a.upd[2], i, j, k)) ez = ca_z * ez + a.sgn * cb_z * (dxHy * ik_x - dyHx * ik_y);
-
-        // CPML_E4: x slabs, y slabs, z slabs
-        if (sx_col && k >= a.slab[0].other.lo[2] && k < a.slab[0].other.hi[2]) {
-            const long long q = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
-            T p0 = a.psi[0][0][q], p1 = a.psi[0][1][q];
-            p0 = be_x * p0 + ced_x * dxHy;  // psi_Ezx
-            p1 = be_x * p1 + ced_x * dxHz;  // psi_Eyx
-            a.psi[0][0][q] = p0;
-            a.psi[0][1][q] = p1;
-            ez = ez + cb_z * p0;
-            ey = ey - cb_y * p1;
-        }
-        if (sy_col && k >= a.slab[1].other.lo[2] && k < a.slab[1].other.hi[2]) {
-            const long long q = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
-            T p0 = a.psi[1][0][q], p1 = a.psi[1][1][q];
-            p0 = be_y * p0 + ced_y * dyHz;  // psi_Exy
-            p1 = be_y * p1 + ced_y * dyHx;  // psi_Ezy
-            a.psi[1][0][q] = p0;
-            a.psi[1][1][q] = p1;
-            ex = ex + cb_x * p0;
-            ez = ez - cb_z * p1;
-        }
-        if (sz_col) {
-            const int lz = slab_local(a.slab[2], k);
-            if (lz >= 0) {
-                const long long q = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
-                const T be_z = pv(a, 2, 2, k), ced_z = pv(a, 2, 3, k);
-                T p0 = a.psi[2][0][q], p1 = a.psi[2][1][q];
-                p0 = be_z * p0 + ced_z * dzHx;  // psi_Eyz
-                p1 = be_z * p1 + ced_z * dzHy;  // psi_Exz
-                a.psi[2][0][q] = p0;
-                a.psi[2][1][q] = p1;
-                ey = ey + cb_y * p0;
-                ex = ex - cb_x * p1;
-            }
-        }
-        Ex[c] = ex;
-        Ey[c] = ey;
-        Ez[c] = ez;
-
-        if (a.ring_k > 0) {
-            T *r = a.ring + (long long)slot * 3 * a.ring_comp + sb + c;
-            if (a.vmask & 1) r[0] = ex;
-            if (a.vmask & 2) r[a.ring_comp] = ey;
-            if (a.vmask & 4) r[2 * a.ring_comp] = ez;
-        }
-
-        // advance the z windows
-#pragma unroll
-        for (int q = 0; q < 3; q++) { wx[q] = wx[q + 1]; wy[q] = wy[q + 1]; }
-        const int kn = k + 2;
-        const bool ok = kn < a.nz;
-        wx[3] = ok ? ldg(Hx + kn * pz + col) : T(0);
-        wy[3] = ok ? ldg(Hy + kn * pz + col) : T(0);
-    }
-}
-
-// ------------------------------------------------------------------ H phase
-//
-// Hx = da_x Hx - s db_x (D+y(Ez)/khdy - D+z(Ey)/khdz)  with D+ forward (2,4):
-//   D+(F)[v] = c1 (F[v+1] - F[v]) + c2 (F[v+2] - F[v-1])
-// da = (1-h)/(1+h), db = (dt/mu)/(1+h), h = msig * m / 2.
-template <typename T, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY) h_phase_kernel(PhaseArgs<T> a) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
-    const int shot = blockIdx.z / nzc;
-    const int k0 = (blockIdx.z % nzc) * a.zchunk;
-    const int k1 = min(k0 + a.zchunk, a.nz);
-    if (i >= a.nx || j >= a.ny) return;
-
-    const long long sb = (long long)shot * a.fshot;
-    const T *__restrict__ Ex = a.f[0] + sb;
-    const T *__restrict__ Ey = a.f[1] + sb;
-    const T *__restrict__ Ez = a.f[2] + sb;
-    T *__restrict__ Hx = a.f[3] + sb;
-    T *__restrict__ Hy = a.f[4] + sb;
-    T *__restrict__ Hz = a.f[5] + sb;
-    const long long py = a.px, pz = a.plane;
-    const T c1 = a.c1, c2 = a.c2;
-
-    const T msh_x = pv(a, 0, 1, i), msh_y = pv(a, 1, 1, j);
-    const T ik_x = pv(a, 0, 7, i), ik_y = pv(a, 1, 7, j);
-    const bool vx = (i >= 1) && (i + 2 < a.nx);
-    const bool vy = (j >= 1) && (j + 2 < a.ny);
-    const int lx = slab_local(a.slab[0], i);
-    const int ly = slab_local(a.slab[1], j);
-    const bool sx_col = lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1];
-    const bool sy_col = ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0];
-    const bool sz_col = i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
-                        j < a.slab[2].other.hi[1];
-    const T bh_x = sx_col ? pv(a, 0, 4, i) : T(0), chd_x = sx_col ? pv(a, 0, 5, i) : T(0);
-    const T bh_y = sy_col ? pv(a, 1, 4, j) : T(0), chd_y = sy_col ? pv(a, 1, 5, j) : T(0);
-
-    // z window of Ex and Ey: w[0..3] = F(k-1), F(k), F(k+1), F(k+2)
-    const long long col = (long long)j * py + i;
-    T wx[4], wy[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int kk = k0 - 1 + q;
-        const bool ok = kk >= 0 && kk < a.nz;
-        wx[q] = ok ? ldg(Ex + kk * pz + col) : T(0);
-        wy[q] = ok ? ldg(Ey + kk * pz + col) : T(0);
-    }
-
-    for (int k = k0; k < k1; ++k) {
-        const long long c = k * pz + col;
-        const bool vz = (k >= 1) && (k + 2 < a.nz);
-        const T ez = ldg(Ez + c);
-
-        T dyEz = T(0), dyEx = T(0), dxEz = T(0), dxEy = T(0), dzEy = T(0), dzEx = T(0), dxEzt = T(0);
-        if (vy) {
-            dyEz = c1 * (ldg(Ez + c + py) - ez) + c2 * (ldg(Ez + c + 2 * py) - ldg(Ez + c - py));
-            dyEx = c1 * (ldg(Ex + c + py) - wx[1]) + c2 * (ldg(Ex + c + 2 * py) - ldg(Ex + c - py));
-        }
-        if (vx) {
-            const T ezp1 = ldg(Ez + c + 1), ezp2 = ldg(Ez + c + 2), ezm1 = ldg(Ez + c - 1);
-            dxEz = c1 * (ezp1 - ez) + c2 * (ezp2 - ezm1);
-            dxEzt = c1 * ezp1 - a.c2t * ez + c2 * ezp2 - c2 * ezm1;  // psi_Hyx stencil (cpu_cpml4.f90:400)
-            dxEy = c1 * (ldg(Ey + c + 1) - wy[1]) + c2 * (ldg(Ey + c + 2) - ldg(Ey + c - 1));
-        }
-        if (vz) {
-            dzEy = c1 * (wy[2] - wy[1]) + c2 * (wy[3] - wy[0]);
-            dzEx = c1 * (wx[2] - wx[1]) + c2 * (wx[3] - wx[0]);
-        }
-
-        const T m = ldg(a.m + (long long)k * pz + col);
-        const T dm = a.dtmu ? ldg(a.dtmu + (long long)k * pz + col) : a.dtmu0;
-        const T msh_z = pv(a, 2, 1, k);
-        const T ik_z = pv(a, 2, 7, k);
-        T da_x = T(1), db_x = dm, da_y = T(1), db_y = dm, da_z = T(1), db_z = dm;
-        if (msh_x != T(0)) { const T h = msh_x * m; const T r = rcp(T(1) + h); da_x = (T(1) - h) * r; db_x = dm * r; }
-        if (msh_y != T(0)) { const T h = msh_y * m; const T r = rcp(T(1) + h); da_y = (T(1) - h) * r; db_y = dm * r; }
-        if (msh_z != T(0)) { const T h = msh_z * m; const T r = rcp(T(1) + h); da_z = (T(1) - h) * r; db_z = dm * r; }
-
-        T hx = Hx[c], hy = Hy[c], hz = Hz[c];
-        if (in_box(a.upd[0], i, j, k)) hx = da_x * hx - a.sgn * db_x * (dyEz * ik_y - dzEy * ik_z);
-        if (in_box(a.upd[1], i, j, k)) hy = da_y * hy - a.sgn * db_y * (dzEx * ik_z - dxEz * ik_x);
-        if (in_box(a.upd[2], i, j, k)) hz = da_z * hz - a.sgn * db_z * (dxEy * ik_x - dyEx * ik_y);
-
-        // CPML_H4: x slabs, y slabs, z slabs
-        if (sx_col && k >= a.slab[0].other.lo[2] && k < a.slab[0].other.hi[2]) {
-            const long long q = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
-            T p0 = a.psi[0][0][q], p1 = a.psi[0][1][q];
-            p0 = bh_x * p0 + chd_x * dxEy;   // psi_Hzx
-            p1 = bh_x * p1 + chd_x * dxEzt;  // psi_Hyx
-            a.psi[0][0][q] = p0;
-            a.psi[0][1][q] = p1;
-            hz = hz - db_z * p0;
-            hy = hy + db_y * p1;
-        }
-        if (sy_col && k >= a.slab[1].other.lo[2] && k < a.slab[1].other.hi[2]) {
-            const long long q = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
-            T p0 = a.psi[1][0][q], p1 = a.psi[1][1][q];
-            p0 = bh_y * p0 + chd_y * dyEz;  // psi_Hxy
-            p1 = bh_y * p1 + chd_y * dyEx;  // psi_Hzy
-            a.psi[1][0][q] = p0;
-            a.psi[1][1][q] = p1;
-            hx = hx - db_x * p0;
-            hz = hz + db_z * p1;
-        }
-        if (sz_col) {
-            const int lz = slab_local(a.slab[2], k);
-            if (lz >= 0) {
-                const long long q = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
-                const T bh_z = pv(a, 2, 4, k), chd_z = pv(a, 2, 5, k);
-                T p0 = a.psi[2][0][q], p1 = a.psi[2][1][q];
-                p0 = bh_z * p0 + chd_z * dzEx;  // psi_Hyz
-                p1 = bh_z * p1 + chd_z * dzEy;  // psi_Hxz
-                a.psi[2][0][q] = p0;
-                a.psi[2][1][q] = p1;
-                hy = hy - db_y * p0;
-                hx = hx + db_x * p1;
-            }
-        }
-        Hx[c] = hx;
-        Hy[c] = hy;
-        Hz[c] = hz;
-
-#pragma unroll
-        for (int q = 0; q < 3; q++) { wx[q] = wx[q + 1]; wy[q] = wy[q + 1]; }
-        const int kn = k + 3;
-        const bool ok = kn < a.nz;
-        wx[3] = ok ? ldg(Ex + kn * pz + col) : T(0);
-        wy[3] = ok ? ldg(Ey + kn * pz + col) : T(0);
-    }
-}
+namespace mittet {
 
 // ---------------------------------------------------------- point sources
 struct SrcPoint {
@@ -433,12 +161,13 @@ __global__ void sample_kernel(SampleArgs<T> a) {
 //
 // X(w_f) = sum_n x[n] dt exp((i-1) sqrt(w0 w_f) n dt), times sqrt(-2 w0/(i w_f))
 // for H traces when hfac is set (cpu_f_to_d_e.f90:140-148, cpu_f_to_d_h.f90:146-148).
+// Trace t is receiver t % nrec_h of its shot (is_h has nrec_h entries).
 // Block = one frequency; threads stride over traces; the weights of a chunk
 // of time samples are computed once per block into shared memory in FP64.
 template <typename T>
 __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, const double *__restrict__ omega,
-                                 int nf, double dt, double omega0, const unsigned char *__restrict__ is_h, int hfac,
-                                 double2 *__restrict__ out) {
+                                 int nf, double dt, double omega0, const unsigned char *__restrict__ is_h, int nrec_h,
+                                 int hfac, double2 *__restrict__ out) {
     constexpr int CH = 256;
     __shared__ double2 w[CH];
     const int f = blockIdx.x;
@@ -474,7 +203,7 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
             }
         }
         if (t < ntrace) {
-            if (hfac && is_h && is_h[t]) {
+            if (hfac && is_h && is_h[t % nrec_h]) {
                 const double r2 = re * hf.x - im * hf.y, i2 = re * hf.y + im * hf.x;
                 re = r2;
                 im = i2;
@@ -486,33 +215,48 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 
 // ---------------------------------------------------- full-volume f_to_d
 //
-// acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring[s][vc][shot][cell]
-// (weights wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt), FP64).
+// Every ring_k steps the E phase has left the last ring_k values of each
+// selected E component in the ring; this kernel folds them into the FP64
+// accumulators:
+//   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring[s][vc][shot][cell],
+//   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
+// One thread per (shot, cell); the ring is read once, the accumulators of up
+// to 8 frequencies are held in registers, the weights sit in shared memory.
 template <typename T>
-__global__ void volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int vmask, int nshot,
-                                  long long fshot, int cnt, int n0, const double2 *__restrict__ wt, int nf,
-                                  double2 *__restrict__ acc) {
-    const long long tot = (long long)nshot * fshot;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
-        const int shot = (int)(e / fshot);
-        const long long cell = e - (long long)shot * fshot;
+__global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int vmask,
+                                                         long long fshot, int cnt, int n0,
+                                                         const double2 *__restrict__ wt, int nf,
+                                                         double2 *__restrict__ acc) {
+    extern __shared__ double2 sw[];  // [cnt][nf]
+    for (int q = threadIdx.x; q < cnt * nf; q += blockDim.x) sw[q] = wt[(long long)n0 * nf + q];
+    __syncthreads();
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ring_comp;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long shot = e / fshot;
+        const long long cell = e - shot * fshot;
         for (int vc = 0; vc < 3; vc++) {
             if (!(vmask >> vc & 1)) continue;
-            double xs[16];
+            double2 *__restrict__ ap = acc + ((shot * 3 + vc) * nf) * fshot + cell;
+            const T *__restrict__ rp = ring + (long long)vc * ring_comp + e;
+            for (int f0 = 0; f0 < nf; f0 += 8) {
+                const int fn = min(8, nf - f0);
+                double ar[8], ai[8];
 #pragma unroll
-            for (int s = 0; s < 16; s++) xs[s] = s < cnt ? (double)ring[((long long)s * 3 + vc) * ring_comp + e] : 0.0;
-            double2 *ap = acc + (((long long)shot * 3 + vc) * nf) * fshot + cell;
-            for (int f = 0; f < nf; f++) {
-                double2 v = ap[(long long)f * fshot];
+                for (int f = 0; f < 8; f++) {
+                    if (f < fn) { const double2 v = ap[(long long)(f0 + f) * fshot]; ar[f] = v.x; ai[f] = v.y; }
+                    else { ar[f] = 0.0; ai[f] = 0.0; }
+                }
+                for (int s = 0; s < cnt; s++) {
+                    const double x = (double)__ldg(rp + (long long)s * 3 * ring_comp);
+                    const double2 *w = sw + s * nf + f0;
 #pragma unroll
-                for (int s = 0; s < 16; s++) {
-                    if (s < cnt) {
-                        const double2 w = wt[(long long)(n0 + s) * nf + f];
-                        v.x += w.x * xs[s];
-                        v.y += w.y * xs[s];
+                    for (int f = 0; f < 8; f++) {
+                        if (f < fn) { ar[f] = fma(w[f].x, x, ar[f]); ai[f] = fma(w[f].y, x, ai[f]); }
                     }
                 }
-                ap[(long long)f * fshot] = v;
+#pragma unroll
+                for (int f = 0; f < 8; f++)
+                    if (f < fn) ap[(long long)(f0 + f) * fshot] = make_double2(ar[f], ai[f]);
             }
         }
     }

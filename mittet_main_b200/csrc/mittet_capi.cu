@@ -13,8 +13,12 @@
 #include <complex>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/mittet.h"
@@ -116,7 +120,9 @@ struct mittet_handle_s {
     DevBuf d_omega;
 
     uint32_t vmask = 0;
-    int ring_k = 16;
+    int ring_k = 32;
+    int var_e = 1, var_h = 1;  // stencil variants (index into variants<T>())
+    bool tuned = false;
     DevBuf ring, acc, wtab;
 
     DevBuf fields[6], psiE[3][2], psiH[3][2];
@@ -150,6 +156,7 @@ void drop_graph(mittet_handle *h) {
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     h->gexec = nullptr;
     h->graph_steps = 0;
+    h->tuned = false;  // the shot count or ring may have changed
 }
 
 int ensure_state(mittet_handle *h) {
@@ -198,7 +205,6 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
     a.c2 = (T)h->ph.c2;
     a.c2t = (T)(h->ph.psi_hyx_typo ? h->ph.c2 : h->ph.c1);
     a.sgn = (T)(e_phase ? h->ph.e_sign : h->ph.h_sign);
-    a.zchunk = 16;
     a.d_step = h->d_step.as<int>();
     if (e_phase && h->vmask) {
         a.ring = h->ring.as<T>();
@@ -209,31 +215,112 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
     return a;
 }
 
-constexpr int BX = 32, BY = 8;
+// Stencil variants (tile BX x BY, KZ cells per thread) the autotuner picks from.
+template <typename T>
+struct Variant {
+    int bx, by, kz;
+    void (*e)(PhaseArgs<T>);
+    void (*h)(PhaseArgs<T>);
+};
+
+template <typename T>
+const std::vector<Variant<T>> &variants() {
+    static const std::vector<Variant<T>> v = {
+#define MITTET_X(a, b, c) {a, b, c, e_phase_kernel<T, a, b, c>, h_phase_kernel<T, a, b, c>},
+        MITTET_STENCIL_VARIANTS(MITTET_X)
+#undef MITTET_X
+    };
+    return v;
+}
+
+template <typename T>
+void launch_phase(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a) {
+    const Variant<T> &v = variants<T>()[vi];
+    dim3 grid((h->g.nx + v.bx - 1) / v.bx, (h->g.ny + v.by - 1) / v.by, h->nshot * ((h->g.nz + v.kz - 1) / v.kz));
+    dim3 block(v.bx, v.by);
+    if (e) v.e<<<grid, block, 0, h->st>>>(a);
+    else v.h<<<grid, block, 0, h->st>>>(a);
+}
 
 template <typename T>
 void launch_step(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha, const InjectArgs<T> &ia_m,
                  const InjectArgs<T> &ia_e, const SampleArgs<T> &sa) {
-    const int nzc = (h->g.nz + ea.zchunk - 1) / ea.zchunk;
-    dim3 grid((h->g.nx + BX - 1) / BX, (h->g.ny + BY - 1) / BY, h->nshot * nzc);
-    dim3 block(BX, BY);
     if (h->has_mag) { inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m); h->launches++; }
-    e_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ea);
+    launch_phase<T>(h, true, h->var_e, ea);
     h->launches++;
     if (h->has_ele) { inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e); h->launches++; }
-    h_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ha);
+    launch_phase<T>(h, false, h->var_h, ha);
     h->launches++;
     sample_kernel<T><<<1, 1024, 0, h->st>>>(sa);
     h->launches++;
 }
 
+// ------------------------------------------------------------- autotuner
+// Picks, per phase, the fastest stencil variant for this grid, shot count and
+// precision by timing each candidate on the handle's own buffers (zero
+// fields, so the state is untouched apart from the ring slot written by the
+// E phase).  Results are cached for the process.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
+
+template <typename T>
+int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
+    const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            h->var_e = it->second.first;
+            h->var_h = it->second.second;
+            return MITTET_OK;
+        }
+    }
+    const char *fix = std::getenv("MITTET_VARIANT");
+    const int nv = (int)variants<T>().size();
+    if (fix) {
+        const int v = std::atoi(fix);
+        if (v >= 0 && v < nv) { h->var_e = h->var_h = v; return MITTET_OK; }
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const long long cells = (long long)h->nshot * h->g.nx * h->g.ny * h->g.nz;
+    const int reps = cells > (1LL << 24) ? 2 : (cells > (1LL << 20) ? 5 : 20);
+    float best[2] = {1e30f, 1e30f};
+    for (int v = 0; v < nv; v++) {
+        for (int ph = 0; ph < 2; ph++) {
+            const PhaseArgs<T> &a = ph == 0 ? ea : ha;
+            launch_phase<T>(h, ph == 0, v, a);  // warm-up
+            CK(cudaEventRecord(e0, h->st));
+            for (int r = 0; r < reps; r++) launch_phase<T>(h, ph == 0, v, a);
+            CK(cudaEventRecord(e1, h->st));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaGetLastError());
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (std::getenv("MITTET_TUNE_LOG"))
+                fprintf(stderr, "autotune %s %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", variants<T>()[v].bx,
+                        variants<T>()[v].by, variants<T>()[v].kz, ms / reps);
+            if (ms < best[ph]) {
+                best[ph] = ms;
+                (ph == 0 ? h->var_e : h->var_h) = v;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = std::make_pair(h->var_e, h->var_h);
+    return MITTET_OK;
+}
+
 template <typename T>
 void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
     const long long tot = (long long)h->nshot * h->fshot;
-    int blocks = (int)std::min<long long>((tot + 255) / 256, 148LL * 16);
-    volume_dft_kernel<T><<<blocks, 256, 0, h->st>>>(h->ring.as<T>(), tot, (int)h->vmask, h->nshot, h->fshot, cnt, n0,
-                                                    h->wtab.as<double2>(), (int)h->omega.size(),
-                                                    h->acc.as<double2>());
+    const int nf = (int)h->omega.size();
+    int blocks = (int)std::min<long long>((tot + 255) / 256, 148LL * 8);
+    volume_dft_kernel<T><<<blocks, 256, (size_t)cnt * nf * sizeof(double2), h->st>>>(
+        h->ring.as<T>(), tot, (int)h->vmask, h->fshot, cnt, n0, h->wtab.as<double2>(), nf, h->acc.as<double2>());
     h->launches++;
 }
 
@@ -300,6 +387,13 @@ int run_forward(mittet_handle *h, int nt) {
     sa.nt = nt;
     sa.d_step = h->d_step.as<int>();
 
+    if (!h->tuned) {
+        rc = autotune<T>(h, ea, ha);
+        if (rc) return rc;
+        rc = ensure_state(h);  // back to zero fields and psi
+        if (rc) return rc;
+        h->tuned = true;
+    }
     h->launches = 0;
     // One graph holds G = ring_k steps (+ the volume flush when enabled).
     const int G = h->ring_k;
@@ -341,7 +435,7 @@ int run_forward(mittet_handle *h, int nt) {
             CK(h->spectra.ensure((size_t)ns * h->nrec * nf * sizeof(double2)));
             trace_dft_kernel<T><<<nf, 256, 0, h->st>>>(h->traces.as<T>(), ns * h->nrec, nt, h->d_omega.as<double>(),
                                                        nf, h->ph.dt, h->ph.omega0, h->rec_is_h.as<unsigned char>(),
-                                                       h->hfac, h->spectra.as<double2>());
+                                                       h->nrec, h->hfac, h->spectra.as<double2>());
             h->launches++;
         }
     }
@@ -387,9 +481,6 @@ int time_kernels(mittet_handle *h, int nsteps, double *ms) {
     sa.traces = h->traces.as<T>();
     sa.nt = nt;
     sa.d_step = h->d_step.as<int>();
-    const int nzc = (h->g.nz + ea.zchunk - 1) / ea.zchunk;
-    dim3 grid((h->g.nx + BX - 1) / BX, (h->g.ny + BY - 1) / BY, h->nshot * nzc);
-    dim3 block(BX, BY);
     cudaEvent_t ev[12];
     for (int q = 0; q < 12; q++) CK(cudaEventCreate(&ev[q]));
     double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -398,11 +489,11 @@ int time_kernels(mittet_handle *h, int nsteps, double *ms) {
         CK(cudaEventRecord(ev[0], h->st));
         if (h->has_mag) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m);
         CK(cudaEventRecord(ev[1], h->st));
-        e_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ea);
+        launch_phase<T>(h, true, h->var_e, ea);
         CK(cudaEventRecord(ev[2], h->st));
         if (h->has_ele) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e);
         CK(cudaEventRecord(ev[3], h->st));
-        h_phase_kernel<T, BX, BY><<<grid, block, 0, h->st>>>(ha);
+        launch_phase<T>(h, false, h->var_h, ha);
         CK(cudaEventRecord(ev[4], h->st));
         sample_kernel<T><<<1, 1024, 0, h->st>>>(sa);  // also advances the step counter
         CK(cudaEventRecord(ev[5], h->st));
@@ -849,8 +940,10 @@ int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *
     if (rc) return rc;
     rc = set_device(h);
     if (rc) return rc;
-    cudaStream_t user = (cudaStream_t)stream;
-    if (user) {
+    // the caller's stream; NULL is the legacy default stream, which the
+    // handle's non-blocking stream does not synchronise with implicitly
+    cudaStream_t user = stream ? (cudaStream_t)stream : cudaStreamLegacy;
+    {
         cudaEvent_t ev;
         CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         CK(cudaEventRecord(ev, user));
@@ -863,7 +956,7 @@ int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *
     const size_t ntr = (size_t)h->nshot * h->nrec;
     if (rec_fd_dev && nf > 0 && ntr > 0)
         CK(cudaMemcpyAsync(rec_fd_dev, h->spectra.p, ntr * nf * sizeof(double2), cudaMemcpyDeviceToDevice, h->st));
-    if (user) {
+    {
         cudaEvent_t ev;
         CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         CK(cudaEventRecord(ev, h->st));
@@ -924,13 +1017,27 @@ int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double 
     CK(cudaMemcpy(dom.p, omega, (size_t)nf * 8, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dish.p, ish.data(), ntrace, cudaMemcpyHostToDevice));
     trace_dft_kernel<double><<<nf, 256>>>(dx_.as<double>(), ntrace, nt, dom.as<double>(), nf, dt, omega0,
-                                          dish.as<unsigned char>(), h_factor ? 1 : 0, dout.as<double2>());
+                                          dish.as<unsigned char>(), ntrace, h_factor ? 1 : 0, dout.as<double2>());
     CK(cudaGetLastError());
     CK(cudaMemcpy(out, dout.p, (size_t)ntrace * nf * 16, cudaMemcpyDeviceToHost));
     return MITTET_OK;
 }
 
 int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1; }
+
+int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg) {
+    if (!h || !e_cfg || !h_cfg) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    if (h->fp64) {
+        const auto &v = variants<double>();
+        e_cfg[0] = v[h->var_e].bx; e_cfg[1] = v[h->var_e].by; e_cfg[2] = v[h->var_e].kz;
+        h_cfg[0] = v[h->var_h].bx; h_cfg[1] = v[h->var_h].by; h_cfg[2] = v[h->var_h].kz;
+    } else {
+        const auto &v = variants<float>();
+        e_cfg[0] = v[h->var_e].bx; e_cfg[1] = v[h->var_e].by; e_cfg[2] = v[h->var_e].kz;
+        h_cfg[0] = v[h->var_h].bx; h_cfg[1] = v[h->var_h].by; h_cfg[2] = v[h->var_h].kz;
+    }
+    return MITTET_OK;
+}
 
 int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms) {
     if (!h || !ms || nsteps <= 0) return fail(MITTET_ERR_INVALID_ARG, "bad timing request");

@@ -241,6 +241,12 @@ class MittetSolver:
         check(self._lib.mittet_time_kernels(self._h, nsteps, _dptr(ms)))
         return dict(zip(["inject_magnetic", "e_phase", "inject_electric", "h_phase", "sample", "volume_dft"], ms.tolist()))
 
+    def tuned_variant(self) -> dict:
+        e = (ctypes.c_int32 * 3)()
+        h = (ctypes.c_int32 * 3)()
+        check(self._lib.mittet_tuned_variant(self._h, e, h))
+        return {"e_phase": list(e), "h_phase": list(h)}
+
     def launch_count(self) -> int:
         return int(self._lib.mittet_last_launch_count(self._h))
 
