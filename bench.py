@@ -162,6 +162,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-seg-steps", type=int, default=4)
+    ap.add_argument("--grid", default="", help="NXxNYxNZ override of the workload grid (profiling cases)")
+    ap.add_argument("--no-volume", action="store_true", help="disable the full-volume f_to_d")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -175,6 +177,10 @@ def main():
     kw = {"precision": prec}
     if args.nt:
         kw["nt"] = args.nt
+    if args.grid:
+        kw["nx"], kw["ny"], kw["nz"] = (int(v) for v in args.grid.split("x"))
+    if args.no_volume and args.workload == "plain_gpu":
+        kw["volume"] = False
     wl = mk(**kw)
 
     if args.impl == "reference":

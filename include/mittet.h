@@ -200,7 +200,8 @@ int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *
 int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms);
 
 /* Stencil variant the autotuner chose for the E and H phases at the last
- * forward: {BX, BY, KZ} = thread tile in x, y and cells per thread in z. */
+ * forward: {VX, BX, BY, KZ} = x cells per thread, thread tile in x and y,
+ * z cells per thread. */
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
 
 /* Number of kernels the last forward launched (for launch accounting). */

@@ -47,6 +47,7 @@ struct PhaseArgs {
     DSlab slab[3];          // slab groups of this phase (x, y, z)
     T c1, c2, c2t;          // stencil weights; c2t = c2 (psi_Hyx typo) or c1
     T sgn;                  // +1 / -1 ("bp" updates)
+    T ik[3];                // 1/d per axis: the 1/ked (1/khd) value of every interior cell
     // full-volume DFT ring (E phase only): ring[slot][vcomp][shot][cell]
     T *ring;
     int ring_k;             // ring depth K (0 = no ring)
@@ -220,44 +221,53 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 // accumulators:
 //   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring[s][vc][shot][cell],
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
-// One thread per (shot, cell); the ring is read once, the accumulators of up
-// to 8 frequencies are held in registers, the weights sit in shared memory.
+// One thread per (component, shot, cell).  Ring values are loaded 16 at a
+// time before any arithmetic (16 loads in flight per thread); accumulators of
+// up to 8 frequencies stay in registers; the weights sit in shared memory.
 template <typename T>
-__global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int vmask,
-                                                         long long fshot, int cnt, int n0,
+__global__ void __launch_bounds__(256, 2) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int nvc,
+                                                         int3 vcs, long long fshot, int cnt, int n0,
                                                          const double2 *__restrict__ wt, int nf,
                                                          double2 *__restrict__ acc) {
     extern __shared__ double2 sw[];  // [cnt][nf]
     for (int q = threadIdx.x; q < cnt * nf; q += blockDim.x) sw[q] = wt[(long long)n0 * nf + q];
     __syncthreads();
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ring_comp;
-         e += (long long)gridDim.x * blockDim.x) {
+    const long long tot = ring_comp * nvc;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < tot; g += (long long)gridDim.x * blockDim.x) {
+        const int vi = (int)(g / ring_comp);
+        const long long e = g - (long long)vi * ring_comp;
+        const int vc = vi == 0 ? vcs.x : (vi == 1 ? vcs.y : vcs.z);
         const long long shot = e / fshot;
         const long long cell = e - shot * fshot;
-        for (int vc = 0; vc < 3; vc++) {
-            if (!(vmask >> vc & 1)) continue;
-            double2 *__restrict__ ap = acc + ((shot * 3 + vc) * nf) * fshot + cell;
-            const T *__restrict__ rp = ring + (long long)vc * ring_comp + e;
-            for (int f0 = 0; f0 < nf; f0 += 8) {
-                const int fn = min(8, nf - f0);
-                double ar[8], ai[8];
+        double2 *__restrict__ ap = acc + ((shot * 3 + vc) * nf) * fshot + cell;
+        const T *__restrict__ rp = ring + (long long)vc * ring_comp + e;
+        for (int f0 = 0; f0 < nf; f0 += 8) {
+            const int fn = min(8, nf - f0);
+            double ar[8], ai[8];
 #pragma unroll
-                for (int f = 0; f < 8; f++) {
-                    if (f < fn) { const double2 v = ap[(long long)(f0 + f) * fshot]; ar[f] = v.x; ai[f] = v.y; }
-                    else { ar[f] = 0.0; ai[f] = 0.0; }
-                }
-                for (int s = 0; s < cnt; s++) {
-                    const double x = (double)__ldg(rp + (long long)s * 3 * ring_comp);
-                    const double2 *w = sw + s * nf + f0;
+            for (int f = 0; f < 8; f++) {
+                if (f < fn) { const double2 v = ap[(long long)(f0 + f) * fshot]; ar[f] = v.x; ai[f] = v.y; }
+                else { ar[f] = 0.0; ai[f] = 0.0; }
+            }
+            for (int s0 = 0; s0 < cnt; s0 += 16) {
+                T xs[16];
 #pragma unroll
-                    for (int f = 0; f < 8; f++) {
-                        if (f < fn) { ar[f] = fma(w[f].x, x, ar[f]); ai[f] = fma(w[f].y, x, ai[f]); }
+                for (int s = 0; s < 16; s++)
+                    xs[s] = (s0 + s < cnt) ? __ldg(rp + (long long)(s0 + s) * 3 * ring_comp) : T(0);
+#pragma unroll
+                for (int s = 0; s < 16; s++) {
+                    if (s0 + s < cnt) {
+                        const double x = (double)xs[s];
+                        const double2 *w = sw + (s0 + s) * nf + f0;
+#pragma unroll
+                        for (int f = 0; f < 8; f++)
+                            if (f < fn) { ar[f] = fma(w[f].x, x, ar[f]); ai[f] = fma(w[f].y, x, ai[f]); }
                     }
                 }
-#pragma unroll
-                for (int f = 0; f < 8; f++)
-                    if (f < fn) ap[(long long)(f0 + f) * fshot] = make_double2(ar[f], ai[f]);
             }
+#pragma unroll
+            for (int f = 0; f < 8; f++)
+                if (f < fn) ap[(long long)(f0 + f) * fshot] = make_double2(ar[f], ai[f]);
         }
     }
 }

@@ -121,7 +121,10 @@ struct mittet_handle_s {
 
     uint32_t vmask = 0;
     int ring_k = 32;
-    int var_e = 1, var_h = 1;  // stencil variants (index into variants<T>())
+    int var_e = 0, var_h = 0;  // stencil variants (index into variants<T>())
+    DevBuf tmaps;              // TileMap per (variant, phase), device copy
+    int tiles[64] = {0};       // tiles per (variant, phase)
+    int tiles_int[64] = {0};   // of which interior
     bool tuned = false;
     DevBuf ring, acc, wtab;
 
@@ -134,6 +137,7 @@ struct mittet_handle_s {
     // cached CUDA graph of G steps
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
+    int64_t graph_launches = 0;
     int graph_key_shots = -1;
     long long graph_key = -1;
 };
@@ -205,6 +209,9 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
     a.c2 = (T)h->ph.c2;
     a.c2t = (T)(h->ph.psi_hyx_typo ? h->ph.c2 : h->ph.c1);
     a.sgn = (T)(e_phase ? h->ph.e_sign : h->ph.h_sign);
+    a.ik[0] = (T)(1.0 / h->g.dx);
+    a.ik[1] = (T)(1.0 / h->g.dy);
+    a.ik[2] = (T)(1.0 / h->g.dz);
     a.d_step = h->d_step.as<int>();
     if (e_phase && h->vmask) {
         a.ring = h->ring.as<T>();
@@ -215,42 +222,162 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
     return a;
 }
 
-// Stencil variants (tile BX x BY, KZ cells per thread) the autotuner picks from.
+// Stencil variants (VX x cells and KZ z cells per thread, BX x BY threads)
+// the autotuner picks from.
 template <typename T>
 struct Variant {
-    int bx, by, kz;
-    void (*e)(PhaseArgs<T>);
-    void (*h)(PhaseArgs<T>);
+    int vx, bx, by, kz;
+    void (*ei)(PhaseArgs<T>, const TileMap *);
+    void (*hi)(PhaseArgs<T>, const TileMap *);
+    void (*es)(PhaseArgs<T>, const TileMap *, int);
+    void (*hs)(PhaseArgs<T>, const TileMap *, int);
 };
 
 template <typename T>
-const std::vector<Variant<T>> &variants() {
-    static const std::vector<Variant<T>> v = {
-#define MITTET_X(a, b, c) {a, b, c, e_phase_kernel<T, a, b, c>, h_phase_kernel<T, a, b, c>},
-        MITTET_STENCIL_VARIANTS(MITTET_X)
+const std::vector<Variant<T>> &variants();
+
+template <>
+const std::vector<Variant<float>> &variants<float>() {
+    static const std::vector<Variant<float>> v = {
+#define MITTET_X(vx, bx, by, kz)                                                                      \
+    {vx, bx, by, kz, e_interior_kernel<float, vx, bx, by, kz>, h_interior_kernel<float, vx, bx, by, kz>, \
+     e_shell_kernel<float, vx, bx, by, kz>, h_shell_kernel<float, vx, bx, by, kz>},
+        MITTET_STENCIL_VARIANTS_F32(MITTET_X)
+#undef MITTET_X
+    };
+    return v;
+}
+template <>
+const std::vector<Variant<double>> &variants<double>() {
+    static const std::vector<Variant<double>> v = {
+#define MITTET_X(vx, bx, by, kz)                                                                        \
+    {vx, bx, by, kz, e_interior_kernel<double, vx, bx, by, kz>, h_interior_kernel<double, vx, bx, by, kz>, \
+     e_shell_kernel<double, vx, bx, by, kz>, h_shell_kernel<double, vx, bx, by, kz>},
+        MITTET_STENCIL_VARIANTS_F64(MITTET_X)
 #undef MITTET_X
     };
     return v;
 }
 
+// Interior box of one phase: per axis, the run of indices around the centre
+// where the general body reduces to the plain update (no CPML profile, no
+// psi slab, inside every component's update range, derivative defined).
+void interior_box(const mittet_handle *h, bool e, int lo[3], int hi[3]) {
+    const Setup &su = h->su;
+    const int n3[3] = {h->g.nx, h->g.ny, h->g.nz};
+    const double d3[3] = {h->g.dx, h->g.dy, h->g.dz};
+    for (int a = 0; a < 3; a++) {
+        const int n = n3[a];
+        const Slab &sl = e ? su.se[a] : su.sh[a];
+        auto ok = [&](int v) {
+            const double sig = prof_at(su, a, e ? P_ESH : P_MSH, v);
+            const double ik = prof_at(su, a, e ? P_IKED : P_IKHD, v);
+            if (sig != 0.0 || ik != 1.0 / d3[a]) return false;
+            if ((v >= sl.nlo && v < sl.nhi) || (v >= sl.flo && v < sl.fhi)) return false;
+            for (int c = 0; c < 3; c++) {
+                const Box &b = su.upd[(e ? 0 : 3) + c];
+                if (v < b.lo[a] || v >= b.hi[a]) return false;
+            }
+            return e ? (v >= 2 && v + 1 < n) : (v >= 1 && v + 2 < n);
+        };
+        const int mid = n / 2;
+        if (!ok(mid)) { lo[a] = hi[a] = 0; continue; }
+        int l = mid, r = mid + 1;
+        while (l - 1 >= 0 && ok(l - 1)) l--;
+        while (r < n && ok(r)) r++;
+        lo[a] = l;
+        hi[a] = r;
+    }
+}
+
+TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int kz) {
+    TileMap t;
+    memset(&t, 0, sizeof(t));
+    const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
+    const int TX = bx * vx;
+    int lo[3], hi[3];
+    interior_box(h, e, lo, hi);
+    int X0 = (lo[0] + vx - 1) / vx * vx;
+    int ntx = hi[0] > X0 ? (hi[0] - X0) / TX : 0;
+    int nty = hi[1] > lo[1] ? (hi[1] - lo[1]) / by : 0;
+    int ntz = hi[2] > lo[2] ? (hi[2] - lo[2]) / kz : 0;
+    auto add = [&](int x0, int y0, int z0, int x1, int y1, int z1, bool full) {
+        if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
+        const int q = t.nbox++;
+        t.lo[q][0] = x0; t.lo[q][1] = y0; t.lo[q][2] = z0;
+        t.hi[q][0] = x1; t.hi[q][1] = y1; t.hi[q][2] = z1;
+        t.ntx[q] = full ? (x1 - x0) / TX : (x1 - x0 + TX - 1) / TX;
+        t.nty[q] = full ? (y1 - y0) / by : (y1 - y0 + by - 1) / by;
+        const int nzt = full ? (z1 - z0) / kz : (z1 - z0 + kz - 1) / kz;
+        t.start[q + 1] = t.start[q] + t.ntx[q] * t.nty[q] * nzt;
+    };
+    if (ntx > 0 && nty > 0 && ntz > 0) {
+        const int X1 = X0 + ntx * TX, Y0 = lo[1], Y1 = lo[1] + nty * by, Z0 = lo[2], Z1 = lo[2] + ntz * kz;
+        t.interior = 1;
+        add(X0, Y0, Z0, X1, Y1, Z1, true);
+        add(0, 0, 0, nx, ny, Z0, false);
+        add(0, 0, Z1, nx, ny, nz, false);
+        add(0, 0, Z0, nx, Y0, Z1, false);
+        add(0, Y1, Z0, nx, ny, Z1, false);
+        add(0, Y0, Z0, X0, Y1, Z1, false);
+        add(X1, Y0, Z0, nx, Y1, Z1, false);
+    } else {
+        add(0, 0, 0, nx, ny, nz, false);
+    }
+    return t;
+}
+
 template <typename T>
-void launch_phase(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a) {
+int upload_tilemaps(mittet_handle *h) {
+    const auto &vs = variants<T>();
+    std::vector<TileMap> maps(2 * vs.size());
+    for (size_t v = 0; v < vs.size(); v++) {
+        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].kz);
+        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].kz);
+        for (int p = 0; p < 2; p++) {
+            const TileMap &t = maps[2 * v + p];
+            h->tiles[2 * v + p] = t.start[t.nbox];
+            h->tiles_int[2 * v + p] = t.interior ? t.start[1] : 0;
+        }
+    }
+    CK(h->tmaps.ensure(maps.size() * sizeof(TileMap)));
+    CK(cudaMemcpy(h->tmaps.p, maps.data(), maps.size() * sizeof(TileMap), cudaMemcpyHostToDevice));
+    return MITTET_OK;
+}
+
+// One phase = the interior kernel over the interior tiles, then the shell
+// kernel over the rest (two launches; the first is skipped on grids too
+// small to have an interior).  Returns the number of launches.
+template <typename T>
+int launch_phase(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a) {
     const Variant<T> &v = variants<T>()[vi];
-    dim3 grid((h->g.nx + v.bx - 1) / v.bx, (h->g.ny + v.by - 1) / v.by, h->nshot * ((h->g.nz + v.kz - 1) / v.kz));
+    const int slot = 2 * vi + (e ? 0 : 1);
+    const TileMap *tm = h->tmaps.as<TileMap>() + slot;
+    const int n_int = h->tiles_int[slot], n_all = h->tiles[slot];
     dim3 block(v.bx, v.by);
-    if (e) v.e<<<grid, block, 0, h->st>>>(a);
-    else v.h<<<grid, block, 0, h->st>>>(a);
+    int n = 0;
+    if (n_int > 0) {
+        dim3 grid(n_int, h->nshot);
+        if (e) v.ei<<<grid, block, 0, h->st>>>(a, tm);
+        else v.hi<<<grid, block, 0, h->st>>>(a, tm);
+        n++;
+    }
+    if (n_all > n_int) {
+        dim3 grid(n_all - n_int, h->nshot);
+        if (e) v.es<<<grid, block, 0, h->st>>>(a, tm, n_int);
+        else v.hs<<<grid, block, 0, h->st>>>(a, tm, n_int);
+        n++;
+    }
+    return n;
 }
 
 template <typename T>
 void launch_step(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha, const InjectArgs<T> &ia_m,
                  const InjectArgs<T> &ia_e, const SampleArgs<T> &sa) {
     if (h->has_mag) { inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m); h->launches++; }
-    launch_phase<T>(h, true, h->var_e, ea);
-    h->launches++;
+    h->launches += launch_phase<T>(h, true, h->var_e, ea);
     if (h->has_ele) { inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e); h->launches++; }
-    launch_phase<T>(h, false, h->var_h, ha);
-    h->launches++;
+    h->launches += launch_phase<T>(h, false, h->var_h, ha);
     sample_kernel<T><<<1, 1024, 0, h->st>>>(sa);
     h->launches++;
 }
@@ -299,8 +426,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             float ms = 0;
             CK(cudaEventElapsedTime(&ms, e0, e1));
             if (std::getenv("MITTET_TUNE_LOG"))
-                fprintf(stderr, "autotune %s %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", variants<T>()[v].bx,
-                        variants<T>()[v].by, variants<T>()[v].kz, ms / reps);
+                fprintf(stderr, "autotune %s vx%d %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", variants<T>()[v].vx,
+                        variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].kz, ms / reps);
             if (ms < best[ph]) {
                 best[ph] = ms;
                 (ph == 0 ? h->var_e : h->var_h) = v;
@@ -318,9 +445,13 @@ template <typename T>
 void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
     const long long tot = (long long)h->nshot * h->fshot;
     const int nf = (int)h->omega.size();
-    int blocks = (int)std::min<long long>((tot + 255) / 256, 148LL * 8);
+    int vc[3] = {0, 0, 0}, nvc = 0;
+    for (int c = 0; c < 3; c++)
+        if (h->vmask >> c & 1) vc[nvc++] = c;
+    int blocks = (int)std::min<long long>((tot * nvc + 255) / 256, 148LL * 16);
     volume_dft_kernel<T><<<blocks, 256, (size_t)cnt * nf * sizeof(double2), h->st>>>(
-        h->ring.as<T>(), tot, (int)h->vmask, h->fshot, cnt, n0, h->wtab.as<double2>(), nf, h->acc.as<double2>());
+        h->ring.as<T>(), tot, nvc, make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, n0, h->wtab.as<double2>(), nf,
+        h->acc.as<double2>());
     h->launches++;
 }
 
@@ -402,7 +533,9 @@ int run_forward(mittet_handle *h, int nt) {
         drop_graph(h);
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        h->launches = 0;
         for (int s = 0; s < G; s++) launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+        h->graph_launches = h->launches;
         cudaError_t ec = cudaStreamEndCapture(h->st, &graph);
         if (ec != cudaSuccess) return fail(MITTET_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
         ec = cudaGraphInstantiate(&h->gexec, graph, 0);
@@ -412,11 +545,10 @@ int run_forward(mittet_handle *h, int nt) {
         h->graph_steps = G;
     }
     h->launches = 0;
-    const long long per_step = (h->has_mag ? 1 : 0) + (h->has_ele ? 1 : 0) + 3;
     int done = 0;
     while (done + G <= nt) {
         CK(cudaGraphLaunch(h->gexec, h->st));
-        h->launches += per_step * G;
+        h->launches += h->graph_launches;
         if (vol) launch_volume_flush<T>(h, G, done);
         done += G;
     }
@@ -676,6 +808,11 @@ int mittet_create(const mittet_grid *g, const mittet_phys *ph, mittet_handle **o
     h->px = (g->nx + 31) / 32 * 32;
     h->plane = (long long)h->px * g->ny;
     h->fshot = h->plane * g->nz;
+    if (h->fshot >= (1LL << 31) - 64) {
+        const long long cells = h->fshot;
+        delete h;
+        return fail(MITTET_ERR_INVALID_ARG, "grid of %lld padded cells exceeds the 2^31 per-shot limit", cells);
+    }
     CpmlConst cc{ph->cpml_nn, ph->cpml_order, ph->cpml_kappa_max, ph->cpml_a_max, ph->cpml_ma, ph->cpml_rcoef,
                  ph->cpml_opt_to_max_x};
     build_setup(ph->flavor, g->nx, g->ny, g->nz, g->dx, g->dy, g->dz, g->ncpml, ph->cmax, ph->dt, cc, h->su);
@@ -706,6 +843,12 @@ int mittet_create(const mittet_grid *g, const mittet_phys *ph, mittet_handle **o
         delete h;
         return fail(e == cudaErrorMemoryAllocation ? MITTET_ERR_OOM : MITTET_ERR_CUDA, "profile upload: %s",
                     cudaGetErrorString(e));
+    }
+    int rc2 = h->fp64 ? upload_tilemaps<double>(h) : upload_tilemaps<float>(h);
+    if (rc2) {
+        cudaStreamDestroy(h->st);
+        delete h;
+        return rc2;
     }
     *out = h;
     return MITTET_OK;
@@ -1027,15 +1170,13 @@ int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1
 
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg) {
     if (!h || !e_cfg || !h_cfg) return fail(MITTET_ERR_INVALID_ARG, "null argument");
-    if (h->fp64) {
-        const auto &v = variants<double>();
-        e_cfg[0] = v[h->var_e].bx; e_cfg[1] = v[h->var_e].by; e_cfg[2] = v[h->var_e].kz;
-        h_cfg[0] = v[h->var_h].bx; h_cfg[1] = v[h->var_h].by; h_cfg[2] = v[h->var_h].kz;
-    } else {
-        const auto &v = variants<float>();
-        e_cfg[0] = v[h->var_e].bx; e_cfg[1] = v[h->var_e].by; e_cfg[2] = v[h->var_e].kz;
-        h_cfg[0] = v[h->var_h].bx; h_cfg[1] = v[h->var_h].by; h_cfg[2] = v[h->var_h].kz;
-    }
+    auto fill = [&](auto &v) {
+        const auto &a = v[h->var_e], &b = v[h->var_h];
+        e_cfg[0] = a.vx; e_cfg[1] = a.bx; e_cfg[2] = a.by; e_cfg[3] = a.kz;
+        h_cfg[0] = b.vx; h_cfg[1] = b.bx; h_cfg[2] = b.by; h_cfg[3] = b.kz;
+    };
+    if (h->fp64) fill(variants<double>());
+    else fill(variants<float>());
     return MITTET_OK;
 }
 

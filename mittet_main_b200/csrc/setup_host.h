@@ -206,7 +206,8 @@ inline bool ranges_in_bounds(const Setup &s) {
 inline void build_setup(int flavor, int nx, int ny, int nz, double dx, double dy, double dz, int ncpml,
                         double cmax, double dt, const CpmlConst &cc, Setup &s) {
     s.nx = nx; s.ny = ny; s.nz = nz;
-    s.nmax = std::max(nx, std::max(ny, nz));
+    // profile row stride, a multiple of 4 so x profiles load as aligned vectors
+    s.nmax = (std::max(nx, std::max(ny, nz)) + 3) / 4 * 4;
     s.prof.assign((size_t)3 * P_COUNT * s.nmax, 0.0);
     const int n3[3] = {nx, ny, nz};
     const double d3[3] = {dx, dy, dz};

@@ -1,13 +1,23 @@
 // stencil.cuh -- the two half-step kernels of the (2,4) Yee + CPML update.
 //
-// Thread mapping: a BX x BY block covers an (x, y) tile; each thread owns KZ
-// consecutive cells of one (i, j) column.  All reads of a thread are issued
-// before its first store (every pointer is __restrict__, fields read in a
-// phase are never written in it, reads go through the read-only path), so a
-// warp keeps ~20-30 independent loads in flight: the kernels are bandwidth
-// kernels and live on memory-level parallelism.  The z-neighbours of the two
-// fields differentiated along z are loaded once per thread (KZ+3 planes) and
-// reused from registers.
+// Work decomposition.  The grid of one phase is split on the host into an
+// interior box (no CPML profile, no psi slab, every component inside its
+// update range, every derivative defined) cut into whole tiles, plus up to
+// six shell boxes around it.  One launch covers all of them: blockIdx.x
+// enumerates the tiles of box 0, then box 1, ... (TileMap, in global
+// memory), blockIdx.y is the shot.  Interior tiles run a straight-line body
+// with no per-cell tests; shell tiles run the general body that restates the
+// reference's index ranges, CPML profiles and psi recurrences.  Both bodies
+// use the same explicit fma forms, so a cell gets bit-identical results
+// whichever body computes it.
+//
+// Thread mapping: a BX x BY block covers one tile in (x, y); each thread owns
+// VX consecutive x cells (one aligned float2/float4/double2 per field and
+// plane) of KZ consecutive z planes.  x neighbours come from the aligned
+// vectors at i0-VX, i0, i0+VX; y and z neighbours are whole vectors.  All
+// loads of a thread are issued before its first store (every pointer is
+// __restrict__, fields read in a phase are never written in it), so a warp
+// keeps ~20 independent 8-16 byte loads in flight.
 //
 // E half step (ncver0027/cpu_eh_field_cpml42.f90:114-158, cpu_cpml4.f90:271-361):
 //   Ex = ca_x Ex + s cb_x (Dy(Hz)/kedy - Dz(Hy)/kedz),  cyclic for Ey, Ez,
@@ -22,16 +32,79 @@
 
 namespace mittet {
 
-template <typename T, int BX, int BY, int KZ>
-__global__ void __launch_bounds__(BX *BY, ((KZ == 1 && sizeof(T) == 4) ? 1024 / (BX * BY) : 512 / (BX * BY)))
-    e_phase_kernel(const PhaseArgs<T> a) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    const int nzc = (a.nz + KZ - 1) / KZ;
-    const int shot = blockIdx.z / nzc;
-    const int kb = (blockIdx.z - shot * nzc) * KZ;
-    if (i >= a.nx || j >= a.ny) return;
+// Boxes of one phase, in the order their tiles are enumerated by blockIdx.x.
+struct TileMap {
+    int nbox;        // boxes in use (<= 7)
+    int interior;    // 1: box 0 is the interior fast-path box
+    int start[8];    // first tile of each box; start[nbox] = tiles in total
+    int lo[7][3], hi[7][3];
+    int ntx[7], nty[7];
+};
 
+template <typename T, int VX>
+struct VecT;
+template <> struct VecT<float, 2> { using type = float2; };
+template <> struct VecT<float, 4> { using type = float4; };
+template <> struct VecT<double, 2> { using type = double2; };
+
+template <typename T, int VX>
+__device__ __forceinline__ void ldv(T (&dst)[VX], const T *__restrict__ p) {
+    using V = typename VecT<T, VX>::type;
+    const V v = __ldg(reinterpret_cast<const V *>(p));
+    const T *s = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int q = 0; q < VX; q++) dst[q] = s[q];
+}
+template <typename T, int VX>
+__device__ __forceinline__ void ldv_rw(T (&dst)[VX], const T *__restrict__ p) {
+    using V = typename VecT<T, VX>::type;
+    const V v = *reinterpret_cast<const V *>(p);
+    const T *s = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int q = 0; q < VX; q++) dst[q] = s[q];
+}
+template <typename T, int VX>
+__device__ __forceinline__ void stv(T *__restrict__ p, const T (&src)[VX]) {
+    using V = typename VecT<T, VX>::type;
+    V v;
+    T *d = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int q = 0; q < VX; q++) d[q] = src[q];
+    *reinterpret_cast<V *>(p) = v;
+}
+template <typename T, int VX>
+__device__ __forceinline__ void zerov(T (&d)[VX]) {
+#pragma unroll
+    for (int q = 0; q < VX; q++) d[q] = T(0);
+}
+
+template <int VX>
+__device__ __forceinline__ unsigned xmask(int i0, int lo, int hi) {
+    unsigned m = 0;
+#pragma unroll
+    for (int v = 0; v < VX; v++) m |= (unsigned)(i0 + v >= lo && i0 + v < hi) << v;
+    return m;
+}
+
+// Explicit fma forms shared by both bodies.
+template <typename T>
+__device__ __forceinline__ T d4(T c1, T c2, T a, T b, T c, T d) {  // c1 (a-b) + c2 (c-d)
+    return fma(c1, a - b, c2 * (c - d));
+}
+template <typename T>
+__device__ __forceinline__ T curl2(T a, T ia, T b, T ib) {  // a ia - b ib
+    return fma(a, ia, -(b * ib));
+}
+template <typename T>
+__device__ __forceinline__ T leap(T ca, T sgcb, T x, T e) {  // ca e + (s cb) x
+    return fma(sgcb, x, ca * e);
+}
+
+#define MITTET_MINB(T, VX, KZ, NT) ((sizeof(T) == 4 && VX == 2 && KZ == 1) ? 768 / (NT) : 512 / (NT))
+
+// ------------------------------------------------------------------ E phase
+template <typename T, int VX, int KZ, bool INT>
+__device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int khi) {
     const long long sb = (long long)shot * a.fshot;
     T *__restrict__ Ex = a.f[0] + sb;
     T *__restrict__ Ey = a.f[1] + sb;
@@ -41,130 +114,210 @@ __global__ void __launch_bounds__(BX *BY, ((KZ == 1 && sizeof(T) == 4) ? 1024 / 
     const T *__restrict__ Hz = a.f[5] + sb;
     const T *__restrict__ M = a.m;
     const T *__restrict__ P = a.prof;
-    const long long py = a.px, pz = a.plane;
-    const int nz = a.nz, nmax = a.nmax;
-    const T c1 = a.c1, c2 = a.c2;
+    const int py = a.px, pz = (int)a.plane, nx = a.nx, ny = a.ny, nz = a.nz, ps = a.nmax;
+    const T c1 = a.c1, c2 = a.c2, sg = a.sgn;
 
-    const T esh_x = __ldg(P + 0 * nmax + i), ik_x = __ldg(P + 6 * nmax + i);
-    const T esh_y = __ldg(P + 8 * nmax + 0 * nmax + j), ik_y = __ldg(P + 8 * nmax + 6 * nmax + j);
-    const bool vx = (i >= 2) && (i + 1 < a.nx);
-    const bool vy = (j >= 2) && (j + 1 < a.ny);
-    const int lx = slab_local(a.slab[0], i);
-    const int ly = slab_local(a.slab[1], j);
-    const bool sx_col = lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1];
-    const bool sy_col = ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0];
-    const bool sz_col = i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
-                        j < a.slab[2].other.hi[1];
-    const long long col = (long long)j * py + i;
+    T esh_x[VX], ik_x[VX];
+    T esh_y, ik_y;
+    bool vy, has_l, has_r;
+    unsigned vxm, ux, uy, uz, sxm, sym, szm;
+    int ly;
+    DSlab S0, S1, S2;
+    if constexpr (INT) {
+#pragma unroll
+        for (int v = 0; v < VX; v++) { esh_x[v] = T(0); ik_x[v] = a.ik[0]; }
+        esh_y = T(0);
+        ik_y = a.ik[1];
+        vy = has_l = has_r = true;
+        vxm = ux = uy = uz = (1u << VX) - 1u;
+        sxm = sym = szm = 0u;
+        ly = -1;
+    } else {
+        ldv<T, VX>(esh_x, P + 0 * ps + i0);
+        ldv<T, VX>(ik_x, P + 6 * ps + i0);
+        esh_y = __ldg(P + 8 * ps + j);
+        ik_y = __ldg(P + 14 * ps + j);
+        vy = (j >= 2) && (j + 1 < ny);
+        has_l = i0 >= VX;
+        has_r = i0 + VX < nx;
+        vxm = 0;
+#pragma unroll
+        for (int v = 0; v < VX; v++) vxm |= (unsigned)(i0 + v >= 2 && i0 + v + 1 < nx) << v;
+        const DBox U0 = a.upd[0], U1 = a.upd[1], U2 = a.upd[2];
+        ux = (j >= U0.lo[1] && j < U0.hi[1]) ? xmask<VX>(i0, U0.lo[0], U0.hi[0]) : 0u;
+        uy = (j >= U1.lo[1] && j < U1.hi[1]) ? xmask<VX>(i0, U1.lo[0], U1.hi[0]) : 0u;
+        uz = (j >= U2.lo[1] && j < U2.hi[1]) ? xmask<VX>(i0, U2.lo[0], U2.hi[0]) : 0u;
+        S0 = a.slab[0];
+        S1 = a.slab[1];
+        S2 = a.slab[2];
+        sxm = 0;
+#pragma unroll
+        for (int v = 0; v < VX; v++) sxm |= (unsigned)(slab_local(S0, i0 + v) >= 0) << v;
+        sxm = (j >= S0.other.lo[1] && j < S0.other.hi[1]) ? sxm : 0u;
+        ly = slab_local(S1, j);
+        sym = ly >= 0 ? xmask<VX>(i0, S1.other.lo[0], S1.other.hi[0]) : 0u;
+        szm = (j >= S2.other.lo[1] && j < S2.other.hi[1]) ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : 0u;
+    }
+    const int col = j * py + i0;
 
     // z window: planes kb-2 .. kb+KZ of Hx and Hy
-    T wx[KZ + 3], wy[KZ + 3];
+    T wx[KZ + 3][VX], wy[KZ + 3][VX];
 #pragma unroll
     for (int q = 0; q < KZ + 3; q++) {
         const int kk = kb - 2 + q;
-        const bool ok = kk >= 0 && kk < nz;
-        wx[q] = ok ? __ldg(Hx + kk * pz + col) : T(0);
-        wy[q] = ok ? __ldg(Hy + kk * pz + col) : T(0);
+        if (INT || (kk >= 0 && kk < nz)) {
+            ldv<T, VX>(wx[q], Hx + kk * pz + col);
+            ldv<T, VX>(wy[q], Hy + kk * pz + col);
+        } else {
+            zerov<T, VX>(wx[q]);
+            zerov<T, VX>(wy[q]);
+        }
     }
     const int slot = a.ring_k > 0 ? (*a.d_step) % a.ring_k : 0;
 
 #pragma unroll
     for (int q = 0; q < KZ; q++) {
         const int k = kb + q;
-        if (k >= nz) break;
-        const long long c = k * pz + col;
-        const bool vz = (k >= 2) && (k + 1 < nz);
-        const T hz = __ldg(Hz + c);
-        T dyHz = T(0), dxHz = T(0), dxHy = T(0), dyHx = T(0), dzHy = T(0), dzHx = T(0);
-        if (vy) {
-            const T a0 = __ldg(Hz + c - py), a1 = __ldg(Hz + c + py), a2 = __ldg(Hz + c - 2 * py);
-            const T b0 = __ldg(Hx + c - py), b1 = __ldg(Hx + c + py), b2 = __ldg(Hx + c - 2 * py);
-            dyHz = c1 * (hz - a0) + c2 * (a1 - a2);
-            dyHx = c1 * (wx[q + 2] - b0) + c2 * (b1 - b2);
-        }
-        if (vx) {
-            const T a0 = __ldg(Hz + c - 1), a1 = __ldg(Hz + c + 1), a2 = __ldg(Hz + c - 2);
-            const T b0 = __ldg(Hy + c - 1), b1 = __ldg(Hy + c + 1), b2 = __ldg(Hy + c - 2);
-            dxHz = c1 * (hz - a0) + c2 * (a1 - a2);
-            dxHy = c1 * (wy[q + 2] - b0) + c2 * (b1 - b2);
-        }
-        if (vz) {
-            dzHy = c1 * (wy[q + 2] - wy[q + 1]) + c2 * (wy[q + 3] - wy[q]);
-            dzHx = c1 * (wx[q + 2] - wx[q + 1]) + c2 * (wx[q + 3] - wx[q]);
-        }
-        const T m = __ldg(M + c);
-        const T esh_z = __ldg(P + 16 * nmax + k), ik_z = __ldg(P + 16 * nmax + 6 * nmax + k);
-        T ex = Ex[c], ey = Ey[c], ez = Ez[c];
-
-        T ca_x = T(1), cb_x = m, ca_y = T(1), cb_y = m, ca_z = T(1), cb_z = m;
-        if (esh_x != T(0)) { const T h = esh_x * m; const T r = rcp(T(1) + h); ca_x = (T(1) - h) * r; cb_x = m * r; }
-        if (esh_y != T(0)) { const T h = esh_y * m; const T r = rcp(T(1) + h); ca_y = (T(1) - h) * r; cb_y = m * r; }
-        if (esh_z != T(0)) { const T h = esh_z * m; const T r = rcp(T(1) + h); ca_z = (T(1) - h) * r; cb_z = m * r; }
-        if (in_box(a.upd[0], i, j, k)) ex = ca_x * ex + a.sgn * cb_x * (dyHz * ik_y - dzHy * ik_z);
-        if (in_box(a.upd[1], i, j, k)) ey = ca_y * ey + a.sgn * cb_y * (dzHx * ik_z - dxHz * ik_x);
-        if (in_box(a.upd[2], i, j, k)) ez = ca_z * ez + a.sgn * cb_z * (dxHy * ik_x - dyHx * ik_y);
-
-        if (sx_col && k >= a.slab[0].other.lo[2] && k < a.slab[0].other.hi[2]) {
-            T *__restrict__ q0 = a.psi[0][0];
-            T *__restrict__ q1 = a.psi[0][1];
-            const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
-            const T be = __ldg(P + 2 * nmax + i), ced = __ldg(P + 3 * nmax + i);
-            const T p0 = be * q0[o] + ced * dxHy;  // psi_Ezx
-            const T p1 = be * q1[o] + ced * dxHz;  // psi_Eyx
-            q0[o] = p0;
-            q1[o] = p1;
-            ez = ez + cb_z * p0;
-            ey = ey - cb_y * p1;
-        }
-        if (sy_col && k >= a.slab[1].other.lo[2] && k < a.slab[1].other.hi[2]) {
-            T *__restrict__ q0 = a.psi[1][0];
-            T *__restrict__ q1 = a.psi[1][1];
-            const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
-            const T be = __ldg(P + 8 * nmax + 2 * nmax + j), ced = __ldg(P + 8 * nmax + 3 * nmax + j);
-            const T p0 = be * q0[o] + ced * dyHz;  // psi_Exy
-            const T p1 = be * q1[o] + ced * dyHx;  // psi_Ezy
-            q0[o] = p0;
-            q1[o] = p1;
-            ex = ex + cb_x * p0;
-            ez = ez - cb_z * p1;
-        }
-        if (sz_col) {
-            const int lz = slab_local(a.slab[2], k);
-            if (lz >= 0) {
-                T *__restrict__ q0 = a.psi[2][0];
-                T *__restrict__ q1 = a.psi[2][1];
-                const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
-                const T be = __ldg(P + 16 * nmax + 2 * nmax + k), ced = __ldg(P + 16 * nmax + 3 * nmax + k);
-                const T p0 = be * q0[o] + ced * dzHx;  // psi_Eyz
-                const T p1 = be * q1[o] + ced * dzHy;  // psi_Exz
-                q0[o] = p0;
-                q1[o] = p1;
-                ey = ey + cb_y * p0;
-                ex = ex - cb_x * p1;
+        if (!INT && k >= khi) break;
+        const int c = k * pz + col;
+        T hzx[3 * VX], hyx[3 * VX];
+        {
+            T t[VX];
+            ldv<T, VX>(t, Hz + c);
+#pragma unroll
+            for (int v = 0; v < VX; v++) { hzx[VX + v] = t[v]; hyx[VX + v] = wy[q + 2][v]; }
+            if (has_l) {
+                ldv<T, VX>(t, Hz + c - VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) hzx[v] = t[v];
+                ldv<T, VX>(t, Hy + c - VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) hyx[v] = t[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < VX; v++) { hzx[v] = T(0); hyx[v] = T(0); }
+            }
+            if (has_r) {
+                ldv<T, VX>(t, Hz + c + VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) hzx[2 * VX + v] = t[v];
+                ldv<T, VX>(t, Hy + c + VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) hyx[2 * VX + v] = t[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < VX; v++) { hzx[2 * VX + v] = T(0); hyx[2 * VX + v] = T(0); }
             }
         }
-        Ex[c] = ex;
-        Ey[c] = ey;
-        Ez[c] = ez;
+        T hzm2[VX], hzm1[VX], hzp1[VX], hxm2[VX], hxm1[VX], hxp1[VX];
+        if (vy) {
+            ldv<T, VX>(hzm2, Hz + c - 2 * py);
+            ldv<T, VX>(hzm1, Hz + c - py);
+            ldv<T, VX>(hzp1, Hz + c + py);
+            ldv<T, VX>(hxm2, Hx + c - 2 * py);
+            ldv<T, VX>(hxm1, Hx + c - py);
+            ldv<T, VX>(hxp1, Hx + c + py);
+        } else {
+            zerov<T, VX>(hzm2); zerov<T, VX>(hzm1); zerov<T, VX>(hzp1);
+            zerov<T, VX>(hxm2); zerov<T, VX>(hxm1); zerov<T, VX>(hxp1);
+        }
+        T m[VX], ex[VX], ey[VX], ez[VX];
+        ldv<T, VX>(m, M + c);
+        ldv_rw<T, VX>(ex, Ex + c);
+        ldv_rw<T, VX>(ey, Ey + c);
+        ldv_rw<T, VX>(ez, Ez + c);
+        T esh_z, ik_z;
+        bool vz, kx, ky, kz;
+        int lz;
+        if constexpr (INT) {
+            esh_z = T(0);
+            ik_z = a.ik[2];
+            vz = kx = ky = kz = true;
+            lz = -1;
+        } else {
+            esh_z = __ldg(P + 16 * ps + k);
+            ik_z = __ldg(P + 22 * ps + k);
+            vz = (k >= 2) && (k + 1 < nz);
+            kx = k >= a.upd[0].lo[2] && k < a.upd[0].hi[2];
+            ky = k >= a.upd[1].lo[2] && k < a.upd[1].hi[2];
+            kz = k >= a.upd[2].lo[2] && k < a.upd[2].hi[2];
+            lz = slab_local(S2, k);
+        }
+
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            const bool vx = vxm >> v & 1;
+            const T dyHz = vy ? d4(c1, c2, hzx[VX + v], hzm1[v], hzp1[v], hzm2[v]) : T(0);
+            const T dyHx = vy ? d4(c1, c2, wx[q + 2][v], hxm1[v], hxp1[v], hxm2[v]) : T(0);
+            const T dxHz = vx ? d4(c1, c2, hzx[VX + v], hzx[VX + v - 1], hzx[VX + v + 1], hzx[VX + v - 2]) : T(0);
+            const T dxHy = vx ? d4(c1, c2, hyx[VX + v], hyx[VX + v - 1], hyx[VX + v + 1], hyx[VX + v - 2]) : T(0);
+            const T dzHy = vz ? d4(c1, c2, wy[q + 2][v], wy[q + 1][v], wy[q + 3][v], wy[q][v]) : T(0);
+            const T dzHx = vz ? d4(c1, c2, wx[q + 2][v], wx[q + 1][v], wx[q + 3][v], wx[q][v]) : T(0);
+            const T mv = m[v];
+            T ca_x = T(1), cb_x = mv, ca_y = T(1), cb_y = mv, ca_z = T(1), cb_z = mv;
+            if (!INT) {
+                if (esh_x[v] != T(0)) { const T h = esh_x[v] * mv; const T r = rcp(T(1) + h); ca_x = (T(1) - h) * r; cb_x = mv * r; }
+                if (esh_y != T(0)) { const T h = esh_y * mv; const T r = rcp(T(1) + h); ca_y = (T(1) - h) * r; cb_y = mv * r; }
+                if (esh_z != T(0)) { const T h = esh_z * mv; const T r = rcp(T(1) + h); ca_z = (T(1) - h) * r; cb_z = mv * r; }
+            }
+            if (kx && (ux >> v & 1)) ex[v] = leap(ca_x, sg * cb_x, curl2(dyHz, ik_y, dzHy, ik_z), ex[v]);
+            if (ky && (uy >> v & 1)) ey[v] = leap(ca_y, sg * cb_y, curl2(dzHx, ik_z, dxHz, ik_x[v]), ey[v]);
+            if (kz && (uz >> v & 1)) ez[v] = leap(ca_z, sg * cb_z, curl2(dxHy, ik_x[v], dyHx, ik_y), ez[v]);
+
+            if (!INT) {
+                if ((sxm >> v & 1) && k >= S0.other.lo[2] && k < S0.other.hi[2]) {
+                    T *__restrict__ q0 = a.psi[0][0] + shot * a.pshot[0];
+                    T *__restrict__ q1 = a.psi[0][1] + shot * a.pshot[0];
+                    const int o = (k * ny + j) * S0.width + slab_local(S0, i0 + v);
+                    const T be = __ldg(P + 2 * ps + i0 + v), ced = __ldg(P + 3 * ps + i0 + v);
+                    const T p0 = fma(be, q0[o], ced * dxHy);  // psi_Ezx
+                    const T p1 = fma(be, q1[o], ced * dxHz);  // psi_Eyx
+                    q0[o] = p0;
+                    q1[o] = p1;
+                    ez[v] = fma(cb_z, p0, ez[v]);
+                    ey[v] = fma(-cb_y, p1, ey[v]);
+                }
+                if ((sym >> v & 1) && k >= S1.other.lo[2] && k < S1.other.hi[2]) {
+                    T *__restrict__ q0 = a.psi[1][0] + shot * a.pshot[1];
+                    T *__restrict__ q1 = a.psi[1][1] + shot * a.pshot[1];
+                    const int o = (k * S1.width + ly) * py + i0 + v;
+                    const T be = __ldg(P + 10 * ps + j), ced = __ldg(P + 11 * ps + j);
+                    const T p0 = fma(be, q0[o], ced * dyHz);  // psi_Exy
+                    const T p1 = fma(be, q1[o], ced * dyHx);  // psi_Ezy
+                    q0[o] = p0;
+                    q1[o] = p1;
+                    ex[v] = fma(cb_x, p0, ex[v]);
+                    ez[v] = fma(-cb_z, p1, ez[v]);
+                }
+                if ((szm >> v & 1) && lz >= 0) {
+                    T *__restrict__ q0 = a.psi[2][0] + shot * a.pshot[2];
+                    T *__restrict__ q1 = a.psi[2][1] + shot * a.pshot[2];
+                    const int o = (lz * ny + j) * py + i0 + v;
+                    const T be = __ldg(P + 18 * ps + k), ced = __ldg(P + 19 * ps + k);
+                    const T p0 = fma(be, q0[o], ced * dzHx);  // psi_Eyz
+                    const T p1 = fma(be, q1[o], ced * dzHy);  // psi_Exz
+                    q0[o] = p0;
+                    q1[o] = p1;
+                    ey[v] = fma(cb_y, p0, ey[v]);
+                    ex[v] = fma(-cb_x, p1, ex[v]);
+                }
+            }
+        }
+        stv<T, VX>(Ex + c, ex);
+        stv<T, VX>(Ey + c, ey);
+        stv<T, VX>(Ez + c, ez);
         if (a.ring_k > 0) {
             T *__restrict__ r = a.ring + (long long)slot * 3 * a.ring_comp + sb + c;
-            if (a.vmask & 1) r[0] = ex;
-            if (a.vmask & 2) r[a.ring_comp] = ey;
-            if (a.vmask & 4) r[2 * a.ring_comp] = ez;
+            if (a.vmask & 1) stv<T, VX>(r, ex);
+            if (a.vmask & 2) stv<T, VX>(r + a.ring_comp, ey);
+            if (a.vmask & 4) stv<T, VX>(r + 2 * a.ring_comp, ez);
         }
     }
 }
 
-template <typename T, int BX, int BY, int KZ>
-__global__ void __launch_bounds__(BX *BY, ((KZ == 1 && sizeof(T) == 4) ? 1024 / (BX * BY) : 512 / (BX * BY)))
-    h_phase_kernel(const PhaseArgs<T> a) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    const int nzc = (a.nz + KZ - 1) / KZ;
-    const int shot = blockIdx.z / nzc;
-    const int kb = (blockIdx.z - shot * nzc) * KZ;
-    if (i >= a.nx || j >= a.ny) return;
-
+// ------------------------------------------------------------------ H phase
+template <typename T, int VX, int KZ, bool INT>
+__device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int khi) {
     const long long sb = (long long)shot * a.fshot;
     const T *__restrict__ Ex = a.f[0] + sb;
     const T *__restrict__ Ey = a.f[1] + sb;
@@ -175,125 +328,281 @@ __global__ void __launch_bounds__(BX *BY, ((KZ == 1 && sizeof(T) == 4) ? 1024 / 
     const T *__restrict__ M = a.m;
     const T *__restrict__ DM = a.dtmu;
     const T *__restrict__ P = a.prof;
-    const long long py = a.px, pz = a.plane;
-    const int nz = a.nz, nmax = a.nmax;
-    const T c1 = a.c1, c2 = a.c2, c2t = a.c2t;
+    const int py = a.px, pz = (int)a.plane, nx = a.nx, ny = a.ny, nz = a.nz, ps = a.nmax;
+    const T c1 = a.c1, c2 = a.c2, c2t = a.c2t, sg = a.sgn;
 
-    const T msh_x = __ldg(P + 1 * nmax + i), ik_x = __ldg(P + 7 * nmax + i);
-    const T msh_y = __ldg(P + 8 * nmax + 1 * nmax + j), ik_y = __ldg(P + 8 * nmax + 7 * nmax + j);
-    const bool vx = (i >= 1) && (i + 2 < a.nx);
-    const bool vy = (j >= 1) && (j + 2 < a.ny);
-    const int lx = slab_local(a.slab[0], i);
-    const int ly = slab_local(a.slab[1], j);
-    const bool sx_col = lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1];
-    const bool sy_col = ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0];
-    const bool sz_col = i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
-                        j < a.slab[2].other.hi[1];
-    const long long col = (long long)j * py + i;
+    T msh_x[VX], ik_x[VX];
+    T msh_y, ik_y;
+    bool vy, has_l, has_r;
+    unsigned vxm, ux, uy, uz, sxm, sym, szm;
+    int ly;
+    DSlab S0, S1, S2;
+    if constexpr (INT) {
+#pragma unroll
+        for (int v = 0; v < VX; v++) { msh_x[v] = T(0); ik_x[v] = a.ik[0]; }
+        msh_y = T(0);
+        ik_y = a.ik[1];
+        vy = has_l = has_r = true;
+        vxm = ux = uy = uz = (1u << VX) - 1u;
+        sxm = sym = szm = 0u;
+        ly = -1;
+    } else {
+        ldv<T, VX>(msh_x, P + 1 * ps + i0);
+        ldv<T, VX>(ik_x, P + 7 * ps + i0);
+        msh_y = __ldg(P + 9 * ps + j);
+        ik_y = __ldg(P + 15 * ps + j);
+        vy = (j >= 1) && (j + 2 < ny);
+        has_l = i0 >= VX;
+        has_r = i0 + VX < nx;
+        vxm = 0;
+#pragma unroll
+        for (int v = 0; v < VX; v++) vxm |= (unsigned)(i0 + v >= 1 && i0 + v + 2 < nx) << v;
+        const DBox U0 = a.upd[0], U1 = a.upd[1], U2 = a.upd[2];
+        ux = (j >= U0.lo[1] && j < U0.hi[1]) ? xmask<VX>(i0, U0.lo[0], U0.hi[0]) : 0u;
+        uy = (j >= U1.lo[1] && j < U1.hi[1]) ? xmask<VX>(i0, U1.lo[0], U1.hi[0]) : 0u;
+        uz = (j >= U2.lo[1] && j < U2.hi[1]) ? xmask<VX>(i0, U2.lo[0], U2.hi[0]) : 0u;
+        S0 = a.slab[0];
+        S1 = a.slab[1];
+        S2 = a.slab[2];
+        sxm = 0;
+#pragma unroll
+        for (int v = 0; v < VX; v++) sxm |= (unsigned)(slab_local(S0, i0 + v) >= 0) << v;
+        sxm = (j >= S0.other.lo[1] && j < S0.other.hi[1]) ? sxm : 0u;
+        ly = slab_local(S1, j);
+        sym = ly >= 0 ? xmask<VX>(i0, S1.other.lo[0], S1.other.hi[0]) : 0u;
+        szm = (j >= S2.other.lo[1] && j < S2.other.hi[1]) ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : 0u;
+    }
+    const int col = j * py + i0;
 
     // z window: planes kb-1 .. kb+KZ+1 of Ex and Ey
-    T wx[KZ + 3], wy[KZ + 3];
+    T wx[KZ + 3][VX], wy[KZ + 3][VX];
 #pragma unroll
     for (int q = 0; q < KZ + 3; q++) {
         const int kk = kb - 1 + q;
-        const bool ok = kk >= 0 && kk < nz;
-        wx[q] = ok ? __ldg(Ex + kk * pz + col) : T(0);
-        wy[q] = ok ? __ldg(Ey + kk * pz + col) : T(0);
+        if (INT || (kk >= 0 && kk < nz)) {
+            ldv<T, VX>(wx[q], Ex + kk * pz + col);
+            ldv<T, VX>(wy[q], Ey + kk * pz + col);
+        } else {
+            zerov<T, VX>(wx[q]);
+            zerov<T, VX>(wy[q]);
+        }
     }
 
 #pragma unroll
     for (int q = 0; q < KZ; q++) {
         const int k = kb + q;
-        if (k >= nz) break;
-        const long long c = k * pz + col;
-        const bool vz = (k >= 1) && (k + 2 < nz);
-        const T ez = __ldg(Ez + c);
-        T dyEz = T(0), dyEx = T(0), dxEz = T(0), dxEy = T(0), dzEy = T(0), dzEx = T(0), dxEzt = T(0);
-        if (vy) {
-            const T a0 = __ldg(Ez + c + py), a1 = __ldg(Ez + c + 2 * py), a2 = __ldg(Ez + c - py);
-            const T b0 = __ldg(Ex + c + py), b1 = __ldg(Ex + c + 2 * py), b2 = __ldg(Ex + c - py);
-            dyEz = c1 * (a0 - ez) + c2 * (a1 - a2);
-            dyEx = c1 * (b0 - wx[q + 1]) + c2 * (b1 - b2);
-        }
-        if (vx) {
-            const T a0 = __ldg(Ez + c + 1), a1 = __ldg(Ez + c + 2), a2 = __ldg(Ez + c - 1);
-            const T b0 = __ldg(Ey + c + 1), b1 = __ldg(Ey + c + 2), b2 = __ldg(Ey + c - 1);
-            dxEz = c1 * (a0 - ez) + c2 * (a1 - a2);
-            dxEzt = c1 * a0 - c2t * ez + c2 * a1 - c2 * a2;  // psi_Hyx stencil, cpu_cpml4.f90:400
-            dxEy = c1 * (b0 - wy[q + 1]) + c2 * (b1 - b2);
-        }
-        if (vz) {
-            dzEy = c1 * (wy[q + 2] - wy[q + 1]) + c2 * (wy[q + 3] - wy[q]);
-            dzEx = c1 * (wx[q + 2] - wx[q + 1]) + c2 * (wx[q + 3] - wx[q]);
-        }
-        const T m = __ldg(M + c);
-        const T dm = DM ? __ldg(DM + c) : a.dtmu0;
-        const T msh_z = __ldg(P + 16 * nmax + 1 * nmax + k), ik_z = __ldg(P + 16 * nmax + 7 * nmax + k);
-        T hx = Hx[c], hy = Hy[c], hz = Hz[c];
-
-        T da_x = T(1), db_x = dm, da_y = T(1), db_y = dm, da_z = T(1), db_z = dm;
-        if (msh_x != T(0)) { const T h = msh_x * m; const T r = rcp(T(1) + h); da_x = (T(1) - h) * r; db_x = dm * r; }
-        if (msh_y != T(0)) { const T h = msh_y * m; const T r = rcp(T(1) + h); da_y = (T(1) - h) * r; db_y = dm * r; }
-        if (msh_z != T(0)) { const T h = msh_z * m; const T r = rcp(T(1) + h); da_z = (T(1) - h) * r; db_z = dm * r; }
-        if (in_box(a.upd[0], i, j, k)) hx = da_x * hx - a.sgn * db_x * (dyEz * ik_y - dzEy * ik_z);
-        if (in_box(a.upd[1], i, j, k)) hy = da_y * hy - a.sgn * db_y * (dzEx * ik_z - dxEz * ik_x);
-        if (in_box(a.upd[2], i, j, k)) hz = da_z * hz - a.sgn * db_z * (dxEy * ik_x - dyEx * ik_y);
-
-        if (sx_col && k >= a.slab[0].other.lo[2] && k < a.slab[0].other.hi[2]) {
-            T *__restrict__ q0 = a.psi[0][0];
-            T *__restrict__ q1 = a.psi[0][1];
-            const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
-            const T bh = __ldg(P + 4 * nmax + i), chd = __ldg(P + 5 * nmax + i);
-            const T p0 = bh * q0[o] + chd * dxEy;   // psi_Hzx
-            const T p1 = bh * q1[o] + chd * dxEzt;  // psi_Hyx
-            q0[o] = p0;
-            q1[o] = p1;
-            hz = hz - db_z * p0;
-            hy = hy + db_y * p1;
-        }
-        if (sy_col && k >= a.slab[1].other.lo[2] && k < a.slab[1].other.hi[2]) {
-            T *__restrict__ q0 = a.psi[1][0];
-            T *__restrict__ q1 = a.psi[1][1];
-            const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
-            const T bh = __ldg(P + 8 * nmax + 4 * nmax + j), chd = __ldg(P + 8 * nmax + 5 * nmax + j);
-            const T p0 = bh * q0[o] + chd * dyEz;  // psi_Hxy
-            const T p1 = bh * q1[o] + chd * dyEx;  // psi_Hzy
-            q0[o] = p0;
-            q1[o] = p1;
-            hx = hx - db_x * p0;
-            hz = hz + db_z * p1;
-        }
-        if (sz_col) {
-            const int lz = slab_local(a.slab[2], k);
-            if (lz >= 0) {
-                T *__restrict__ q0 = a.psi[2][0];
-                T *__restrict__ q1 = a.psi[2][1];
-                const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
-                const T bh = __ldg(P + 16 * nmax + 4 * nmax + k), chd = __ldg(P + 16 * nmax + 5 * nmax + k);
-                const T p0 = bh * q0[o] + chd * dzEx;  // psi_Hyz
-                const T p1 = bh * q1[o] + chd * dzEy;  // psi_Hxz
-                q0[o] = p0;
-                q1[o] = p1;
-                hy = hy - db_y * p0;
-                hx = hx + db_x * p1;
+        if (!INT && k >= khi) break;
+        const int c = k * pz + col;
+        T ezx[3 * VX], eyx[3 * VX];
+        {
+            T t[VX];
+            ldv<T, VX>(t, Ez + c);
+#pragma unroll
+            for (int v = 0; v < VX; v++) { ezx[VX + v] = t[v]; eyx[VX + v] = wy[q + 1][v]; }
+            if (has_l) {
+                ldv<T, VX>(t, Ez + c - VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) ezx[v] = t[v];
+                ldv<T, VX>(t, Ey + c - VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) eyx[v] = t[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < VX; v++) { ezx[v] = T(0); eyx[v] = T(0); }
+            }
+            if (has_r) {
+                ldv<T, VX>(t, Ez + c + VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) ezx[2 * VX + v] = t[v];
+                ldv<T, VX>(t, Ey + c + VX);
+#pragma unroll
+                for (int v = 0; v < VX; v++) eyx[2 * VX + v] = t[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < VX; v++) { ezx[2 * VX + v] = T(0); eyx[2 * VX + v] = T(0); }
             }
         }
-        Hx[c] = hx;
-        Hy[c] = hy;
-        Hz[c] = hz;
+        T ezm1[VX], ezp1[VX], ezp2[VX], exm1[VX], exp1[VX], exp2[VX];
+        if (vy) {
+            ldv<T, VX>(ezm1, Ez + c - py);
+            ldv<T, VX>(ezp1, Ez + c + py);
+            ldv<T, VX>(ezp2, Ez + c + 2 * py);
+            ldv<T, VX>(exm1, Ex + c - py);
+            ldv<T, VX>(exp1, Ex + c + py);
+            ldv<T, VX>(exp2, Ex + c + 2 * py);
+        } else {
+            zerov<T, VX>(ezm1); zerov<T, VX>(ezp1); zerov<T, VX>(ezp2);
+            zerov<T, VX>(exm1); zerov<T, VX>(exp1); zerov<T, VX>(exp2);
+        }
+        T m[VX], dm[VX], hx[VX], hy[VX], hz[VX];
+        ldv<T, VX>(m, M + c);
+        if (DM) {
+            ldv<T, VX>(dm, DM + c);
+        } else {
+#pragma unroll
+            for (int v = 0; v < VX; v++) dm[v] = a.dtmu0;
+        }
+        ldv_rw<T, VX>(hx, Hx + c);
+        ldv_rw<T, VX>(hy, Hy + c);
+        ldv_rw<T, VX>(hz, Hz + c);
+        T msh_z, ik_z;
+        bool vz, kx, ky, kz;
+        int lz;
+        if constexpr (INT) {
+            msh_z = T(0);
+            ik_z = a.ik[2];
+            vz = kx = ky = kz = true;
+            lz = -1;
+        } else {
+            msh_z = __ldg(P + 17 * ps + k);
+            ik_z = __ldg(P + 23 * ps + k);
+            vz = (k >= 1) && (k + 2 < nz);
+            kx = k >= a.upd[0].lo[2] && k < a.upd[0].hi[2];
+            ky = k >= a.upd[1].lo[2] && k < a.upd[1].hi[2];
+            kz = k >= a.upd[2].lo[2] && k < a.upd[2].hi[2];
+            lz = slab_local(S2, k);
+        }
+
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            const bool vx = vxm >> v & 1;
+            const T ez = ezx[VX + v];
+            const T dyEz = vy ? d4(c1, c2, ezp1[v], ez, ezp2[v], ezm1[v]) : T(0);
+            const T dyEx = vy ? d4(c1, c2, exp1[v], wx[q + 1][v], exp2[v], exm1[v]) : T(0);
+            const T dxEz = vx ? d4(c1, c2, ezx[VX + v + 1], ez, ezx[VX + v + 2], ezx[VX + v - 1]) : T(0);
+            const T dxEy = vx ? d4(c1, c2, eyx[VX + v + 1], eyx[VX + v], eyx[VX + v + 2], eyx[VX + v - 1]) : T(0);
+            const T dzEy = vz ? d4(c1, c2, wy[q + 2][v], wy[q + 1][v], wy[q + 3][v], wy[q][v]) : T(0);
+            const T dzEx = vz ? d4(c1, c2, wx[q + 2][v], wx[q + 1][v], wx[q + 3][v], wx[q][v]) : T(0);
+            const T mv = m[v], dmv = dm[v];
+            T da_x = T(1), db_x = dmv, da_y = T(1), db_y = dmv, da_z = T(1), db_z = dmv;
+            if (!INT) {
+                if (msh_x[v] != T(0)) { const T h = msh_x[v] * mv; const T r = rcp(T(1) + h); da_x = (T(1) - h) * r; db_x = dmv * r; }
+                if (msh_y != T(0)) { const T h = msh_y * mv; const T r = rcp(T(1) + h); da_y = (T(1) - h) * r; db_y = dmv * r; }
+                if (msh_z != T(0)) { const T h = msh_z * mv; const T r = rcp(T(1) + h); da_z = (T(1) - h) * r; db_z = dmv * r; }
+            }
+            if (kx && (ux >> v & 1)) hx[v] = leap(da_x, -sg * db_x, curl2(dyEz, ik_y, dzEy, ik_z), hx[v]);
+            if (ky && (uy >> v & 1)) hy[v] = leap(da_y, -sg * db_y, curl2(dzEx, ik_z, dxEz, ik_x[v]), hy[v]);
+            if (kz && (uz >> v & 1)) hz[v] = leap(da_z, -sg * db_z, curl2(dxEy, ik_x[v], dyEx, ik_y), hz[v]);
+
+            if (!INT) {
+                if ((sxm >> v & 1) && k >= S0.other.lo[2] && k < S0.other.hi[2]) {
+                    T *__restrict__ q0 = a.psi[0][0] + shot * a.pshot[0];
+                    T *__restrict__ q1 = a.psi[0][1] + shot * a.pshot[0];
+                    const int o = (k * ny + j) * S0.width + slab_local(S0, i0 + v);
+                    const T bh = __ldg(P + 4 * ps + i0 + v), chd = __ldg(P + 5 * ps + i0 + v);
+                    // psi_Hyx stencil (cpu_cpml4.f90:400): c1 Ez(i+1) - c2t Ez(i) + c2 Ez(i+2) - c2 Ez(i-1)
+                    const T dxEzt = vx ? fma(c1, ezx[VX + v + 1], -(c2t * ez)) + c2 * (ezx[VX + v + 2] - ezx[VX + v - 1]) : T(0);
+                    const T p0 = fma(bh, q0[o], chd * dxEy);   // psi_Hzx
+                    const T p1 = fma(bh, q1[o], chd * dxEzt);  // psi_Hyx
+                    q0[o] = p0;
+                    q1[o] = p1;
+                    hz[v] = fma(-db_z, p0, hz[v]);
+                    hy[v] = fma(db_y, p1, hy[v]);
+                }
+                if ((sym >> v & 1) && k >= S1.other.lo[2] && k < S1.other.hi[2]) {
+                    T *__restrict__ q0 = a.psi[1][0] + shot * a.pshot[1];
+                    T *__restrict__ q1 = a.psi[1][1] + shot * a.pshot[1];
+                    const int o = (k * S1.width + ly) * py + i0 + v;
+                    const T bh = __ldg(P + 12 * ps + j), chd = __ldg(P + 13 * ps + j);
+                    const T p0 = fma(bh, q0[o], chd * dyEz);  // psi_Hxy
+                    const T p1 = fma(bh, q1[o], chd * dyEx);  // psi_Hzy
+                    q0[o] = p0;
+                    q1[o] = p1;
+                    hx[v] = fma(-db_x, p0, hx[v]);
+                    hz[v] = fma(db_z, p1, hz[v]);
+                }
+                if ((szm >> v & 1) && lz >= 0) {
+                    T *__restrict__ q0 = a.psi[2][0] + shot * a.pshot[2];
+                    T *__restrict__ q1 = a.psi[2][1] + shot * a.pshot[2];
+                    const int o = (lz * ny + j) * py + i0 + v;
+                    const T bh = __ldg(P + 20 * ps + k), chd = __ldg(P + 21 * ps + k);
+                    const T p0 = fma(bh, q0[o], chd * dzEx);  // psi_Hyz
+                    const T p1 = fma(bh, q1[o], chd * dzEy);  // psi_Hxz
+                    q0[o] = p0;
+                    q1[o] = p1;
+                    hy[v] = fma(-db_y, p0, hy[v]);
+                    hx[v] = fma(db_x, p1, hx[v]);
+                }
+            }
+        }
+        stv<T, VX>(Hx + c, hx);
+        stv<T, VX>(Hy + c, hy);
+        stv<T, VX>(Hz + c, hz);
     }
 }
 
-// Tile/depth variants the autotuner chooses from (BX, BY, KZ).
-#define MITTET_STENCIL_VARIANTS(X) \
-    X(32, 4, 1)                    \
-    X(32, 8, 1)                    \
-    X(64, 4, 1)                    \
-    X(32, 16, 1)                   \
-    X(32, 4, 2)                    \
-    X(32, 8, 2)                    \
-    X(64, 2, 2)                    \
-    X(32, 4, 4)                    \
-    X(32, 8, 4)
+// Locate this CTA's box and tile (tile index b over all boxes).
+template <int VX, int BX, int BY, int KZ>
+__device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int b, int &i0, int &j, int &kb, int &khi,
+                                       bool &inside) {
+    const int nbox = __ldg(&tm->nbox);
+    int q = 0;
+    for (int t = 1; t < nbox; t++)
+        if (b >= __ldg(&tm->start[t])) q = t;
+    const int local = b - __ldg(&tm->start[q]);
+    const int ntx = __ldg(&tm->ntx[q]), nty = __ldg(&tm->nty[q]);
+    const int tx = local % ntx, r = local / ntx;
+    const int ty = r % nty, tz = r / nty;
+    i0 = __ldg(&tm->lo[q][0]) + (tx * BX + (int)threadIdx.x) * VX;
+    j = __ldg(&tm->lo[q][1]) + ty * BY + (int)threadIdx.y;
+    kb = __ldg(&tm->lo[q][2]) + tz * KZ;
+    khi = __ldg(&tm->hi[q][2]);
+    inside = i0 < __ldg(&tm->hi[q][0]) && j < __ldg(&tm->hi[q][1]);
+}
+
+// Interior tiles (box 0 when tm->interior): straight-line body, own register budget.
+template <typename T, int VX, int BX, int BY, int KZ>
+__global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, KZ, BX *BY))
+    e_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {
+    int i0, j, kb, khi;
+    bool inside;
+    locate<VX, BX, BY, KZ>(tm, blockIdx.x, i0, j, kb, khi, inside);
+    e_cells<T, VX, KZ, true>(a, blockIdx.y, i0, j, kb, kb + KZ);
+}
+template <typename T, int VX, int BX, int BY, int KZ>
+__global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, KZ, BX *BY))
+    h_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {
+    int i0, j, kb, khi;
+    bool inside;
+    locate<VX, BX, BY, KZ>(tm, blockIdx.x, i0, j, kb, khi, inside);
+    h_cells<T, VX, KZ, true>(a, blockIdx.y, i0, j, kb, kb + KZ);
+}
+
+// Shell tiles (every box after the interior one): the general body.
+template <typename T, int VX, int BX, int BY, int KZ>
+__global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))
+    e_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {
+    int i0, j, kb, khi;
+    bool inside;
+    locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);
+    if (inside) e_cells<T, VX, KZ, false>(a, blockIdx.y, i0, j, kb, khi);
+}
+template <typename T, int VX, int BX, int BY, int KZ>
+__global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))
+    h_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {
+    int i0, j, kb, khi;
+    bool inside;
+    locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);
+    if (inside) h_cells<T, VX, KZ, false>(a, blockIdx.y, i0, j, kb, khi);
+}
+
+// Variants the autotuner chooses from: (VX, BX, BY, KZ).
+#define MITTET_STENCIL_VARIANTS_F32(X) \
+    X(2, 32, 4, 1)                     \
+    X(2, 32, 8, 1)                     \
+    X(2, 16, 8, 1)                     \
+    X(2, 64, 2, 1)                     \
+    X(4, 32, 4, 1)                     \
+    X(4, 16, 8, 1)                     \
+    X(4, 8, 16, 1)                     \
+    X(2, 32, 4, 2)                     \
+    X(4, 16, 4, 2)
+#define MITTET_STENCIL_VARIANTS_F64(X) \
+    X(2, 32, 4, 1)                     \
+    X(2, 32, 8, 1)                     \
+    X(2, 16, 8, 1)                     \
+    X(2, 64, 2, 1)                     \
+    X(2, 32, 4, 2)                     \
+    X(2, 16, 4, 2)
 
 }  // namespace mittet

@@ -242,8 +242,8 @@ class MittetSolver:
         return dict(zip(["inject_magnetic", "e_phase", "inject_electric", "h_phase", "sample", "volume_dft"], ms.tolist()))
 
     def tuned_variant(self) -> dict:
-        e = (ctypes.c_int32 * 3)()
-        h = (ctypes.c_int32 * 3)()
+        e = (ctypes.c_int32 * 4)()
+        h = (ctypes.c_int32 * 4)()
         check(self._lib.mittet_tuned_variant(self._h, e, h))
         return {"e_phase": list(e), "h_phase": list(h)}
 

@@ -129,17 +129,19 @@ def test_batched_shots_equal_single_shots():
         assert np.array_equal(spec[k], sp1[0])
 
 
-def test_linearity_in_source_amplitude():
-    # amplitudes large enough that no sample is an FP32 denormal, where doubling is not exact
-    wl = W.small_case(nt=100, precision=FP32)
+@pytest.mark.parametrize("prec", [FP32, FP64])
+def test_linearity_in_source_amplitude(prec):
+    # Doubling is exact for normal numbers, but the stencil's precursors ahead
+    # of the wavefront reach the denormal range, so compare in rel-L2.
+    wl = W.small_case(nt=100, precision=prec)
     x, y, z, c, k, a = wl.shots[0].points[0]
-    wl = replace(wl, shots=[Shot(points=[(x, y, z, c, k, 2.0 ** 60)])])
-    wl2 = replace(wl, shots=[Shot(points=[(x, y, z, c, k, 2.0 ** 61)])])
+    wl2 = replace(wl, shots=[Shot(points=[(x, y, z, c, k, 2.0 * a)])])
     with W.make_solver(wl) as s:
-        _, t1 = s.forward(wl.nt, want_traces=True)
+        sp1, t1 = s.forward(wl.nt, want_traces=True)
     with W.make_solver(wl2) as s:
-        _, t2 = s.forward(wl.nt, want_traces=True)
-    assert np.array_equal(2.0 * t1, t2)  # scaling by 2 is exact in binary floating point
+        sp2, t2 = s.forward(wl.nt, want_traces=True)
+    assert rel_l2(t2, 2.0 * t1) <= (1e-7 if prec == FP32 else 1e-15)
+    assert rel_l2(sp2, 2.0 * sp1) <= (1e-7 if prec == FP32 else 1e-15)
 
 
 def test_volume_dft_matches_oracle_dft_of_traces():
