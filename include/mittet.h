@@ -207,6 +207,33 @@ int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);
 
+/* Forward solve that allocates no device memory.  No counterpart in the
+ * reference (whose Fortran/C drivers own static arrays); it exists for hosts
+ * that cannot call cudaMalloc/cudaFree: cudaFree synchronises the whole
+ * device and stalls other streams of a serving process, code running during
+ * stream capture may not allocate, and some hosts' device memory belongs to
+ * another allocator.  Every intermediate buffer lives in one file-scope
+ * __device__ array of 32 MiB that each GPU loading the library keeps until
+ * exit; a solve whose padded layout does not fit (about 96^3 cells with a few
+ * hundred receivers for a few thousand steps), or with more than 256 cells
+ * on an axis, 64 points, 2048 receivers or 256 frequencies, is rejected with
+ * MITTET_ERR_INVALID_ARG.  FP32 fields with an FP64 f_to_d, one shot (every
+ * point has shot 0), uniform permeability phys->mu0.
+ *   sigma_dev:   device, nx*ny*nz doubles, x fastest
+ *   wavelet_dev: device, nt+1 doubles, w[n] = s(n dt)
+ *   pts, rec, omega: host arrays (copied into the device array)
+ *   rec_fd_dev:  device output, [nrec][nf] complex (interleaved doubles)
+ *   stream:      cudaStream_t (NULL = legacy default stream); the call only
+ *                enqueues work, results are ready when the stream reaches it.
+ * The first call on a device looks up the array's address with that device
+ * current; make it before any stream capture.  Calls share the array and it
+ * keeps the last call's contents (what must start at zero is cleared by each
+ * call); calls that overlap on the GPU race on it. */
+int mittet_forward_noalloc(const mittet_grid *grid, const mittet_phys *phys, const double *sigma_dev,
+                           int32_t npoint, const mittet_point_source *pts, int32_t nt, const double *wavelet_dev,
+                           int32_t nrec, const mittet_receiver *rec, int32_t nf, const double *omega,
+                           int32_t h_factor, double *rec_fd_dev, void *stream);
+
 /* Message of the calling thread's last error; returns its length. */
 int mittet_last_error(char *buf, size_t len);
 

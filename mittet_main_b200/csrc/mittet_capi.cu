@@ -87,6 +87,11 @@ DSlab to_dslab(const Slab &s) {
 
 }  // namespace
 
+namespace mittet {
+// Lets the other translation unit of the library report through mittet_last_error.
+void set_last_error(const char *msg) { g_err = msg; }
+}  // namespace mittet
+
 struct mittet_handle_s {
     mittet_grid g{};
     mittet_phys ph{};
