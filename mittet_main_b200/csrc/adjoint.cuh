@@ -1,0 +1,428 @@
+// adjoint.cuh -- discrete adjoint of the forward step, for the FWI gradient.
+//
+// The forward step is linear in the state (E, H, psi_E, psi_H) for a fixed
+// model; its transpose is applied step by step in reverse time.  Each half
+// step's transpose is split in two kernels so that no kernel reads a
+// neighbour value another thread writes:
+//   *_own  (one cell): from the adjoint of the phase output it forms the
+//          adjoint weight mu of every derivative the phase used at that cell,
+//          the cell's gradient terms, and the adjoint of the phase input of
+//          its own field (lambda <- ca lambda, psi-adjoint <- b psi-adjoint);
+//   *_gather (one cell): adds the transposed (2,4) differences of those mu
+//          to the other field's adjoint, reading mu at the neighbours.
+// Adjoint step n (reverse of forward step n):
+//   inject a_H[n] -> lambda_H ; H_own ; H_gather (-> lambda_E) ;
+//   inject a_E[n] -> lambda_E ; source terms ; E_own ; E_gather (-> lambda_H).
+// Gradient of the misfit with respect to sigma (m = 2 w0 dt / sigma):
+//   E phase, every cell:  lambda_E1 [ (in range) dca E0 + (dcb/cb)(E1 - (in range ? ca E0 : E0)) ],
+//     h = esig m / 2, ca = (1-h)/(1+h), dca = 2h/(sigma(1+h)^2), dcb/cb = -1/(sigma(1+h));
+//   H phase, CPML cells:  lambda_H1 [ (in range) dda H0 + (ddb/db)(H1 - (in range ? da H0 : H0)) ],
+//     h = msig m / 2, dda = 2h/(sigma(1+h)^2), ddb/db = h/(sigma(1+h));
+//   electric source gain dt 2 w0/(sigma vol): lambda_E1s g w / sigma.
+#pragma once
+
+namespace mittet {
+
+template <typename T>
+struct AdjArgs {
+    // forward states of this step: E0, H0 = state before the step, E1, H1 = after
+    const T *E0[3], *H0[3], *E1[3], *H1[3];
+    T *lam[6];        // adjoint fields Ex..Hz, [shot][cell]
+    T *lpsi[3][2];    // adjoint psi of this phase's slab groups
+    T *mu[7];         // derivative adjoint weights
+    double *grad;     // [shot][cell] gradient accumulators
+    const T *m;       // model word 2 w0 dt / sigma
+    const T *dtmu;
+    T dtmu0;
+    const T *prof;
+    int nmax;
+    int nx, ny, nz, px;
+    long long plane, fshot;
+    long long pshot[3];
+    DBox upd[3];
+    DSlab slab[3];
+    T c1, c2, c2t, sgn;
+    double inv2w0dt;  // 1/(2 w0 dt): 1/sigma = m * inv2w0dt
+};
+
+__device__ __forceinline__ bool adj_cell(int &i, int &j, int &k, int &shot, int nx, int ny, int nz) {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int zz = blockIdx.z;
+    k = zz % nz;
+    shot = zz / nz;
+    return i < nx && j < ny;
+}
+
+template <typename T>
+__device__ __forceinline__ T pget(const AdjArgs<T> &a, int axis, int which, int v) {
+    return __ldg(a.prof + ((size_t)axis * 8 + which) * a.nmax + v);
+}
+
+// ---------------------------------------------------------------- H phase
+// mu[0] Dy+Ez, mu[1] Dz+Ey, mu[2] Dz+Ex, mu[3] Dx+Ez, mu[4] typo Dx Ez (psi_Hyx), mu[5] Dx+Ey, mu[6] Dy+Ex
+template <typename T>
+__global__ void adj_h_own_kernel(AdjArgs<T> a) {
+    int i, j, k, shot;
+    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long sb = (long long)shot * a.fshot;
+    const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
+    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
+    const T m = a.m[cm];
+    const T dm = a.dtmu ? a.dtmu[cm] : a.dtmu0;
+    const T msh[3] = {pget(a, 0, 1, i), pget(a, 1, 1, j), pget(a, 2, 1, k)};
+    const T ik[3] = {pget(a, 0, 7, i), pget(a, 1, 7, j), pget(a, 2, 7, k)};
+    T da[3], db[3];
+    for (int q = 0; q < 3; q++) {
+        if (msh[q] != T(0)) {
+            const T h = msh[q] * m;
+            const T r = rcp(T(1) + h);
+            da[q] = (T(1) - h) * r;
+            db[q] = dm * r;
+        } else {
+            da[q] = T(1);
+            db[q] = dm;
+        }
+    }
+    const bool in0 = in_box(a.upd[0], i, j, k), in1 = in_box(a.upd[1], i, j, k), in2 = in_box(a.upd[2], i, j, k);
+    const T L0 = a.lam[3][c], L1 = a.lam[4][c], L2 = a.lam[5][c];
+    const T s = a.sgn;
+    T mu0 = in0 ? -s * db[0] * ik[1] * L0 : T(0);
+    T mu1 = in0 ? s * db[0] * ik[2] * L0 : T(0);
+    T mu2 = in1 ? -s * db[1] * ik[2] * L1 : T(0);
+    T mu3 = in1 ? s * db[1] * ik[0] * L1 : T(0);
+    T mu4 = T(0);
+    T mu5 = in2 ? -s * db[2] * ik[0] * L2 : T(0);
+    T mu6 = in2 ? s * db[2] * ik[1] * L2 : T(0);
+    // slab psi adjoints
+    const int lx = slab_local(a.slab[0], i), ly = slab_local(a.slab[1], j), lz = slab_local(a.slab[2], k);
+    if (lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1] && k >= a.slab[0].other.lo[2] &&
+        k < a.slab[0].other.hi[2]) {
+        const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
+        const T bh = pget(a, 0, 4, i), chd = pget(a, 0, 5, i);
+        const T lzx = a.lpsi[0][0][o] - db[2] * L2;  // psi_Hzx
+        const T lyx = a.lpsi[0][1][o] + db[1] * L1;  // psi_Hyx
+        a.lpsi[0][0][o] = bh * lzx;
+        a.lpsi[0][1][o] = bh * lyx;
+        mu5 += chd * lzx;
+        mu4 += chd * lyx;
+    }
+    if (ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0] && k >= a.slab[1].other.lo[2] &&
+        k < a.slab[1].other.hi[2]) {
+        const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
+        const T bh = pget(a, 1, 4, j), chd = pget(a, 1, 5, j);
+        const T lxy = a.lpsi[1][0][o] - db[0] * L0;  // psi_Hxy
+        const T lzy = a.lpsi[1][1][o] + db[2] * L2;  // psi_Hzy
+        a.lpsi[1][0][o] = bh * lxy;
+        a.lpsi[1][1][o] = bh * lzy;
+        mu0 += chd * lxy;
+        mu6 += chd * lzy;
+    }
+    if (lz >= 0 && i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
+        j < a.slab[2].other.hi[1]) {
+        const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
+        const T bh = pget(a, 2, 4, k), chd = pget(a, 2, 5, k);
+        const T lyz = a.lpsi[2][0][o] - db[1] * L1;  // psi_Hyz
+        const T lxz = a.lpsi[2][1][o] + db[0] * L0;  // psi_Hxz
+        a.lpsi[2][0][o] = bh * lyz;
+        a.lpsi[2][1][o] = bh * lxz;
+        mu2 += chd * lyz;
+        mu1 += chd * lxz;
+    }
+    a.mu[0][c] = mu0; a.mu[1][c] = mu1; a.mu[2][c] = mu2; a.mu[3][c] = mu3;
+    a.mu[4][c] = mu4; a.mu[5][c] = mu5; a.mu[6][c] = mu6;
+    // gradient (CPML cells only: interior da, db do not depend on sigma)
+    double gsum = 0.0;
+    const double isig = (double)m * a.inv2w0dt;
+    const bool in[3] = {in0, in1, in2};
+    const T L[3] = {L0, L1, L2};
+    for (int q = 0; q < 3; q++) {
+        if (msh[q] == T(0)) continue;
+        const double h = (double)msh[q] * (double)m;
+        const double dda = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
+        const double rdb = h * isig / (1.0 + h);
+        const double h0 = (double)a.H0[q][c], h1 = (double)a.H1[q][c];
+        gsum += (double)L[q] * ((in[q] ? dda * h0 : 0.0) + rdb * (h1 - (in[q] ? (double)da[q] * h0 : h0)));
+    }
+    if (gsum != 0.0) a.grad[c] += gsum;
+    a.lam[3][c] = in0 ? da[0] * L0 : L0;
+    a.lam[4][c] = in1 ? da[1] * L1 : L1;
+    a.lam[5][c] = in2 ? da[2] * L2 : L2;
+}
+
+// (D+^T mu)[u] = c1 mu[u-1] - c1 mu[u] + c2 mu[u-2] - c2 mu[u+1];  typo: c2t replaces c1 on mu[u]
+template <typename T>
+__device__ __forceinline__ T dplus_t(const T *__restrict__ mu, long long c, long long s, int v, int n, T c1, T c2, T c1u) {
+    T r = -c1u * mu[c];
+    if (v >= 1) r += c1 * mu[c - s];
+    if (v >= 2) r += c2 * mu[c - 2 * s];
+    if (v + 1 < n) r -= c2 * mu[c + s];
+    return r;
+}
+
+template <typename T>
+__global__ void adj_h_gather_kernel(AdjArgs<T> a) {
+    int i, j, k, shot;
+    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i;
+    const long long sy = a.px, sz = a.plane;
+    const T c1 = a.c1, c2 = a.c2;
+    const T gz = dplus_t(a.mu[0], c, sy, j, a.ny, c1, c2, c1) + dplus_t(a.mu[3], c, 1, i, a.nx, c1, c2, c1) +
+                 dplus_t(a.mu[4], c, 1, i, a.nx, c1, c2, a.c2t);
+    const T gy = dplus_t(a.mu[1], c, sz, k, a.nz, c1, c2, c1) + dplus_t(a.mu[5], c, 1, i, a.nx, c1, c2, c1);
+    const T gx = dplus_t(a.mu[2], c, sz, k, a.nz, c1, c2, c1) + dplus_t(a.mu[6], c, sy, j, a.ny, c1, c2, c1);
+    a.lam[0][c] += gx;
+    a.lam[1][c] += gy;
+    a.lam[2][c] += gz;
+}
+
+// ---------------------------------------------------------------- E phase
+// mu[0] DyHz, mu[1] DzHy, mu[2] DzHx, mu[3] DxHz, mu[4] DxHy, mu[5] DyHx
+template <typename T>
+__global__ void adj_e_own_kernel(AdjArgs<T> a) {
+    int i, j, k, shot;
+    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long sb = (long long)shot * a.fshot;
+    const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
+    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
+    const T m = a.m[cm];
+    const T esh[3] = {pget(a, 0, 0, i), pget(a, 1, 0, j), pget(a, 2, 0, k)};
+    const T ik[3] = {pget(a, 0, 6, i), pget(a, 1, 6, j), pget(a, 2, 6, k)};
+    T ca[3], cb[3];
+    for (int q = 0; q < 3; q++) {
+        if (esh[q] != T(0)) {
+            const T h = esh[q] * m;
+            const T r = rcp(T(1) + h);
+            ca[q] = (T(1) - h) * r;
+            cb[q] = m * r;
+        } else {
+            ca[q] = T(1);
+            cb[q] = m;
+        }
+    }
+    const bool in0 = in_box(a.upd[0], i, j, k), in1 = in_box(a.upd[1], i, j, k), in2 = in_box(a.upd[2], i, j, k);
+    const T L0 = a.lam[0][c], L1 = a.lam[1][c], L2 = a.lam[2][c];
+    const T s = a.sgn;
+    T mu0 = in0 ? s * cb[0] * ik[1] * L0 : T(0);   // DyHz
+    T mu1 = in0 ? -s * cb[0] * ik[2] * L0 : T(0);  // DzHy
+    T mu2 = in1 ? s * cb[1] * ik[2] * L1 : T(0);   // DzHx
+    T mu3 = in1 ? -s * cb[1] * ik[0] * L1 : T(0);  // DxHz
+    T mu4 = in2 ? s * cb[2] * ik[0] * L2 : T(0);   // DxHy
+    T mu5 = in2 ? -s * cb[2] * ik[1] * L2 : T(0);  // DyHx
+    const int lx = slab_local(a.slab[0], i), ly = slab_local(a.slab[1], j), lz = slab_local(a.slab[2], k);
+    if (lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1] && k >= a.slab[0].other.lo[2] &&
+        k < a.slab[0].other.hi[2]) {
+        const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
+        const T be = pget(a, 0, 2, i), ced = pget(a, 0, 3, i);
+        const T lzx = a.lpsi[0][0][o] + cb[2] * L2;  // psi_Ezx
+        const T lyx = a.lpsi[0][1][o] - cb[1] * L1;  // psi_Eyx
+        a.lpsi[0][0][o] = be * lzx;
+        a.lpsi[0][1][o] = be * lyx;
+        mu4 += ced * lzx;
+        mu3 += ced * lyx;
+    }
+    if (ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0] && k >= a.slab[1].other.lo[2] &&
+        k < a.slab[1].other.hi[2]) {
+        const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
+        const T be = pget(a, 1, 2, j), ced = pget(a, 1, 3, j);
+        const T lxy = a.lpsi[1][0][o] + cb[0] * L0;  // psi_Exy
+        const T lzy = a.lpsi[1][1][o] - cb[2] * L2;  // psi_Ezy
+        a.lpsi[1][0][o] = be * lxy;
+        a.lpsi[1][1][o] = be * lzy;
+        mu0 += ced * lxy;
+        mu5 += ced * lzy;
+    }
+    if (lz >= 0 && i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
+        j < a.slab[2].other.hi[1]) {
+        const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
+        const T be = pget(a, 2, 2, k), ced = pget(a, 2, 3, k);
+        const T lyz = a.lpsi[2][0][o] + cb[1] * L1;  // psi_Eyz
+        const T lxz = a.lpsi[2][1][o] - cb[0] * L0;  // psi_Exz
+        a.lpsi[2][0][o] = be * lyz;
+        a.lpsi[2][1][o] = be * lxz;
+        mu2 += ced * lyz;
+        mu1 += ced * lxz;
+    }
+    a.mu[0][c] = mu0; a.mu[1][c] = mu1; a.mu[2][c] = mu2;
+    a.mu[3][c] = mu3; a.mu[4][c] = mu4; a.mu[5][c] = mu5;
+    // gradient: every cell (cb = m/(1+h) depends on sigma everywhere)
+    const double isig = (double)m * a.inv2w0dt;
+    const bool in[3] = {in0, in1, in2};
+    const T L[3] = {L0, L1, L2};
+    double gsum = 0.0;
+    for (int q = 0; q < 3; q++) {
+        const double h = (double)esh[q] * (double)m;
+        const double dca = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
+        const double rcb = -isig / (1.0 + h);
+        const double e0 = (double)a.E0[q][c], e1 = (double)a.E1[q][c];
+        gsum += (double)L[q] * ((in[q] ? dca * e0 : 0.0) + rcb * (e1 - (in[q] ? (double)ca[q] * e0 : e0)));
+    }
+    a.grad[c] += gsum;
+    a.lam[0][c] = in0 ? ca[0] * L0 : L0;
+    a.lam[1][c] = in1 ? ca[1] * L1 : L1;
+    a.lam[2][c] = in2 ? ca[2] * L2 : L2;
+}
+
+// (D^T mu)[u] = c1 mu[u] - c1 mu[u+1] + c2 mu[u-1] - c2 mu[u+2]
+template <typename T>
+__device__ __forceinline__ T dminus_t(const T *__restrict__ mu, long long c, long long s, int v, int n, T c1, T c2) {
+    T r = c1 * mu[c];
+    if (v + 1 < n) r -= c1 * mu[c + s];
+    if (v >= 1) r += c2 * mu[c - s];
+    if (v + 2 < n) r -= c2 * mu[c + 2 * s];
+    return r;
+}
+
+template <typename T>
+__global__ void adj_e_gather_kernel(AdjArgs<T> a) {
+    int i, j, k, shot;
+    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i;
+    const long long sy = a.px, sz = a.plane;
+    const T c1 = a.c1, c2 = a.c2;
+    const T hz = dminus_t(a.mu[0], c, sy, j, a.ny, c1, c2) + dminus_t(a.mu[3], c, 1, i, a.nx, c1, c2);
+    const T hy = dminus_t(a.mu[1], c, sz, k, a.nz, c1, c2) + dminus_t(a.mu[4], c, 1, i, a.nx, c1, c2);
+    const T hx = dminus_t(a.mu[2], c, sz, k, a.nz, c1, c2) + dminus_t(a.mu[5], c, sy, j, a.ny, c1, c2);
+    a.lam[3][c] += hx;
+    a.lam[4][c] += hy;
+    a.lam[5][c] += hz;
+}
+
+// ---------------------------------------------------------------- sources
+// Adjoint sources a[shot][rec][n] = sum_f Re(conj(R[shot][rec][f]) W_rf[n]),
+// W_rf[n] = hf dt exp((i-1) sqrt(w0 w_f) n dt) with the H factor on H receivers.
+__global__ void adj_source_kernel(const double2 *__restrict__ R, int ntr, int nrec, int nf, int nt,
+                                  const double *__restrict__ omega, double dt, double omega0,
+                                  const unsigned char *__restrict__ is_h, int hfac, double *__restrict__ out) {
+    const long long tot = (long long)ntr * nt;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(e / nt), n = (int)(e - (long long)t * nt);
+        const bool h = hfac && is_h[t % nrec];
+        double acc = 0.0;
+        for (int f = 0; f < nf; f++) {
+            const double xa = sqrt(omega0 * omega[f]) * (double)n * dt;
+            double s, cs;
+            sincos(xa, &s, &cs);
+            const double e0 = exp(-xa) * dt;
+            double wr = e0 * cs, wi = e0 * s;
+            if (h) {
+                const double r = sqrt(2.0 * omega0 / omega[f]) * 0.70710678118654752440;
+                const double a2 = wr * r - wi * r, b2 = wr * r + wi * r;
+                wr = a2;
+                wi = b2;
+            }
+            const double2 res = R[(long long)t * nf + f];
+            acc += res.x * wr + res.y * wi;  // Re(conj(res) * w)
+        }
+        out[e] = acc;
+    }
+}
+
+// Adds a[shot][rec][n] to the adjoint field of each receiver of one kind (E or H).
+template <typename T>
+__global__ void adj_inject_kernel(T *lam0, T *lam1, T *lam2, T *lam3, T *lam4, T *lam5, const long long *rec_off,
+                                  const int *rec_comp, int nrec, int nshot, long long fshot, const double *asrc,
+                                  int nt, int n, int want_h) {
+    T *lam[6] = {lam0, lam1, lam2, lam3, lam4, lam5};
+    const int tot = nrec * nshot;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int s = q / nrec, r = q % nrec;
+        const int cpt = rec_comp[r];
+        if ((cpt >= 3) != (want_h != 0)) continue;
+        atomicAdd(lam[cpt] + (long long)s * fshot + rec_off[r], (T)asrc[(long long)q * nt + n]);
+    }
+}
+
+struct AdjSrc {
+    long long off;   // cell offset within the shot (padded layout)
+    long long moff;  // model offset of the cell
+    int shot, comp, kind, i, j, k;
+    double g;        // gain (as SrcPoint::g)
+};
+
+// Source terms of adjoint step n for one kind of point:
+//  magnetic (run before the H own kernel, lambda_H is lambda of H after the H phase):
+//    the H own kernel used the stored H (before the magnetic injection) as H0; the
+//    injection changed H0 by -g w[n+1]: add lambda (d term/d H0) (-g w[n+1]).
+//  electric (run before the E own kernel, lambda_E is lambda of E1s):
+//    sigma in the gain: + lambda g wbar / sigma, and the E own kernel used E1s as
+//    E1 = E1s + g wbar: add lambda (dcb/cb) g wbar.
+template <typename T>
+__global__ void adj_src_kernel(AdjArgs<T> a, const AdjSrc *__restrict__ pts, int npts, const double *__restrict__ wave,
+                               int n, int kind, int shot0, int shot1) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npts) return;
+    const AdjSrc p = pts[q];
+    if (p.kind != kind || p.shot < shot0 || p.shot >= shot1) return;
+    const long long c = (long long)(p.shot - shot0) * a.fshot + p.off;
+    const double m = (double)a.m[p.moff];
+    const double isig = m * a.inv2w0dt;
+    if (kind == 0) {
+        if (p.comp < 3) return;
+        const int ax = p.comp - 3;
+        const int v = ax == 0 ? p.i : (ax == 1 ? p.j : p.k);
+        const double msh = (double)pget(a, ax, 1, v);
+        if (msh == 0.0) return;
+        const double h = msh * m;
+        const double da = (1.0 - h) / (1.0 + h);
+        const double dda = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
+        const double rdb = h * isig / (1.0 + h);
+        const bool in = in_box(a.upd[ax], p.i, p.j, p.k);
+        const double dterm = in ? dda - rdb * da : -rdb;
+        const double L = (double)a.lam[p.comp][c];
+        atomicAdd(a.grad + c, L * dterm * (-p.g * wave[n + 1]));
+    } else {
+        if (p.comp > 2) return;
+        const int ax = p.comp;
+        const int v = ax == 0 ? p.i : (ax == 1 ? p.j : p.k);
+        const double esh = (double)pget(a, ax, 0, v);
+        const double h = esh * m;
+        const double rcb = -isig / (1.0 + h);
+        const double wbar = (wave[n] + wave[n + 1]) / 2.0;
+        const double L = (double)a.lam[p.comp][c];
+        atomicAdd(a.grad + c, L * (p.g * wbar * isig + rcb * p.g * wbar));
+    }
+}
+
+// Copies the six field arrays of a group of shots into one history slot.
+template <typename T>
+__global__ void copy_state_kernel(const T *f0, const T *f1, const T *f2, const T *f3, const T *f4, const T *f5,
+                                  T *dst, long long len) {
+    const T *src[6] = {f0, f1, f2, f3, f4, f5};
+    for (int c = 0; c < 6; c++)
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x)
+            dst[c * len + e] = src[c][e];
+}
+
+// grad_out[cell] = sum over shots of grad[shot][cell], zero outside the frame
+// [ncpml, n-ncpml) on every axis (satan_i calc_gamma, fwi3d_cpu_function_v1.4.c:2359-2361).
+__global__ void grad_reduce_kernel(const double *__restrict__ g, int nshot, long long fshot, int nx, int ny, int nz,
+                                   int px, long long plane, int ncpml, double *__restrict__ out) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % nx);
+        const int j = (int)((e / nx) % ny);
+        const int k = (int)(e / ((long long)nx * ny));
+        double s = 0.0;
+        if (i >= ncpml && i < nx - ncpml && j >= ncpml && j < ny - ncpml && k >= ncpml && k < nz - ncpml) {
+            const long long c = (long long)k * plane + (long long)j * px + i;
+            for (int q = 0; q < nshot; q++) s += g[(long long)q * fshot + c];
+        }
+        out[e] = s;
+    }
+}
+
+// residual R = S - obs and misfit 0.5 sum |R|^2 (one block reduction per launch, atomically added)
+__global__ void residual_kernel(const double2 *__restrict__ S, const double2 *__restrict__ obs, long long n,
+                                double2 *__restrict__ R, double *misfit) {
+    double acc = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double2 r = make_double2(S[e].x - obs[e].x, S[e].y - obs[e].y);
+        R[e] = r;
+        acc += 0.5 * (r.x * r.x + r.y * r.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(misfit, acc);
+}
+
+}  // namespace mittet

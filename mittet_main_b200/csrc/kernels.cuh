@@ -221,16 +221,24 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 // accumulators:
 //   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring[s][vc][shot][cell],
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
-// One thread per (component, shot, cell).  Ring values are loaded 16 at a
-// time before any arithmetic (16 loads in flight per thread); accumulators of
-// up to 8 frequencies stay in registers; the weights sit in shared memory.
+// One thread per (component, shot, cell).  The sum over the ring is formed in
+// the field precision T (at most 32 terms; for FP32 fields the partial sum
+// carries ~1e-7 relative error) and added to the FP64 accumulator once per
+// flush.  Ring values are loaded 16 at a time before any arithmetic; the
+// weights of the flush sit in shared memory.
 template <typename T>
-__global__ void __launch_bounds__(256, 2) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int nvc,
+__global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int nvc,
                                                          int3 vcs, long long fshot, int cnt, int n0,
                                                          const double2 *__restrict__ wt, int nf,
                                                          double2 *__restrict__ acc) {
-    extern __shared__ double2 sw[];  // [cnt][nf]
-    for (int q = threadIdx.x; q < cnt * nf; q += blockDim.x) sw[q] = wt[(long long)n0 * nf + q];
+    extern __shared__ unsigned char sw_raw[];
+    T *swr = reinterpret_cast<T *>(sw_raw);  // [cnt][nf] real parts
+    T *swi = swr + cnt * nf;                 // [cnt][nf] imaginary parts
+    for (int q = threadIdx.x; q < cnt * nf; q += blockDim.x) {
+        const double2 w = wt[(long long)n0 * nf + q];
+        swr[q] = (T)w.x;
+        swi[q] = (T)w.y;
+    }
     __syncthreads();
     const long long tot = ring_comp * nvc;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < tot; g += (long long)gridDim.x * blockDim.x) {
@@ -243,12 +251,9 @@ __global__ void __launch_bounds__(256, 2) volume_dft_kernel(const T *__restrict_
         const T *__restrict__ rp = ring + (long long)vc * ring_comp + e;
         for (int f0 = 0; f0 < nf; f0 += 8) {
             const int fn = min(8, nf - f0);
-            double ar[8], ai[8];
+            T pr[8], pi[8];
 #pragma unroll
-            for (int f = 0; f < 8; f++) {
-                if (f < fn) { const double2 v = ap[(long long)(f0 + f) * fshot]; ar[f] = v.x; ai[f] = v.y; }
-                else { ar[f] = 0.0; ai[f] = 0.0; }
-            }
+            for (int f = 0; f < 8; f++) { pr[f] = T(0); pi[f] = T(0); }
             for (int s0 = 0; s0 < cnt; s0 += 16) {
                 T xs[16];
 #pragma unroll
@@ -257,17 +262,22 @@ __global__ void __launch_bounds__(256, 2) volume_dft_kernel(const T *__restrict_
 #pragma unroll
                 for (int s = 0; s < 16; s++) {
                     if (s0 + s < cnt) {
-                        const double x = (double)xs[s];
-                        const double2 *w = sw + (s0 + s) * nf + f0;
+                        const T *wr = swr + (s0 + s) * nf + f0;
+                        const T *wi = swi + (s0 + s) * nf + f0;
 #pragma unroll
                         for (int f = 0; f < 8; f++)
-                            if (f < fn) { ar[f] = fma(w[f].x, x, ar[f]); ai[f] = fma(w[f].y, x, ai[f]); }
+                            if (f < fn) { pr[f] = fma(wr[f], xs[s], pr[f]); pi[f] = fma(wi[f], xs[s], pi[f]); }
                     }
                 }
             }
 #pragma unroll
             for (int f = 0; f < 8; f++)
-                if (f < fn) ap[(long long)(f0 + f) * fshot] = make_double2(ar[f], ai[f]);
+                if (f < fn) {
+                    double2 v = ap[(long long)(f0 + f) * fshot];
+                    v.x += (double)pr[f];
+                    v.y += (double)pi[f];
+                    ap[(long long)(f0 + f) * fshot] = v;
+                }
         }
     }
 }

@@ -23,6 +23,7 @@
 
 #include "../../include/mittet.h"
 #include "kernels.cuh"
+#include "adjoint.cuh"
 #include "setup_host.h"
 
 using namespace mittet;
@@ -454,7 +455,7 @@ void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
     for (int c = 0; c < 3; c++)
         if (h->vmask >> c & 1) vc[nvc++] = c;
     int blocks = (int)std::min<long long>((tot * nvc + 255) / 256, 148LL * 16);
-    volume_dft_kernel<T><<<blocks, 256, (size_t)cnt * nf * sizeof(double2), h->st>>>(
+    volume_dft_kernel<T><<<blocks, 256, (size_t)cnt * nf * 2 * sizeof(T), h->st>>>(
         h->ring.as<T>(), tot, nvc, make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, n0, h->wtab.as<double2>(), nf,
         h->acc.as<double2>());
     h->launches++;
@@ -653,6 +654,18 @@ int time_kernels(mittet_handle *h, int nsteps, double *ms) {
     return MITTET_OK;
 }
 
+
+// ------------------------------------------------------------------ gradient
+// Forward (receiver spectra, misfit) -> adjoint sources -> per group of shots:
+// forward pass keeping a checkpoint every K steps, then segments in reverse:
+// recompute the segment's K states from its checkpoint into a history
+// buffer and run the adjoint steps over it.  Shot groups are sized so the
+// history fits in a share of the free device memory.
+template <typename T>
+int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double *misfit_out, double *grad_out);
+
+int validate_ready(mittet_handle *h, int nt);
+
 int validate_ready(mittet_handle *h, int nt) {
     if (!h->has_model) return fail(MITTET_ERR_STATE, "mittet_set_model has not been called");
     if (h->nshot <= 0) return fail(MITTET_ERR_STATE, "mittet_set_sources has not been called");
@@ -688,6 +701,271 @@ int upload_sources(mittet_handle *h) {
     CK(cudaStreamSynchronize(h->st));
     h->npts = (int)dp.size();
     drop_graph(h);
+    return MITTET_OK;
+}
+
+template <typename T>
+int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double *misfit_out, double *grad_out) {
+    const int ns = h->nshot, nrec = h->nrec, nf = (int)h->omega.size();
+    const uint32_t vmask_saved = h->vmask;
+    if (h->vmask) { h->vmask = 0; drop_graph(h); }
+    int rc = run_forward<T>(h, nt);
+    h->vmask = vmask_saved;
+    if (vmask_saved) drop_graph(h);
+    if (rc) return rc;
+    const size_t nspec = (size_t)ns * nrec * nf;
+    DevBuf d_obs, d_R, d_mis, d_asrc;
+    CK(d_obs.ensure(nspec * sizeof(double2)));
+    CK(d_R.ensure(nspec * sizeof(double2)));
+    CK(d_mis.ensure(sizeof(double)));
+    CK(d_asrc.ensure((size_t)ns * nrec * nt * sizeof(double)));
+    CK(cudaMemcpyAsync(d_obs.p, obs_host, nspec * sizeof(double2), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemsetAsync(d_mis.p, 0, sizeof(double), h->st));
+    residual_kernel<<<64, 256, 0, h->st>>>(h->spectra.as<double2>(), d_obs.as<double2>(), (long long)nspec,
+                                           d_R.as<double2>(), d_mis.as<double>());
+    adj_source_kernel<<<256, 256, 0, h->st>>>(d_R.as<double2>(), ns * nrec, nrec, nf, nt, h->d_omega.as<double>(),
+                                              h->ph.dt, h->ph.omega0, h->rec_is_h.as<unsigned char>(), h->hfac,
+                                              d_asrc.as<double>());
+    CK(cudaGetLastError());
+    double mis = 0.0;
+    CK(cudaMemcpyAsync(&mis, d_mis.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    *misfit_out = mis;
+
+    // source points, absolute shots
+    const double vol = h->g.dx * h->g.dy * h->g.dz;
+    std::vector<AdjSrc> asp(h->pts.size());
+    for (size_t q = 0; q < h->pts.size(); q++) {
+        const mittet_point_source &p = h->pts[q];
+        const size_t c0 = ((size_t)(p.iz - 1) * h->g.ny + (p.iy - 1)) * h->g.nx + (p.ix - 1);
+        AdjSrc &a = asp[q];
+        a.off = ((long long)(p.iz - 1) * h->g.ny + (p.iy - 1)) * h->px + (p.ix - 1);
+        a.moff = a.off;
+        a.shot = p.shot; a.comp = p.comp; a.kind = p.kind;
+        a.i = p.ix - 1; a.j = p.iy - 1; a.k = p.iz - 1;
+        a.g = p.kind == MITTET_SRC_MAGNETIC ? p.amp * h->ph.dt / (h->mu_h.empty() ? h->ph.mu0 : h->mu_h[c0]) / vol
+                                            : p.amp * h->ph.dt * 2.0 * h->ph.omega0 / h->sigma_h[c0] / vol;
+    }
+    DevBuf d_asp;
+    CK(d_asp.ensure(std::max<size_t>(asp.size(), 1) * sizeof(AdjSrc)));
+    CK(cudaMemcpyAsync(d_asp.p, asp.data(), asp.size() * sizeof(AdjSrc), cudaMemcpyHostToDevice, h->st));
+
+    // group size from memory
+    size_t psiE = 0, psiH = 0;
+    for (int a = 0; a < 3; a++) { psiE += 2 * psi_elems(h, h->su.se[a], a); psiH += 2 * psi_elems(h, h->su.sh[a], a); }
+    const int ncheck = (nt + K - 1) / K;
+    const size_t F = (size_t)h->fshot;
+    const size_t per_shot = h->esz * ((size_t)(K + 1) * 6 * F + (size_t)ncheck * (6 * F + psiE + psiH) + 6 * F +
+                                      psiE + psiH + 6 * F + psiE + psiH + 7 * F) + 8 * F;
+    size_t freeb = 0, totb = 0;
+    CK(cudaMemGetInfo(&freeb, &totb));
+    const size_t budget = (size_t)(0.75 * (double)freeb);
+    int G = (int)std::min<size_t>((size_t)ns, std::max<size_t>(1, budget / std::max<size_t>(per_shot, 1)));
+    if ((size_t)G * per_shot > budget) return fail(MITTET_ERR_OOM, "one shot of the gradient needs %zu bytes, %zu free", per_shot, freeb);
+
+    DevBuf fl[6], pe[3][2], pH[3][2], hist, ck, lam[6], lpe[3][2], lph[3][2], mu[7], gacc, gred, d_gsrc;
+    const size_t gF = (size_t)G * F;
+    for (int c = 0; c < 6; c++) { CK(fl[c].ensure(gF * h->esz)); CK(lam[c].ensure(gF * h->esz)); }
+    for (int c = 0; c < 7; c++) CK(mu[c].ensure(gF * h->esz));
+    for (int a = 0; a < 3; a++)
+        for (int w = 0; w < 2; w++) {
+            const size_t ne = (size_t)G * psi_elems(h, h->su.se[a], a), nh = (size_t)G * psi_elems(h, h->su.sh[a], a);
+            CK(pe[a][w].ensure(ne * h->esz)); CK(pH[a][w].ensure(nh * h->esz));
+            CK(lpe[a][w].ensure(ne * h->esz)); CK(lph[a][w].ensure(nh * h->esz));
+        }
+    CK(hist.ensure((size_t)(K + 1) * 6 * gF * h->esz));
+    const size_t ck_stride = (6 * F + psiE + psiH) * (size_t)G * h->esz;
+    CK(ck.ensure((size_t)ncheck * ck_stride));
+    CK(gacc.ensure(gF * sizeof(double)));
+    const size_t ncell = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    CK(gred.ensure(ncell * sizeof(double)));
+    std::vector<double> gsum(ncell, 0.0), gpart(ncell);
+    for (int c = 0; c < 7; c++) CK(cudaMemsetAsync(mu[c].p, 0, gF * h->esz, h->st));
+
+    const int ns_saved = h->nshot;
+    const int vmask_keep = (int)h->vmask;
+    h->vmask = 0;
+    for (int s0 = 0; s0 < ns; s0 += G) {
+        const int s1 = std::min(ns, s0 + G), Gg = s1 - s0;
+        h->nshot = Gg;
+        // group-local source list for the forward injection
+        std::vector<SrcPoint> gp;
+        for (size_t q = 0; q < h->pts.size(); q++) {
+            const mittet_point_source &p = h->pts[q];
+            if (p.shot < s0 || p.shot >= s1) continue;
+            SrcPoint sp;
+            sp.off = (long long)(p.shot - s0) * h->fshot + asp[q].off;
+            sp.comp = p.comp;
+            sp.kind = p.kind;
+            sp.g = asp[q].g;
+            gp.push_back(sp);
+        }
+        DevBuf d_gp;
+        CK(d_gp.ensure(std::max<size_t>(gp.size(), 1) * sizeof(SrcPoint)));
+        CK(cudaMemcpyAsync(d_gp.p, gp.data(), gp.size() * sizeof(SrcPoint), cudaMemcpyHostToDevice, h->st));
+        PhaseArgs<T> ea = phase_args<T>(h, true), ha = phase_args<T>(h, false);
+        for (int c = 0; c < 6; c++) { ea.f[c] = fl[c].as<T>(); ha.f[c] = fl[c].as<T>(); }
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 2; w++) { ea.psi[a][w] = pe[a][w].as<T>(); ha.psi[a][w] = pH[a][w].as<T>(); }
+        ea.ring_k = 0;
+        InjectArgs<T> ia;
+        memset(&ia, 0, sizeof(ia));
+        for (int c = 0; c < 6; c++) ia.f[c] = fl[c].as<T>();
+        ia.pts = d_gp.as<SrcPoint>();
+        ia.npts = (int)gp.size();
+        ia.wave = h->wave.as<double>();
+        ia.d_step = h->d_step.as<int>();
+        InjectArgs<T> ia_m = ia, ia_e = ia;
+        ia_m.kind = 0;
+        ia_e.kind = 1;
+        SampleArgs<T> sa;
+        memset(&sa, 0, sizeof(sa));
+        for (int c = 0; c < 6; c++) sa.f[c] = fl[c].as<T>();
+        sa.nrec = 0;
+        sa.nshot = Gg;
+        sa.fshot = h->fshot;
+        sa.traces = h->traces.as<T>();
+        sa.nt = nt;
+        sa.d_step = h->d_step.as<int>();
+        bool hm = false, he = false;
+        for (const auto &q : gp) { hm |= q.kind == 0; he |= q.kind == 1; }
+        const bool mag0 = h->has_mag, ele0 = h->has_ele;
+        h->has_mag = hm;
+        h->has_ele = he;
+        auto save_state = [&](char *dst) -> int {
+            size_t o = 0;
+            for (int c = 0; c < 6; c++) { CK(cudaMemcpyAsync(dst + o, fl[c].p, (size_t)Gg * F * h->esz, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * F * h->esz; }
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 2; w++) {
+                    const size_t ne = (size_t)Gg * psi_elems(h, h->su.se[a], a) * h->esz, nh = (size_t)Gg * psi_elems(h, h->su.sh[a], a) * h->esz;
+                    CK(cudaMemcpyAsync(dst + o, pe[a][w].p, ne, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * psi_elems(h, h->su.se[a], a) * h->esz;
+                    CK(cudaMemcpyAsync(dst + o, pH[a][w].p, nh, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * psi_elems(h, h->su.sh[a], a) * h->esz;
+                }
+            return MITTET_OK;
+        };
+        auto load_state = [&](const char *src) -> int {
+            size_t o = 0;
+            for (int c = 0; c < 6; c++) { CK(cudaMemcpyAsync(fl[c].p, src + o, (size_t)Gg * F * h->esz, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * F * h->esz; }
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 2; w++) {
+                    const size_t ne = (size_t)Gg * psi_elems(h, h->su.se[a], a) * h->esz, nh = (size_t)Gg * psi_elems(h, h->su.sh[a], a) * h->esz;
+                    CK(cudaMemcpyAsync(pe[a][w].p, src + o, ne, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * psi_elems(h, h->su.se[a], a) * h->esz;
+                    CK(cudaMemcpyAsync(pH[a][w].p, src + o, nh, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * psi_elems(h, h->su.sh[a], a) * h->esz;
+                }
+            return MITTET_OK;
+        };
+        auto set_step = [&](int n) -> int {
+            CK(cudaMemcpyAsync(h->d_step.p, &n, sizeof(int), cudaMemcpyHostToDevice, h->st));
+            CK(cudaStreamSynchronize(h->st));  // n lives on the host stack
+            return MITTET_OK;
+        };
+        auto fwd_step = [&]() {
+            if (h->has_mag) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m);
+            launch_phase<T>(h, true, h->var_e, ea);
+            if (h->has_ele) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e);
+            launch_phase<T>(h, false, h->var_h, ha);
+            sample_kernel<T><<<1, 32, 0, h->st>>>(sa);
+        };
+        // forward pass with checkpoints
+        for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(fl[c].p, 0, gF * h->esz, h->st));
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 2; w++) {
+                CK(cudaMemsetAsync(pe[a][w].p, 0, (size_t)G * psi_elems(h, h->su.se[a], a) * h->esz, h->st));
+                CK(cudaMemsetAsync(pH[a][w].p, 0, (size_t)G * psi_elems(h, h->su.sh[a], a) * h->esz, h->st));
+            }
+        if ((rc = set_step(0))) return rc;
+        for (int n = 0; n < nt; n++) {
+            if (n % K == 0 && (rc = save_state(ck.as<char>() + (size_t)(n / K) * ck_stride))) return rc;
+            fwd_step();
+        }
+        CK(cudaGetLastError());
+        // adjoint
+        for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(lam[c].p, 0, gF * h->esz, h->st));
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 2; w++) {
+                CK(cudaMemsetAsync(lpe[a][w].p, 0, (size_t)G * psi_elems(h, h->su.se[a], a) * h->esz, h->st));
+                CK(cudaMemsetAsync(lph[a][w].p, 0, (size_t)G * psi_elems(h, h->su.sh[a], a) * h->esz, h->st));
+            }
+        CK(cudaMemsetAsync(gacc.p, 0, gF * sizeof(double), h->st));
+        AdjArgs<T> aa;
+        memset(&aa, 0, sizeof(aa));
+        aa.m = h->m.as<T>();
+        aa.dtmu = h->has_mu ? h->dtmu.as<T>() : nullptr;
+        aa.dtmu0 = (T)(h->ph.dt / h->ph.mu0);
+        aa.prof = h->prof.as<T>();
+        aa.nmax = h->su.nmax;
+        aa.nx = h->g.nx; aa.ny = h->g.ny; aa.nz = h->g.nz; aa.px = h->px;
+        aa.plane = h->plane; aa.fshot = h->fshot;
+        aa.c1 = (T)h->ph.c1; aa.c2 = (T)h->ph.c2; aa.c2t = (T)(h->ph.psi_hyx_typo ? h->ph.c2 : h->ph.c1);
+        aa.inv2w0dt = 1.0 / (2.0 * h->ph.omega0 * h->ph.dt);
+        for (int c = 0; c < 6; c++) aa.lam[c] = lam[c].as<T>();
+        aa.grad = gacc.as<double>();
+        AdjArgs<T> ah = aa, ae = aa;
+        for (int ax = 0; ax < 3; ax++) {
+            ah.pshot[ax] = (long long)psi_elems(h, h->su.sh[ax], ax);
+            ae.pshot[ax] = (long long)psi_elems(h, h->su.se[ax], ax);
+            ah.slab[ax] = to_dslab(h->su.sh[ax]);
+            ae.slab[ax] = to_dslab(h->su.se[ax]);
+            ah.upd[ax] = to_dbox(h->su.upd[3 + ax]);
+            ae.upd[ax] = to_dbox(h->su.upd[ax]);
+            for (int w = 0; w < 2; w++) { ah.lpsi[ax][w] = lph[ax][w].as<T>(); ae.lpsi[ax][w] = lpe[ax][w].as<T>(); }
+        }
+        ah.sgn = (T)h->ph.h_sign;
+        ae.sgn = (T)h->ph.e_sign;
+        for (int c = 0; c < 7; c++) { ah.mu[c] = mu[c].as<T>(); ae.mu[c] = mu[c].as<T>(); }
+        const dim3 ablk(32, 8), agrd((h->g.nx + 31) / 32, (h->g.ny + 7) / 8, h->g.nz * Gg);
+        const T *H = hist.as<T>();
+        const size_t slot = 6 * gF;
+        for (int seg = ncheck - 1; seg >= 0; seg--) {
+            const int n0 = seg * K, n1 = std::min(nt, n0 + K);
+            if ((rc = load_state(ck.as<char>() + (size_t)seg * ck_stride))) return rc;
+            if ((rc = set_step(n0))) return rc;
+            copy_state_kernel<T><<<512, 256, 0, h->st>>>(fl[0].as<T>(), fl[1].as<T>(), fl[2].as<T>(), fl[3].as<T>(),
+                                                         fl[4].as<T>(), fl[5].as<T>(), hist.as<T>(), (long long)gF);
+            for (int q = 0; q < n1 - n0; q++) {
+                fwd_step();
+                copy_state_kernel<T><<<512, 256, 0, h->st>>>(fl[0].as<T>(), fl[1].as<T>(), fl[2].as<T>(),
+                                                             fl[3].as<T>(), fl[4].as<T>(), fl[5].as<T>(),
+                                                             hist.as<T>() + (size_t)(q + 1) * slot, (long long)gF);
+            }
+            CK(cudaGetLastError());
+            for (int n = n1 - 1; n >= n0; n--) {
+                const int q = n - n0;
+                for (int c = 0; c < 3; c++) {
+                    ah.E0[c] = ae.E0[c] = H + (size_t)q * slot + c * gF;
+                    ah.H0[c] = ae.H0[c] = H + (size_t)q * slot + (3 + c) * gF;
+                    ah.E1[c] = ae.E1[c] = H + (size_t)(q + 1) * slot + c * gF;
+                    ah.H1[c] = ae.H1[c] = H + (size_t)(q + 1) * slot + (3 + c) * gF;
+                }
+                const double *asrc = d_asrc.as<double>() + (size_t)s0 * nrec * nt;
+                adj_inject_kernel<T><<<4, 256, 0, h->st>>>(aa.lam[0], aa.lam[1], aa.lam[2], aa.lam[3], aa.lam[4],
+                                                          aa.lam[5], h->rec_off.as<long long>(), h->rec_comp.as<int>(),
+                                                          nrec, Gg, h->fshot, asrc, nt, n, 1);
+                if (hm) adj_src_kernel<T><<<(int)(asp.size() + 63) / 64, 64, 0, h->st>>>(ah, d_asp.as<AdjSrc>(), (int)asp.size(), h->wave.as<double>(), n, 0, s0, s1);
+                adj_h_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
+                adj_h_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
+                adj_inject_kernel<T><<<4, 256, 0, h->st>>>(aa.lam[0], aa.lam[1], aa.lam[2], aa.lam[3], aa.lam[4],
+                                                          aa.lam[5], h->rec_off.as<long long>(), h->rec_comp.as<int>(),
+                                                          nrec, Gg, h->fshot, asrc, nt, n, 0);
+                if (he) adj_src_kernel<T><<<(int)(asp.size() + 63) / 64, 64, 0, h->st>>>(ae, d_asp.as<AdjSrc>(), (int)asp.size(), h->wave.as<double>(), n, 1, s0, s1);
+                adj_e_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
+                adj_e_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
+            }
+            CK(cudaGetLastError());
+        }
+        h->has_mag = mag0;
+        h->has_ele = ele0;
+        grad_reduce_kernel<<<512, 256, 0, h->st>>>(gacc.as<double>(), Gg, h->fshot, h->g.nx, h->g.ny, h->g.nz, h->px,
+                                                   h->plane, h->g.ncpml, gred.as<double>());
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(gpart.data(), gred.p, ncell * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        for (size_t e = 0; e < ncell; e++) gsum[e] += gpart[e];
+    }
+    h->nshot = ns_saved;
+    h->vmask = (uint32_t)vmask_keep;
+    drop_graph(h);
+    memcpy(grad_out, gsum.data(), ncell * sizeof(double));
     return MITTET_OK;
 }
 
@@ -1199,9 +1477,19 @@ int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms) {
 
 int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t checkpoint_every, double *misfit,
                     double *grad) {
-    (void)nt; (void)obs; (void)checkpoint_every; (void)misfit; (void)grad;
-    if (!h) return fail(MITTET_ERR_INVALID_ARG, "null handle");
-    return fail(MITTET_ERR_STATE, "gradient is not available in this build");
+    if (!h || !obs || !misfit || !grad) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    int rc = validate_ready(h, nt);
+    if (rc) return rc;
+    if (h->nrec <= 0 || h->omega.empty()) return fail(MITTET_ERR_STATE, "the gradient needs receivers and frequencies");
+    for (double w : h->omega)
+        if (!(w > 0)) return fail(MITTET_ERR_INVALID_ARG, "gradient frequencies must be positive");
+    for (const auto &p : h->pts)
+        if ((p.kind == MITTET_SRC_ELECTRIC) != (p.comp < 3))
+            return fail(MITTET_ERR_INVALID_ARG, "gradient supports electric points on E and magnetic points on H");
+    const int K = checkpoint_every > 0 ? checkpoint_every : 200;
+    rc = set_device(h);
+    if (rc) return rc;
+    return h->fp64 ? run_gradient<double>(h, nt, obs, K, misfit, grad) : run_gradient<float>(h, nt, obs, K, misfit, grad);
 }
 
 }  // extern "C"

@@ -493,3 +493,282 @@ void orc_dft(int nt, double dt, double omega0, const double *x, int nf, const do
         out[2 * f + 1] = cimag(acc);
     }
 }
+
+/* ======================================================================
+ * Discrete adjoint gradient d(misfit)/d(sigma) of one shot.
+ *
+ * No counterpart in the reference (satan_i forms its gradient from
+ * frequency-domain reciprocity fields, satan_i/fwi3d_cpu_function_v1.4.c:
+ * 2246-2384); this is the exact derivative of the restated forward path
+ * above, written here in scatter form (each forward operation's transpose
+ * applied in reverse order) to check the GPU's gather-form adjoint.
+ *
+ *   misfit = 1/2 sum_{r,f} |S_rf - obs_rf|^2,  S_rf = sum_n d_r[n] W_rf[n],
+ *   W_rf[n] = hf_r(f) dt exp((i-1) sqrt(w0 w_f) n dt),
+ *   hf = sqrt(-2 w0/(i w)) for H receivers when hfac, else 1.
+ * Adjoint source at receiver r, step n: a_r[n] = Re(conj(S_rf - obs_rf) W_rf[n]).
+ * sigma enters through ca, cb (every cell), da, db (CPML cells only) and the
+ * electric source gain; the gradient is returned for every cell.
+ * ====================================================================== */
+
+static void dplus_t(double *lam, size_t c, size_t s, double c1, double c2, double mu) {
+    /* transpose of D+(F)[c] = c1 (F[c+s]-F[c]) + c2 (F[c+2s]-F[c-s]) */
+    lam[c + s] += c1 * mu; lam[c] -= c1 * mu; lam[c + 2 * s] += c2 * mu; lam[c - s] -= c2 * mu;
+}
+static void dtypo_t(double *lam, size_t c, size_t s, double c1, double c2, double c2t, double mu) {
+    /* transpose of c1 F[c+s] - c2t F[c] + c2 F[c+2s] - c2 F[c-s] */
+    lam[c + s] += c1 * mu; lam[c] -= c2t * mu; lam[c + 2 * s] += c2 * mu; lam[c - s] -= c2 * mu;
+}
+static void dminus_t(double *lam, size_t c, size_t s, double c1, double c2, double mu) {
+    /* transpose of D(F)[c] = c1 (F[c]-F[c-s]) + c2 (F[c+s]-F[c-2s]) */
+    lam[c] += c1 * mu; lam[c - s] -= c1 * mu; lam[c + s] += c2 * mu; lam[c - 2 * s] -= c2 * mu;
+}
+
+int orc_gradient(const orc_params *p, const double *sigma, const double *mu,
+                 int nsrc, const int64_t *src_cell, const int32_t *src_comp,
+                 const int32_t *src_kind, const double *src_amp,
+                 int nt, const double *wavelet,
+                 int nrec, const int64_t *rec_cell, const int32_t *rec_comp,
+                 int nf, const double *omega, int hfac, const double *obs,
+                 double *misfit, double *grad, double *spec) {
+    orc_state s;
+    memset(&s, 0, sizeof(s));
+    if (state_init(&s, p, sigma, mu)) { state_free(&s); return -1; }
+    const int nx = s.nx, ny = s.ny, nz = s.nz;
+    const size_t n = s.n, sx = 1, sy = (size_t)nx, sz = (size_t)nx * ny;
+    const double vol = p->dx * p->dy * p->dz;
+    double *hist = malloc(sizeof(double) * 6 * n * (size_t)(nt + 1));
+    double *tr = malloc(sizeof(double) * (size_t)nrec * nt);
+    if (!hist || !tr) { free(hist); free(tr); state_free(&s); return -1; }
+    memset(hist, 0, sizeof(double) * 6 * n);
+    /* forward, keeping every state (E, H after each step) */
+    for (int t = 0; t < nt; t++) {
+        for (int q = 0; q < nsrc; q++) {
+            if (src_kind[q] != SRC_MAGNETIC) continue;
+            int64_t c = src_cell[q];
+            s.f[src_comp[q]][c] = s.f[src_comp[q]][c] - src_amp[q] * wavelet[t + 1] * p->dt / mu[c] / p->dx / p->dy / p->dz;
+        }
+        e_phase(&s, p);
+        for (int q = 0; q < nsrc; q++) {
+            if (src_kind[q] != SRC_ELECTRIC) continue;
+            int64_t c = src_cell[q];
+            s.f[src_comp[q]][c] -= src_amp[q] * (wavelet[t] + wavelet[t + 1]) / 2.f * p->dt * 2.f * p->omega0 / sigma[c] / p->dx / p->dy / p->dz;
+        }
+        h_phase(&s, p);
+        for (int r = 0; r < nrec; r++) tr[(size_t)r * nt + t] = s.f[rec_comp[r]][rec_cell[r]];
+        for (int c = 0; c < 6; c++) memcpy(hist + ((size_t)(t + 1) * 6 + c) * n, s.f[c], n * sizeof(double));
+    }
+    /* spectra, residual, misfit, adjoint sources */
+    double complex *R = malloc(sizeof(double complex) * (size_t)nrec * nf);
+    double *asrc = malloc(sizeof(double) * (size_t)nrec * nt);
+    double J = 0.0;
+    for (int r = 0; r < nrec; r++) {
+        for (int f = 0; f < nf; f++) {
+            double complex hf = 1.0;
+            if (hfac && rec_comp[r] >= 3) hf = csqrt(-2.0 * p->omega0 / I / omega[f]);
+            const double sw = sqrt(p->omega0 * omega[f]);
+            double complex acc = 0.0;
+            for (int t = 0; t < nt; t++) acc += hf * (tr[(size_t)r * nt + t] * p->dt * cexp((I - 1.0) * sw * t * p->dt));
+            const double complex res = acc - (obs[2 * ((size_t)r * nf + f)] + I * obs[2 * ((size_t)r * nf + f) + 1]);
+            R[(size_t)r * nf + f] = res;
+            J += 0.5 * creal(res * conj(res));
+            if (spec) { spec[2 * ((size_t)r * nf + f)] = creal(acc); spec[2 * ((size_t)r * nf + f) + 1] = cimag(acc); }
+        }
+        for (int t = 0; t < nt; t++) {
+            double a = 0.0;
+            for (int f = 0; f < nf; f++) {
+                double complex hf = 1.0;
+                if (hfac && rec_comp[r] >= 3) hf = csqrt(-2.0 * p->omega0 / I / omega[f]);
+                const double sw = sqrt(p->omega0 * omega[f]);
+                const double complex W = hf * p->dt * cexp((I - 1.0) * sw * t * p->dt);
+                a += creal(conj(R[(size_t)r * nf + f]) * W);
+            }
+            asrc[(size_t)r * nt + t] = a;
+        }
+    }
+    *misfit = J;
+
+    /* adjoint sweep */
+    double *lam[6], *lpsE[6], *lpsH[6];
+    for (int c = 0; c < 6; c++) {
+        lam[c] = calloc(n, sizeof(double)); lpsE[c] = calloc(n, sizeof(double)); lpsH[c] = calloc(n, sizeof(double));
+    }
+    memset(grad, 0, n * sizeof(double));
+    double *H0 = malloc(sizeof(double) * 3 * n), *E1 = malloc(sizeof(double) * 3 * n);
+    const double c1 = p->c1, c2 = p->c2, c2t = p->psi_hyx_typo ? p->c2 : p->c1;
+    const double se = (double)p->e_sign, sh = (double)p->h_sign;
+    const double dt = p->dt;
+    for (int t = nt - 1; t >= 0; t--) {
+        const double *Eh0 = hist + ((size_t)t * 6) * n, *Hh0 = hist + ((size_t)t * 6 + 3) * n;
+        const double *Eh1 = hist + ((size_t)(t + 1) * 6) * n, *Hh1 = hist + ((size_t)(t + 1) * 6 + 3) * n;
+        /* forward states of this step: H before the H phase (magnetic injection applied),
+         * E after the E phase (electric injection undone) */
+        memcpy(H0, Hh0, sizeof(double) * 3 * n);
+        memcpy(E1, Eh1, sizeof(double) * 3 * n);
+        for (int q = 0; q < nsrc; q++) {
+            const int64_t c = src_cell[q];
+            if (src_kind[q] == SRC_MAGNETIC && src_comp[q] >= 3)
+                H0[(size_t)(src_comp[q] - 3) * n + c] -= src_amp[q] * wavelet[t + 1] * dt / mu[c] / p->dx / p->dy / p->dz;
+            if (src_kind[q] == SRC_ELECTRIC && src_comp[q] < 3)
+                E1[(size_t)src_comp[q] * n + c] += src_amp[q] * (wavelet[t] + wavelet[t + 1]) / 2.f * dt * 2.f * p->omega0 / sigma[c] / p->dx / p->dy / p->dz;
+        }
+        /* sampling adjoint */
+        for (int r = 0; r < nrec; r++) lam[rec_comp[r]][rec_cell[r]] += asrc[(size_t)r * nt + t];
+
+        /* ---- H phase transpose ---- */
+        double *lEx = lam[0], *lEy = lam[1], *lEz = lam[2], *lHx = lam[3], *lHy = lam[4], *lHz = lam[5];
+        /* gradient of the H phase (CPML cells): uses lam of H after the phase */
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const size_t c = IDX(i, j, k);
+                    const double w2 = 2.0 * p->omega0;
+                    const double ms[3] = {s.pr[0].msig[i], s.pr[1].msig[j], s.pr[2].msig[k]};
+                    for (int a = 0; a < 3; a++) {
+                        if (ms[a] == 0.0) continue;
+                        const double h = ms[a] * dt * p->omega0 / sigma[c];
+                        (void)w2;
+                        const double da = s.da[a][c];
+                        const double dda = 2.0 * h / (sigma[c] * (1.0 + h) * (1.0 + h));
+                        const double rdb = h / (sigma[c] * (1.0 + h));
+                        const int in = inbox(&s.upd[3 + a], i, j, k);
+                        const double h0 = H0[(size_t)a * n + c], h1 = Hh1[(size_t)a * n + c];
+                        grad[c] += lam[3 + a][c] * ((in ? dda * h0 : 0.0) + rdb * (h1 - (in ? da * h0 : h0)));
+                    }
+                }
+        /* z slabs, y slabs, x slabs (reverse of CPML_H4), then the main update */
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const size_t c = IDX(i, j, k);
+                    if (inslab(&s.sh[2], 2, i, j, k)) {
+                        const double bh = s.pr[2].bh[k], chd = s.pr[2].ch[k] / p->dz;
+                        const double lxz = lpsH[5][c] + s.db[0][c] * lHx[c];
+                        const double lyz = lpsH[4][c] - s.db[1][c] * lHy[c];
+                        lpsH[5][c] = bh * lxz; lpsH[4][c] = bh * lyz;
+                        dplus_t(lEy, c, sz, c1, c2, chd * lxz);
+                        dplus_t(lEx, c, sz, c1, c2, chd * lyz);
+                    }
+                    if (inslab(&s.sh[1], 1, i, j, k)) {
+                        const double bh = s.pr[1].bh[j], chd = s.pr[1].ch[j] / p->dy;
+                        const double lxy = lpsH[2][c] - s.db[0][c] * lHx[c];
+                        const double lzy = lpsH[3][c] + s.db[2][c] * lHz[c];
+                        lpsH[2][c] = bh * lxy; lpsH[3][c] = bh * lzy;
+                        dplus_t(lEz, c, sy, c1, c2, chd * lxy);
+                        dplus_t(lEx, c, sy, c1, c2, chd * lzy);
+                    }
+                    if (inslab(&s.sh[0], 0, i, j, k)) {
+                        const double bh = s.pr[0].bh[i], chd = s.pr[0].ch[i] / p->dx;
+                        const double lzx = lpsH[1][c] - s.db[2][c] * lHz[c];
+                        const double lyx = lpsH[0][c] + s.db[1][c] * lHy[c];
+                        lpsH[1][c] = bh * lzx; lpsH[0][c] = bh * lyx;
+                        dplus_t(lEy, c, sx, c1, c2, chd * lzx);
+                        dtypo_t(lEz, c, sx, c1, c2, c2t, chd * lyx);
+                    }
+                }
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const size_t c = IDX(i, j, k);
+                    const double iky = 1.0 / s.pr[1].khd[j], ikz = 1.0 / s.pr[2].khd[k], ikx = 1.0 / s.pr[0].khd[i];
+                    if (inbox(&s.upd[3], i, j, k)) {
+                        const double w = -sh * s.db[0][c] * lHx[c];
+                        dplus_t(lEz, c, sy, c1, c2, w * iky);
+                        dplus_t(lEy, c, sz, c1, c2, -w * ikz);
+                        lHx[c] *= s.da[0][c];
+                    }
+                    if (inbox(&s.upd[4], i, j, k)) {
+                        const double w = -sh * s.db[1][c] * lHy[c];
+                        dplus_t(lEx, c, sz, c1, c2, w * ikz);
+                        dplus_t(lEz, c, sx, c1, c2, -w * ikx);
+                        lHy[c] *= s.da[1][c];
+                    }
+                    if (inbox(&s.upd[5], i, j, k)) {
+                        const double w = -sh * s.db[2][c] * lHz[c];
+                        dplus_t(lEy, c, sx, c1, c2, w * ikx);
+                        dplus_t(lEx, c, sy, c1, c2, -w * iky);
+                        lHz[c] *= s.da[2][c];
+                    }
+                }
+        /* ---- electric source transpose: sigma enters through the gain ---- */
+        for (int q = 0; q < nsrc; q++) {
+            if (src_kind[q] != SRC_ELECTRIC) continue;
+            const int64_t c = src_cell[q];
+            const double g = src_amp[q] * (wavelet[t] + wavelet[t + 1]) / 2.0 * dt * 2.0 * p->omega0 / sigma[c] / vol;
+            grad[c] += lam[src_comp[q]][c] * g / sigma[c];
+        }
+        /* ---- E phase transpose ---- */
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const size_t c = IDX(i, j, k);
+                    const double es[3] = {s.pr[0].esig[i], s.pr[1].esig[j], s.pr[2].esig[k]};
+                    for (int a = 0; a < 3; a++) {
+                        const double h = es[a] * dt * p->omega0 / sigma[c];
+                        const double ca = s.ca[a][c];
+                        const double dca = 2.0 * h / (sigma[c] * (1.0 + h) * (1.0 + h));
+                        const double rcb = -1.0 / (sigma[c] * (1.0 + h));
+                        const int in = inbox(&s.upd[a], i, j, k);
+                        const double e0 = Eh0[(size_t)a * n + c], e1 = E1[(size_t)a * n + c];
+                        grad[c] += lam[a][c] * ((in ? dca * e0 : 0.0) + rcb * (e1 - (in ? ca * e0 : e0)));
+                    }
+                }
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const size_t c = IDX(i, j, k);
+                    if (inslab(&s.se[2], 2, i, j, k)) {
+                        const double be = s.pr[2].be[k], ced = s.pr[2].ce[k] / p->dz;
+                        const double lyz = lpsE[4][c] + s.cb[1][c] * lEy[c];
+                        const double lxz = lpsE[5][c] - s.cb[0][c] * lEx[c];
+                        lpsE[4][c] = be * lyz; lpsE[5][c] = be * lxz;
+                        dminus_t(lHx, c, sz, c1, c2, ced * lyz);
+                        dminus_t(lHy, c, sz, c1, c2, ced * lxz);
+                    }
+                    if (inslab(&s.se[1], 1, i, j, k)) {
+                        const double be = s.pr[1].be[j], ced = s.pr[1].ce[j] / p->dy;
+                        const double lxy = lpsE[2][c] + s.cb[0][c] * lEx[c];
+                        const double lzy = lpsE[3][c] - s.cb[2][c] * lEz[c];
+                        lpsE[2][c] = be * lxy; lpsE[3][c] = be * lzy;
+                        dminus_t(lHz, c, sy, c1, c2, ced * lxy);
+                        dminus_t(lHx, c, sy, c1, c2, ced * lzy);
+                    }
+                    if (inslab(&s.se[0], 0, i, j, k)) {
+                        const double be = s.pr[0].be[i], ced = s.pr[0].ce[i] / p->dx;
+                        const double lzx = lpsE[0][c] + s.cb[2][c] * lEz[c];
+                        const double lyx = lpsE[1][c] - s.cb[1][c] * lEy[c];
+                        lpsE[0][c] = be * lzx; lpsE[1][c] = be * lyx;
+                        dminus_t(lHy, c, sx, c1, c2, ced * lzx);
+                        dminus_t(lHz, c, sx, c1, c2, ced * lyx);
+                    }
+                }
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const size_t c = IDX(i, j, k);
+                    const double iky = 1.0 / s.pr[1].ked[j], ikz = 1.0 / s.pr[2].ked[k], ikx = 1.0 / s.pr[0].ked[i];
+                    if (inbox(&s.upd[0], i, j, k)) {
+                        const double w = se * s.cb[0][c] * lEx[c];
+                        dminus_t(lHz, c, sy, c1, c2, w * iky);
+                        dminus_t(lHy, c, sz, c1, c2, -w * ikz);
+                        lEx[c] *= s.ca[0][c];
+                    }
+                    if (inbox(&s.upd[1], i, j, k)) {
+                        const double w = se * s.cb[1][c] * lEy[c];
+                        dminus_t(lHx, c, sz, c1, c2, w * ikz);
+                        dminus_t(lHz, c, sx, c1, c2, -w * ikx);
+                        lEy[c] *= s.ca[1][c];
+                    }
+                    if (inbox(&s.upd[2], i, j, k)) {
+                        const double w = se * s.cb[2][c] * lEz[c];
+                        dminus_t(lHy, c, sx, c1, c2, w * ikx);
+                        dminus_t(lHx, c, sy, c1, c2, -w * iky);
+                        lEz[c] *= s.ca[2][c];
+                    }
+                }
+    }
+    for (int c = 0; c < 6; c++) { free(lam[c]); free(lpsE[c]); free(lpsH[c]); }
+    free(H0); free(E1); free(hist); free(tr); free(R); free(asrc);
+    state_free(&s);
+    return 0;
+}

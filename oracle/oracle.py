@@ -268,3 +268,56 @@ def time_oracle_steps(p: Params, sigma, mu, sources, wavelet, n_short=2, n_long=
         forward(p, sigma, mu, sources, wavelet, [], n)
         t.append(_time.perf_counter() - t0)
     return max(t[1] - t[0], 1e-9) / (n_long - n_short)
+
+
+def gradient(p: Params, sigma, mu, sources, wavelet, receivers, nt, omega, obs, h_factor=True):
+    """Discrete-adjoint gradient of one shot (oracle/mittet_oracle.c orc_gradient).
+    obs: [nrec, nf] complex.  Returns (misfit, grad [nz, ny, nx], spectra [nrec, nf])."""
+    L = lib()
+    if not hasattr(L, "_grad_sig"):
+        P = ctypes.POINTER
+        L.orc_gradient.argtypes = [
+            P(OrcParams), P(ctypes.c_double), P(ctypes.c_double),
+            ctypes.c_int, P(ctypes.c_int64), P(ctypes.c_int32), P(ctypes.c_int32), P(ctypes.c_double),
+            ctypes.c_int, P(ctypes.c_double),
+            ctypes.c_int, P(ctypes.c_int64), P(ctypes.c_int32),
+            ctypes.c_int, P(ctypes.c_double), ctypes.c_int, P(ctypes.c_double),
+            P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double)]
+        L.orc_gradient.restype = ctypes.c_int
+        L._grad_sig = True
+    sigma = np.ascontiguousarray(sigma, dtype=np.float64).reshape(-1)
+    mu = np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    wavelet = np.ascontiguousarray(wavelet, dtype=np.float64)
+    sc = np.array([cell_index(p, *s[:3]) for s in sources], dtype=np.int64)
+    sk = np.array([COMPS[s[3]] for s in sources], dtype=np.int32)
+    sd = np.array([s[4] for s in sources], dtype=np.int32)
+    sa = np.array([s[5] for s in sources], dtype=np.float64)
+    rc = np.array([cell_index(p, *r[:3]) for r in receivers], dtype=np.int64)
+    rk = np.array([COMPS[r[3]] for r in receivers], dtype=np.int32)
+    om = np.ascontiguousarray(omega, dtype=np.float64)
+    ob = np.zeros((len(receivers), om.size, 2))
+    ob[..., 0] = np.real(obs)
+    ob[..., 1] = np.imag(obs)
+    mis = np.zeros(1)
+    g = np.zeros(sigma.size)
+    spec = np.zeros((len(receivers), om.size, 2))
+    cp = p.to_c()
+    r = L.orc_gradient(ctypes.byref(cp), _ptr(sigma, ctypes.c_double), _ptr(mu, ctypes.c_double),
+                       len(sources), _ptr(sc, ctypes.c_int64), _ptr(sk, ctypes.c_int32), _ptr(sd, ctypes.c_int32),
+                       _ptr(sa, ctypes.c_double), nt, _ptr(wavelet, ctypes.c_double),
+                       len(receivers), _ptr(rc, ctypes.c_int64), _ptr(rk, ctypes.c_int32),
+                       om.size, _ptr(om, ctypes.c_double), 1 if h_factor else 0, _ptr(ob, ctypes.c_double),
+                       _ptr(mis, ctypes.c_double), _ptr(g, ctypes.c_double), _ptr(spec, ctypes.c_double))
+    if r != 0:
+        raise MemoryError("oracle allocation failed")
+    return float(mis[0]), g.reshape(p.nz, p.ny, p.nx), spec[..., 0] + 1j * spec[..., 1]
+
+
+def misfit(p: Params, sigma, mu, sources, wavelet, receivers, nt, omega, obs, h_factor=True):
+    """0.5 sum |S - obs|^2 from a plain forward (for finite differences)."""
+    tr = forward(p, sigma, mu, sources, wavelet, receivers, nt)
+    J = 0.0
+    for r, rec in enumerate(receivers):
+        S = dft(tr[r], p.dt, p.omega0, omega, h_factor=h_factor and rec[3].startswith("h"))
+        J += 0.5 * float(np.sum(np.abs(S - obs[r]) ** 2))
+    return J
