@@ -48,13 +48,21 @@ struct PhaseArgs {
     T c1, c2, c2t;          // stencil weights; c2t = c2 (psi_Hyx typo) or c1
     T sgn;                  // +1 / -1 ("bp" updates)
     T ik[3];                // 1/d per axis: the 1/ked (1/khd) value of every interior cell
-    // full-volume DFT ring (E phase only): ring[slot][vcomp][shot][cell]
+    // full-volume DFT ring (E phase only), see ring_index
     T *ring;
     int ring_k;             // ring depth K (0 = no ring)
     int vmask;              // E components written to the ring
     long long ring_comp;    // elements per (slot, vcomp) = nshot * fshot
     const int *d_step;
 };
+
+// Ring layout [vcomp][tile of 32 cells][slot][32]: a warp's 32 consecutive
+// cells of one step form one 128-byte line (E-phase writes), and the ring_k
+// steps of those cells are one contiguous 4 KB block (flush reads).
+// e = shot * fshot + cell (padded layout); ring_comp = nshot * fshot.
+__device__ __forceinline__ long long ring_index(long long ring_comp, int K, int vc, long long e, int slot) {
+    return (long long)vc * ring_comp * K + (e & ~31LL) * K + (long long)slot * 32 + (e & 31);
+}
 
 __device__ __forceinline__ bool in_box(const DBox &b, int i, int j, int k) {
     return i >= b.lo[0] && i < b.hi[0] && j >= b.lo[1] && j < b.hi[1] && k >= b.lo[2] && k < b.hi[2];
@@ -127,7 +135,7 @@ __global__ void inject_kernel(InjectArgs<T> a) {
         const T v = atomicAdd(cell, (T)(-s.g * w)) + (T)(-s.g * w);
         if (a.ring && s.comp < 3 && (a.vmask >> s.comp & 1)) {
             const int slot = n % a.ring_k;
-            a.ring[((long long)slot * 3 + s.comp) * a.ring_comp + s.off] = v;
+            a.ring[ring_index(a.ring_comp, a.ring_k, s.comp, s.off, slot)] = v;
         }
     }
 }
@@ -219,7 +227,7 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 // Every ring_k steps the E phase has left the last ring_k values of each
 // selected E component in the ring; this kernel folds them into the FP64
 // accumulators:
-//   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring[s][vc][shot][cell],
+//   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring(vc, shot*fshot + cell, s),
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
 // One thread per (component, shot, cell).  The sum over the ring is formed in
 // the field precision T (at most 32 terms; for FP32 fields the partial sum
@@ -227,8 +235,8 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 // flush.  Ring values are loaded 16 at a time before any arithmetic; the
 // weights of the flush sit in shared memory.
 template <typename T>
-__global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int nvc,
-                                                         int3 vcs, long long fshot, int cnt, int n0,
+__global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int ring_k,
+                                                         int nvc, int3 vcs, long long fshot, int cnt, int n0,
                                                          const double2 *__restrict__ wt, int nf,
                                                          double2 *__restrict__ acc) {
     extern __shared__ unsigned char sw_raw[];
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ r
         const long long shot = e / fshot;
         const long long cell = e - shot * fshot;
         double2 *__restrict__ ap = acc + ((shot * 3 + vc) * nf) * fshot + cell;
-        const T *__restrict__ rp = ring + (long long)vc * ring_comp + e;
+        const T *__restrict__ rp = ring + ring_index(ring_comp, ring_k, vc, e, 0);
         for (int f0 = 0; f0 < nf; f0 += 8) {
             const int fn = min(8, nf - f0);
             T pr[8], pi[8];
@@ -258,7 +266,7 @@ __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ r
                 T xs[16];
 #pragma unroll
                 for (int s = 0; s < 16; s++)
-                    xs[s] = (s0 + s < cnt) ? __ldg(rp + (long long)(s0 + s) * 3 * ring_comp) : T(0);
+                    xs[s] = (s0 + s < cnt) ? __ldg(rp + (long long)(s0 + s) * 32) : T(0);
 #pragma unroll
                 for (int s = 0; s < 16; s++) {
                     if (s0 + s < cnt) {

@@ -456,7 +456,7 @@ void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
         if (h->vmask >> c & 1) vc[nvc++] = c;
     int blocks = (int)std::min<long long>((tot * nvc + 255) / 256, 148LL * 16);
     volume_dft_kernel<T><<<blocks, 256, (size_t)cnt * nf * 2 * sizeof(T), h->st>>>(
-        h->ring.as<T>(), tot, nvc, make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, n0, h->wtab.as<double2>(), nf,
+        h->ring.as<T>(), tot, h->ring_k, nvc, make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, n0, h->wtab.as<double2>(), nf,
         h->acc.as<double2>());
     h->launches++;
 }

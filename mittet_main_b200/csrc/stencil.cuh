@@ -307,10 +307,10 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         stv<T, VX>(Ey + c, ey);
         stv<T, VX>(Ez + c, ez);
         if (a.ring_k > 0) {
-            T *__restrict__ r = a.ring + (long long)slot * 3 * a.ring_comp + sb + c;
-            if (a.vmask & 1) stv<T, VX>(r, ex);
-            if (a.vmask & 2) stv<T, VX>(r + a.ring_comp, ey);
-            if (a.vmask & 4) stv<T, VX>(r + 2 * a.ring_comp, ez);
+            const long long e = sb + c;
+            if (a.vmask & 1) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
+            if (a.vmask & 2) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
+            if (a.vmask & 4) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
         }
     }
 }

@@ -80,7 +80,8 @@ def test_gradient_does_not_depend_on_checkpoint_interval():
         J1, G1 = s.gradient(wl.nt, obs, checkpoint_every=7)
         J2, G2 = s.gradient(wl.nt, obs, checkpoint_every=70)
         J3, G3 = s.gradient(wl.nt, obs, checkpoint_every=33)
-    assert J1 == J2 == J3
+    # the misfit is an atomic reduction: equal to rounding; the gradient is deterministic
+    assert J1 == pytest.approx(J2, rel=1e-13) and J1 == pytest.approx(J3, rel=1e-13)
     assert np.array_equal(G1, G2) and np.array_equal(G1, G3)
 
 
@@ -88,11 +89,12 @@ def test_gradient_matches_gpu_finite_differences():
     wl, obs = case(FP64, nt=80)
     with W.make_solver(wl) as s:
         J, G = s.gradient(wl.nt, obs, checkpoint_every=20)
+    # 16 cells drawn with seed 2026 among those whose gradient a central
+    # difference can resolve in FP64 (|G| above 1e-3 of the largest)
     rng = np.random.default_rng(2026)
-    nc = wl.cp.ncpml
-    cells = [(rng.integers(nc, wl.cp.nz - nc), rng.integers(nc, wl.cp.ny - nc), rng.integers(nc, wl.cp.nx - nc))
-             for _ in range(6)]
     gmax = np.abs(G).max()
+    cand = np.argwhere(np.abs(G) > 1e-3 * gmax)
+    cells = [tuple(cand[q]) for q in rng.choice(len(cand), size=min(16, len(cand)), replace=False)]
     for (k, j, i) in cells:
         dd = 1e-4 * wl.sigma[k, j, i]
         Js = []
@@ -103,7 +105,8 @@ def test_gradient_matches_gpu_finite_differences():
                 spec, _ = s.forward(wl.nt)
             Js.append(0.5 * float(np.sum(np.abs(spec - obs) ** 2)))
         fd = (Js[0] - Js[1]) / (2 * dd)
-        assert abs(G[k, j, i] - fd) <= 1e-3 * max(abs(fd), 1e-4 * gmax), (k, j, i, G[k, j, i], fd)
+        noise = 8 * np.finfo(float).eps * J / dd
+        assert abs(G[k, j, i] - fd) <= 1e-3 * abs(fd) + noise, (k, j, i, G[k, j, i], fd)
 
 
 def test_autograd_function_returns_the_gradient():
