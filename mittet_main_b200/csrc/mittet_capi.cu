@@ -130,7 +130,8 @@ struct mittet_handle_s {
     int var_e = 0, var_h = 0;  // stencil variants (index into variants<T>())
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
     int tiles[64] = {0};       // tiles per (variant, phase)
-    int tiles_int[64] = {0};   // of which interior
+    int tiles_int[64] = {0};   // tiles [0, tiles_int) interior
+    int tiles_face[64] = {0};  // tiles [tiles_int, tiles_face) faces
     bool tuned = false;
     DevBuf ring, acc, wtab;
 
@@ -235,6 +236,8 @@ struct Variant {
     int vx, bx, by, kz;
     void (*ei)(PhaseArgs<T>, const TileMap *);
     void (*hi)(PhaseArgs<T>, const TileMap *);
+    void (*ef)(PhaseArgs<T>, const TileMap *, int);
+    void (*hf)(PhaseArgs<T>, const TileMap *, int);
     void (*es)(PhaseArgs<T>, const TileMap *, int);
     void (*hs)(PhaseArgs<T>, const TileMap *, int);
 };
@@ -247,6 +250,7 @@ const std::vector<Variant<float>> &variants<float>() {
     static const std::vector<Variant<float>> v = {
 #define MITTET_X(vx, bx, by, kz)                                                                      \
     {vx, bx, by, kz, e_interior_kernel<float, vx, bx, by, kz>, h_interior_kernel<float, vx, bx, by, kz>, \
+     e_face_kernel<float, vx, bx, by, kz>, h_face_kernel<float, vx, bx, by, kz>,                         \
      e_shell_kernel<float, vx, bx, by, kz>, h_shell_kernel<float, vx, bx, by, kz>},
         MITTET_STENCIL_VARIANTS_F32(MITTET_X)
 #undef MITTET_X
@@ -258,6 +262,7 @@ const std::vector<Variant<double>> &variants<double>() {
     static const std::vector<Variant<double>> v = {
 #define MITTET_X(vx, bx, by, kz)                                                                        \
     {vx, bx, by, kz, e_interior_kernel<double, vx, bx, by, kz>, h_interior_kernel<double, vx, bx, by, kz>, \
+     e_face_kernel<double, vx, bx, by, kz>, h_face_kernel<double, vx, bx, by, kz>,                         \
      e_shell_kernel<double, vx, bx, by, kz>, h_shell_kernel<double, vx, bx, by, kz>},
         MITTET_STENCIL_VARIANTS_F64(MITTET_X)
 #undef MITTET_X
@@ -303,32 +308,48 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
     const int TX = bx * vx;
     int lo[3], hi[3];
     interior_box(h, e, lo, hi);
-    int X0 = (lo[0] + vx - 1) / vx * vx;
-    int ntx = hi[0] > X0 ? (hi[0] - X0) / TX : 0;
-    int nty = hi[1] > lo[1] ? (hi[1] - lo[1]) / by : 0;
-    int ntz = hi[2] > lo[2] ? (hi[2] - lo[2]) / kz : 0;
-    auto add = [&](int x0, int y0, int z0, int x1, int y1, int z1, bool full) {
+    // x box edges are multiples of 4 cells, so every vector width divides them
+    const int X0 = (lo[0] + 3) / 4 * 4;
+    const int ntx = hi[0] > X0 ? (hi[0] - X0) / TX : 0;
+    const int nty = hi[1] > lo[1] ? (hi[1] - lo[1]) / by : 0;
+    const int ntz = hi[2] > lo[2] ? (hi[2] - lo[2]) / kz : 0;
+    auto add = [&](int kind, int x0, int y0, int z0, int x1, int y1, int z1) {
         if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
         const int q = t.nbox++;
+        t.kind[q] = kind;
         t.lo[q][0] = x0; t.lo[q][1] = y0; t.lo[q][2] = z0;
         t.hi[q][0] = x1; t.hi[q][1] = y1; t.hi[q][2] = z1;
-        t.ntx[q] = full ? (x1 - x0) / TX : (x1 - x0 + TX - 1) / TX;
-        t.nty[q] = full ? (y1 - y0) / by : (y1 - y0 + by - 1) / by;
-        const int nzt = full ? (z1 - z0) / kz : (z1 - z0 + kz - 1) / kz;
+        t.ntx[q] = (x1 - x0 + TX - 1) / TX;
+        t.nty[q] = (y1 - y0 + by - 1) / by;
+        const int nzt = (z1 - z0 + kz - 1) / kz;
         t.start[q + 1] = t.start[q] + t.ntx[q] * t.nty[q] * nzt;
     };
     if (ntx > 0 && nty > 0 && ntz > 0) {
         const int X1 = X0 + ntx * TX, Y0 = lo[1], Y1 = lo[1] + nty * by, Z0 = lo[2], Z1 = lo[2] + ntz * kz;
-        t.interior = 1;
-        add(X0, Y0, Z0, X1, Y1, Z1, true);
-        add(0, 0, 0, nx, ny, Z0, false);
-        add(0, 0, Z1, nx, ny, nz, false);
-        add(0, 0, Z0, nx, Y0, Z1, false);
-        add(0, Y1, Z0, nx, ny, Z1, false);
-        add(0, Y0, Z0, X0, Y1, Z1, false);
-        add(X1, Y0, Z0, nx, Y1, Z1, false);
+        add(0, X0, Y0, Z0, X1, Y1, Z1);
+        t.g0 = t.start[t.nbox];
+        add(1, 0, Y0, Z0, X0, Y1, Z1);   // x faces
+        add(1, X1, Y0, Z0, nx, Y1, Z1);
+        add(2, X0, 0, Z0, X1, Y0, Z1);   // y faces
+        add(2, X0, Y1, Z0, X1, ny, Z1);
+        add(4, X0, Y0, 0, X1, Y1, Z0);   // z faces
+        add(4, X0, Y0, Z1, X1, Y1, nz);
+        t.g1 = t.start[t.nbox];
+        const int zr[2][2] = {{0, Z0}, {Z1, nz}};
+        for (int zz = 0; zz < 2; zz++) {  // rings around the z faces
+            const int za = zr[zz][0], zb = zr[zz][1];
+            add(7, 0, 0, za, nx, Y0, zb);
+            add(7, 0, Y1, za, nx, ny, zb);
+            add(7, 0, Y0, za, X0, Y1, zb);
+            add(7, X1, Y0, za, nx, Y1, zb);
+        }
+        add(7, 0, 0, Z0, X0, Y0, Z1);     // vertical edges
+        add(7, X1, 0, Z0, nx, Y0, Z1);
+        add(7, 0, Y1, Z0, X0, ny, Z1);
+        add(7, X1, Y1, Z0, nx, ny, Z1);
     } else {
-        add(0, 0, 0, nx, ny, nz, false);
+        t.g0 = t.g1 = 0;
+        add(7, 0, 0, 0, nx, ny, nz);
     }
     return t;
 }
@@ -343,7 +364,8 @@ int upload_tilemaps(mittet_handle *h) {
         for (int p = 0; p < 2; p++) {
             const TileMap &t = maps[2 * v + p];
             h->tiles[2 * v + p] = t.start[t.nbox];
-            h->tiles_int[2 * v + p] = t.interior ? t.start[1] : 0;
+            h->tiles_int[2 * v + p] = t.g0;
+            h->tiles_face[2 * v + p] = t.g1;
         }
     }
     CK(h->tmaps.ensure(maps.size() * sizeof(TileMap)));
@@ -359,19 +381,25 @@ int launch_phase(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a) {
     const Variant<T> &v = variants<T>()[vi];
     const int slot = 2 * vi + (e ? 0 : 1);
     const TileMap *tm = h->tmaps.as<TileMap>() + slot;
-    const int n_int = h->tiles_int[slot], n_all = h->tiles[slot];
+    const int g0 = h->tiles_int[slot], g1 = h->tiles_face[slot], n_all = h->tiles[slot];
     dim3 block(v.bx, v.by);
     int n = 0;
-    if (n_int > 0) {
-        dim3 grid(n_int, h->nshot);
+    if (g0 > 0) {
+        dim3 grid(g0, h->nshot);
         if (e) v.ei<<<grid, block, 0, h->st>>>(a, tm);
         else v.hi<<<grid, block, 0, h->st>>>(a, tm);
         n++;
     }
-    if (n_all > n_int) {
-        dim3 grid(n_all - n_int, h->nshot);
-        if (e) v.es<<<grid, block, 0, h->st>>>(a, tm, n_int);
-        else v.hs<<<grid, block, 0, h->st>>>(a, tm, n_int);
+    if (g1 > g0) {
+        dim3 grid(g1 - g0, h->nshot);
+        if (e) v.ef<<<grid, block, 0, h->st>>>(a, tm, g0);
+        else v.hf<<<grid, block, 0, h->st>>>(a, tm, g0);
+        n++;
+    }
+    if (n_all > g1) {
+        dim3 grid(n_all - g1, h->nshot);
+        if (e) v.es<<<grid, block, 0, h->st>>>(a, tm, g1);
+        else v.hs<<<grid, block, 0, h->st>>>(a, tm, g1);
         n++;
     }
     return n;

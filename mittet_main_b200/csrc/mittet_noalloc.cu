@@ -238,7 +238,8 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
     TileMap tm;
     memset(&tm, 0, sizeof(tm));
     tm.nbox = 1;
-    tm.interior = 0;
+    tm.g0 = tm.g1 = 0;
+    tm.kind[0] = 7;
     tm.hi[0][0] = nx; tm.hi[0][1] = ny; tm.hi[0][2] = nz;
     tm.ntx[0] = (nx + NA_BX * NA_VX - 1) / (NA_BX * NA_VX);
     tm.nty[0] = (ny + NA_BY - 1) / NA_BY;

@@ -2,14 +2,16 @@
 //
 // Work decomposition.  The grid of one phase is split on the host into an
 // interior box (no CPML profile, no psi slab, every component inside its
-// update range, every derivative defined) cut into whole tiles, plus up to
-// six shell boxes around it.  One launch covers all of them: blockIdx.x
-// enumerates the tiles of box 0, then box 1, ... (TileMap, in global
-// memory), blockIdx.y is the shot.  Interior tiles run a straight-line body
-// with no per-cell tests; shell tiles run the general body that restates the
-// reference's index ranges, CPML profiles and psi recurrences.  Both bodies
-// use the same explicit fma forms, so a cell gets bit-identical results
-// whichever body computes it.
+// update range, every derivative defined) cut into whole tiles, six faces
+// around it that need the reference's CPML/range handling along one axis
+// only, and twelve edge/corner boxes that need it along several.  The body
+// is one template specialised by a mask GM of the axes handled generally, so
+// the interior (GM = 0) is straight-line code, a face carries one axis's
+// CPML terms, and only edges and corners (GM = 7) pay for all of them.
+// Three launches per phase (interior, faces, general); blockIdx.x
+// enumerates tiles through a TileMap in global memory, blockIdx.y is the
+// shot.  Every body uses the same explicit fma forms, so a cell gets
+// bit-identical results whichever body computes it.
 //
 // Thread mapping: a BX x BY block covers one tile in (x, y); each thread owns
 // VX consecutive x cells (one aligned float2/float4/double2 per field and
@@ -32,13 +34,17 @@
 
 namespace mittet {
 
-// Boxes of one phase, in the order their tiles are enumerated by blockIdx.x.
+// Boxes of one phase, in the order their tiles are enumerated: the interior
+// box, then six faces (CPML / range handling along one axis only), then the
+// edge and corner boxes (general handling).  kind = mask of the axes that
+// need general handling (0 interior, 1/2/4 faces, 7 general).
 struct TileMap {
-    int nbox;        // boxes in use (<= 7)
-    int interior;    // 1: box 0 is the interior fast-path box
-    int start[8];    // first tile of each box; start[nbox] = tiles in total
-    int lo[7][3], hi[7][3];
-    int ntx[7], nty[7];
+    int nbox;
+    int g0, g1;       // tiles [0, g0) interior, [g0, g1) faces, [g1, start[nbox]) general
+    int start[25];    // first tile of each box
+    int kind[24];
+    int lo[24][3], hi[24][3];
+    int ntx[24], nty[24];
 };
 
 template <typename T, int VX>
@@ -103,7 +109,7 @@ __device__ __forceinline__ T leap(T ca, T sgcb, T x, T e) {  // ca e + (s cb) x
 #define MITTET_MINB(T, VX, KZ, NT) ((sizeof(T) == 4 && VX == 2 && KZ == 1) ? 768 / (NT) : 512 / (NT))
 
 // ------------------------------------------------------------------ E phase
-template <typename T, int VX, int KZ, bool INT>
+template <typename T, int VX, int KZ, int GM>
 __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int khi) {
     const long long sb = (long long)shot * a.fshot;
     T *__restrict__ Ex = a.f[0] + sb;
@@ -117,47 +123,50 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
     const int py = a.px, pz = (int)a.plane, nx = a.nx, ny = a.ny, nz = a.nz, ps = a.nmax;
     const T c1 = a.c1, c2 = a.c2, sg = a.sgn;
 
+    // GM bit 0/1/2: general handling along x/y/z; a clear bit means every
+    // cell of the box is interior along that axis (no CPML profile, no psi
+    // slab, inside every update range, derivative defined).
+    constexpr bool GX = (GM & 1) != 0, GY = (GM & 2) != 0, GZ = (GM & 4) != 0;
     T esh_x[VX], ik_x[VX];
     T esh_y, ik_y;
-    bool vy, has_l, has_r;
-    unsigned vxm, ux, uy, uz, sxm, sym, szm;
-    int ly;
-    DSlab S0, S1, S2;
-    if constexpr (INT) {
-#pragma unroll
-        for (int v = 0; v < VX; v++) { esh_x[v] = T(0); ik_x[v] = a.ik[0]; }
-        esh_y = T(0);
-        ik_y = a.ik[1];
-        vy = has_l = has_r = true;
-        vxm = ux = uy = uz = (1u << VX) - 1u;
-        sxm = sym = szm = 0u;
-        ly = -1;
-    } else {
+    if constexpr (GX) {
         ldv<T, VX>(esh_x, P + 0 * ps + i0);
         ldv<T, VX>(ik_x, P + 6 * ps + i0);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VX; v++) { esh_x[v] = T(0); ik_x[v] = a.ik[0]; }
+    }
+    if constexpr (GY) {
         esh_y = __ldg(P + 8 * ps + j);
         ik_y = __ldg(P + 14 * ps + j);
-        vy = (j >= 2) && (j + 1 < ny);
-        has_l = i0 >= VX;
-        has_r = i0 + VX < nx;
+    } else {
+        esh_y = T(0);
+        ik_y = a.ik[1];
+    }
+    const bool vy = GY ? ((j >= 2) && (j + 1 < ny)) : true;
+    const bool has_l = GX ? (i0 >= VX) : true;
+    const bool has_r = GX ? (i0 + VX < nx) : true;
+    unsigned vxm = (1u << VX) - 1u;
+    if constexpr (GX) {
         vxm = 0;
 #pragma unroll
         for (int v = 0; v < VX; v++) vxm |= (unsigned)(i0 + v >= 2 && i0 + v + 1 < nx) << v;
-        const DBox U0 = a.upd[0], U1 = a.upd[1], U2 = a.upd[2];
-        ux = (j >= U0.lo[1] && j < U0.hi[1]) ? xmask<VX>(i0, U0.lo[0], U0.hi[0]) : 0u;
-        uy = (j >= U1.lo[1] && j < U1.hi[1]) ? xmask<VX>(i0, U1.lo[0], U1.hi[0]) : 0u;
-        uz = (j >= U2.lo[1] && j < U2.hi[1]) ? xmask<VX>(i0, U2.lo[0], U2.hi[0]) : 0u;
-        S0 = a.slab[0];
-        S1 = a.slab[1];
-        S2 = a.slab[2];
-        sxm = 0;
+    }
+    const DBox U0 = a.upd[0], U1 = a.upd[1], U2 = a.upd[2];
+    const unsigned all = (1u << VX) - 1u;
+    const unsigned ux = (!GY || (j >= U0.lo[1] && j < U0.hi[1])) ? (GX ? xmask<VX>(i0, U0.lo[0], U0.hi[0]) : all) : 0u;
+    const unsigned uy = (!GY || (j >= U1.lo[1] && j < U1.hi[1])) ? (GX ? xmask<VX>(i0, U1.lo[0], U1.hi[0]) : all) : 0u;
+    const unsigned uz = (!GY || (j >= U2.lo[1] && j < U2.hi[1])) ? (GX ? xmask<VX>(i0, U2.lo[0], U2.hi[0]) : all) : 0u;
+    const DSlab S0 = a.slab[0], S1 = a.slab[1], S2 = a.slab[2];
+    unsigned sxm = 0;
+    if constexpr (GX) {
 #pragma unroll
         for (int v = 0; v < VX; v++) sxm |= (unsigned)(slab_local(S0, i0 + v) >= 0) << v;
-        sxm = (j >= S0.other.lo[1] && j < S0.other.hi[1]) ? sxm : 0u;
-        ly = slab_local(S1, j);
-        sym = ly >= 0 ? xmask<VX>(i0, S1.other.lo[0], S1.other.hi[0]) : 0u;
-        szm = (j >= S2.other.lo[1] && j < S2.other.hi[1]) ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : 0u;
+        if (GY && !(j >= S0.other.lo[1] && j < S0.other.hi[1])) sxm = 0u;
     }
+    const int ly = GY ? slab_local(S1, j) : -1;
+    const unsigned sym = ly >= 0 ? (GX ? xmask<VX>(i0, S1.other.lo[0], S1.other.hi[0]) : all) : 0u;
+    const unsigned szm = GZ ? ((!GY || (j >= S2.other.lo[1] && j < S2.other.hi[1])) ? (GX ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : all) : 0u) : 0u;
     const int col = j * py + i0;
 
     // z window: planes kb-2 .. kb+KZ of Hx and Hy
@@ -165,7 +174,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
 #pragma unroll
     for (int q = 0; q < KZ + 3; q++) {
         const int kk = kb - 2 + q;
-        if (INT || (kk >= 0 && kk < nz)) {
+        if (!GZ || (kk >= 0 && kk < nz)) {
             ldv<T, VX>(wx[q], Hx + kk * pz + col);
             ldv<T, VX>(wy[q], Hy + kk * pz + col);
         } else {
@@ -178,7 +187,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
 #pragma unroll
     for (int q = 0; q < KZ; q++) {
         const int k = kb + q;
-        if (!INT && k >= khi) break;
+        if (GM != 0 && k >= khi) break;
         const int c = k * pz + col;
         T hzx[3 * VX], hyx[3 * VX];
         {
@@ -229,7 +238,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         T esh_z, ik_z;
         bool vz, kx, ky, kz;
         int lz;
-        if constexpr (INT) {
+        if constexpr (!GZ) {
             esh_z = T(0);
             ik_z = a.ik[2];
             vz = kx = ky = kz = true;
@@ -238,11 +247,13 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
             esh_z = __ldg(P + 16 * ps + k);
             ik_z = __ldg(P + 22 * ps + k);
             vz = (k >= 2) && (k + 1 < nz);
-            kx = k >= a.upd[0].lo[2] && k < a.upd[0].hi[2];
-            ky = k >= a.upd[1].lo[2] && k < a.upd[1].hi[2];
-            kz = k >= a.upd[2].lo[2] && k < a.upd[2].hi[2];
+            kx = k >= U0.lo[2] && k < U0.hi[2];
+            ky = k >= U1.lo[2] && k < U1.hi[2];
+            kz = k >= U2.lo[2] && k < U2.hi[2];
             lz = slab_local(S2, k);
         }
+        const bool s0k = !GZ || (k >= S0.other.lo[2] && k < S0.other.hi[2]);
+        const bool s1k = !GZ || (k >= S1.other.lo[2] && k < S1.other.hi[2]);
 
 #pragma unroll
         for (int v = 0; v < VX; v++) {
@@ -255,17 +266,15 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
             const T dzHx = vz ? d4(c1, c2, wx[q + 2][v], wx[q + 1][v], wx[q + 3][v], wx[q][v]) : T(0);
             const T mv = m[v];
             T ca_x = T(1), cb_x = mv, ca_y = T(1), cb_y = mv, ca_z = T(1), cb_z = mv;
-            if (!INT) {
-                if (esh_x[v] != T(0)) { const T h = esh_x[v] * mv; const T r = rcp(T(1) + h); ca_x = (T(1) - h) * r; cb_x = mv * r; }
-                if (esh_y != T(0)) { const T h = esh_y * mv; const T r = rcp(T(1) + h); ca_y = (T(1) - h) * r; cb_y = mv * r; }
-                if (esh_z != T(0)) { const T h = esh_z * mv; const T r = rcp(T(1) + h); ca_z = (T(1) - h) * r; cb_z = mv * r; }
-            }
+            if (GX && esh_x[v] != T(0)) { const T h = esh_x[v] * mv; const T r = rcp(T(1) + h); ca_x = (T(1) - h) * r; cb_x = mv * r; }
+            if (GY && esh_y != T(0)) { const T h = esh_y * mv; const T r = rcp(T(1) + h); ca_y = (T(1) - h) * r; cb_y = mv * r; }
+            if (GZ && esh_z != T(0)) { const T h = esh_z * mv; const T r = rcp(T(1) + h); ca_z = (T(1) - h) * r; cb_z = mv * r; }
             if (kx && (ux >> v & 1)) ex[v] = leap(ca_x, sg * cb_x, curl2(dyHz, ik_y, dzHy, ik_z), ex[v]);
             if (ky && (uy >> v & 1)) ey[v] = leap(ca_y, sg * cb_y, curl2(dzHx, ik_z, dxHz, ik_x[v]), ey[v]);
             if (kz && (uz >> v & 1)) ez[v] = leap(ca_z, sg * cb_z, curl2(dxHy, ik_x[v], dyHx, ik_y), ez[v]);
 
-            if (!INT) {
-                if ((sxm >> v & 1) && k >= S0.other.lo[2] && k < S0.other.hi[2]) {
+            {
+                if (GX && (sxm >> v & 1) && s0k) {
                     T *__restrict__ q0 = a.psi[0][0] + shot * a.pshot[0];
                     T *__restrict__ q1 = a.psi[0][1] + shot * a.pshot[0];
                     const int o = (k * ny + j) * S0.width + slab_local(S0, i0 + v);
@@ -277,7 +286,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
                     ez[v] = fma(cb_z, p0, ez[v]);
                     ey[v] = fma(-cb_y, p1, ey[v]);
                 }
-                if ((sym >> v & 1) && k >= S1.other.lo[2] && k < S1.other.hi[2]) {
+                if (GY && (sym >> v & 1) && s1k) {
                     T *__restrict__ q0 = a.psi[1][0] + shot * a.pshot[1];
                     T *__restrict__ q1 = a.psi[1][1] + shot * a.pshot[1];
                     const int o = (k * S1.width + ly) * py + i0 + v;
@@ -289,7 +298,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
                     ex[v] = fma(cb_x, p0, ex[v]);
                     ez[v] = fma(-cb_z, p1, ez[v]);
                 }
-                if ((szm >> v & 1) && lz >= 0) {
+                if (GZ && (szm >> v & 1) && lz >= 0) {
                     T *__restrict__ q0 = a.psi[2][0] + shot * a.pshot[2];
                     T *__restrict__ q1 = a.psi[2][1] + shot * a.pshot[2];
                     const int o = (lz * ny + j) * py + i0 + v;
@@ -316,7 +325,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
 }
 
 // ------------------------------------------------------------------ H phase
-template <typename T, int VX, int KZ, bool INT>
+template <typename T, int VX, int KZ, int GM>
 __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int khi) {
     const long long sb = (long long)shot * a.fshot;
     const T *__restrict__ Ex = a.f[0] + sb;
@@ -331,47 +340,50 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
     const int py = a.px, pz = (int)a.plane, nx = a.nx, ny = a.ny, nz = a.nz, ps = a.nmax;
     const T c1 = a.c1, c2 = a.c2, c2t = a.c2t, sg = a.sgn;
 
+    // GM bit 0/1/2: general handling along x/y/z; a clear bit means every
+    // cell of the box is interior along that axis (no CPML profile, no psi
+    // slab, inside every update range, derivative defined).
+    constexpr bool GX = (GM & 1) != 0, GY = (GM & 2) != 0, GZ = (GM & 4) != 0;
     T msh_x[VX], ik_x[VX];
     T msh_y, ik_y;
-    bool vy, has_l, has_r;
-    unsigned vxm, ux, uy, uz, sxm, sym, szm;
-    int ly;
-    DSlab S0, S1, S2;
-    if constexpr (INT) {
-#pragma unroll
-        for (int v = 0; v < VX; v++) { msh_x[v] = T(0); ik_x[v] = a.ik[0]; }
-        msh_y = T(0);
-        ik_y = a.ik[1];
-        vy = has_l = has_r = true;
-        vxm = ux = uy = uz = (1u << VX) - 1u;
-        sxm = sym = szm = 0u;
-        ly = -1;
-    } else {
+    if constexpr (GX) {
         ldv<T, VX>(msh_x, P + 1 * ps + i0);
         ldv<T, VX>(ik_x, P + 7 * ps + i0);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VX; v++) { msh_x[v] = T(0); ik_x[v] = a.ik[0]; }
+    }
+    if constexpr (GY) {
         msh_y = __ldg(P + 9 * ps + j);
         ik_y = __ldg(P + 15 * ps + j);
-        vy = (j >= 1) && (j + 2 < ny);
-        has_l = i0 >= VX;
-        has_r = i0 + VX < nx;
+    } else {
+        msh_y = T(0);
+        ik_y = a.ik[1];
+    }
+    const bool vy = GY ? ((j >= 1) && (j + 2 < ny)) : true;
+    const bool has_l = GX ? (i0 >= VX) : true;
+    const bool has_r = GX ? (i0 + VX < nx) : true;
+    unsigned vxm = (1u << VX) - 1u;
+    if constexpr (GX) {
         vxm = 0;
 #pragma unroll
         for (int v = 0; v < VX; v++) vxm |= (unsigned)(i0 + v >= 1 && i0 + v + 2 < nx) << v;
-        const DBox U0 = a.upd[0], U1 = a.upd[1], U2 = a.upd[2];
-        ux = (j >= U0.lo[1] && j < U0.hi[1]) ? xmask<VX>(i0, U0.lo[0], U0.hi[0]) : 0u;
-        uy = (j >= U1.lo[1] && j < U1.hi[1]) ? xmask<VX>(i0, U1.lo[0], U1.hi[0]) : 0u;
-        uz = (j >= U2.lo[1] && j < U2.hi[1]) ? xmask<VX>(i0, U2.lo[0], U2.hi[0]) : 0u;
-        S0 = a.slab[0];
-        S1 = a.slab[1];
-        S2 = a.slab[2];
-        sxm = 0;
+    }
+    const DBox U0 = a.upd[0], U1 = a.upd[1], U2 = a.upd[2];
+    const unsigned all = (1u << VX) - 1u;
+    const unsigned ux = (!GY || (j >= U0.lo[1] && j < U0.hi[1])) ? (GX ? xmask<VX>(i0, U0.lo[0], U0.hi[0]) : all) : 0u;
+    const unsigned uy = (!GY || (j >= U1.lo[1] && j < U1.hi[1])) ? (GX ? xmask<VX>(i0, U1.lo[0], U1.hi[0]) : all) : 0u;
+    const unsigned uz = (!GY || (j >= U2.lo[1] && j < U2.hi[1])) ? (GX ? xmask<VX>(i0, U2.lo[0], U2.hi[0]) : all) : 0u;
+    const DSlab S0 = a.slab[0], S1 = a.slab[1], S2 = a.slab[2];
+    unsigned sxm = 0;
+    if constexpr (GX) {
 #pragma unroll
         for (int v = 0; v < VX; v++) sxm |= (unsigned)(slab_local(S0, i0 + v) >= 0) << v;
-        sxm = (j >= S0.other.lo[1] && j < S0.other.hi[1]) ? sxm : 0u;
-        ly = slab_local(S1, j);
-        sym = ly >= 0 ? xmask<VX>(i0, S1.other.lo[0], S1.other.hi[0]) : 0u;
-        szm = (j >= S2.other.lo[1] && j < S2.other.hi[1]) ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : 0u;
+        if (GY && !(j >= S0.other.lo[1] && j < S0.other.hi[1])) sxm = 0u;
     }
+    const int ly = GY ? slab_local(S1, j) : -1;
+    const unsigned sym = ly >= 0 ? (GX ? xmask<VX>(i0, S1.other.lo[0], S1.other.hi[0]) : all) : 0u;
+    const unsigned szm = GZ ? ((!GY || (j >= S2.other.lo[1] && j < S2.other.hi[1])) ? (GX ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : all) : 0u) : 0u;
     const int col = j * py + i0;
 
     // z window: planes kb-1 .. kb+KZ+1 of Ex and Ey
@@ -379,7 +391,7 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
 #pragma unroll
     for (int q = 0; q < KZ + 3; q++) {
         const int kk = kb - 1 + q;
-        if (INT || (kk >= 0 && kk < nz)) {
+        if (!GZ || (kk >= 0 && kk < nz)) {
             ldv<T, VX>(wx[q], Ex + kk * pz + col);
             ldv<T, VX>(wy[q], Ey + kk * pz + col);
         } else {
@@ -391,7 +403,7 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
 #pragma unroll
     for (int q = 0; q < KZ; q++) {
         const int k = kb + q;
-        if (!INT && k >= khi) break;
+        if (GM != 0 && k >= khi) break;
         const int c = k * pz + col;
         T ezx[3 * VX], eyx[3 * VX];
         {
@@ -448,7 +460,7 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         T msh_z, ik_z;
         bool vz, kx, ky, kz;
         int lz;
-        if constexpr (INT) {
+        if constexpr (!GZ) {
             msh_z = T(0);
             ik_z = a.ik[2];
             vz = kx = ky = kz = true;
@@ -457,11 +469,13 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
             msh_z = __ldg(P + 17 * ps + k);
             ik_z = __ldg(P + 23 * ps + k);
             vz = (k >= 1) && (k + 2 < nz);
-            kx = k >= a.upd[0].lo[2] && k < a.upd[0].hi[2];
-            ky = k >= a.upd[1].lo[2] && k < a.upd[1].hi[2];
-            kz = k >= a.upd[2].lo[2] && k < a.upd[2].hi[2];
+            kx = k >= U0.lo[2] && k < U0.hi[2];
+            ky = k >= U1.lo[2] && k < U1.hi[2];
+            kz = k >= U2.lo[2] && k < U2.hi[2];
             lz = slab_local(S2, k);
         }
+        const bool s0k = !GZ || (k >= S0.other.lo[2] && k < S0.other.hi[2]);
+        const bool s1k = !GZ || (k >= S1.other.lo[2] && k < S1.other.hi[2]);
 
 #pragma unroll
         for (int v = 0; v < VX; v++) {
@@ -475,17 +489,15 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
             const T dzEx = vz ? d4(c1, c2, wx[q + 2][v], wx[q + 1][v], wx[q + 3][v], wx[q][v]) : T(0);
             const T mv = m[v], dmv = dm[v];
             T da_x = T(1), db_x = dmv, da_y = T(1), db_y = dmv, da_z = T(1), db_z = dmv;
-            if (!INT) {
-                if (msh_x[v] != T(0)) { const T h = msh_x[v] * mv; const T r = rcp(T(1) + h); da_x = (T(1) - h) * r; db_x = dmv * r; }
-                if (msh_y != T(0)) { const T h = msh_y * mv; const T r = rcp(T(1) + h); da_y = (T(1) - h) * r; db_y = dmv * r; }
-                if (msh_z != T(0)) { const T h = msh_z * mv; const T r = rcp(T(1) + h); da_z = (T(1) - h) * r; db_z = dmv * r; }
-            }
+            if (GX && msh_x[v] != T(0)) { const T h = msh_x[v] * mv; const T r = rcp(T(1) + h); da_x = (T(1) - h) * r; db_x = dmv * r; }
+            if (GY && msh_y != T(0)) { const T h = msh_y * mv; const T r = rcp(T(1) + h); da_y = (T(1) - h) * r; db_y = dmv * r; }
+            if (GZ && msh_z != T(0)) { const T h = msh_z * mv; const T r = rcp(T(1) + h); da_z = (T(1) - h) * r; db_z = dmv * r; }
             if (kx && (ux >> v & 1)) hx[v] = leap(da_x, -sg * db_x, curl2(dyEz, ik_y, dzEy, ik_z), hx[v]);
             if (ky && (uy >> v & 1)) hy[v] = leap(da_y, -sg * db_y, curl2(dzEx, ik_z, dxEz, ik_x[v]), hy[v]);
             if (kz && (uz >> v & 1)) hz[v] = leap(da_z, -sg * db_z, curl2(dxEy, ik_x[v], dyEx, ik_y), hz[v]);
 
-            if (!INT) {
-                if ((sxm >> v & 1) && k >= S0.other.lo[2] && k < S0.other.hi[2]) {
+            {
+                if (GX && (sxm >> v & 1) && s0k) {
                     T *__restrict__ q0 = a.psi[0][0] + shot * a.pshot[0];
                     T *__restrict__ q1 = a.psi[0][1] + shot * a.pshot[0];
                     const int o = (k * ny + j) * S0.width + slab_local(S0, i0 + v);
@@ -499,7 +511,7 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
                     hz[v] = fma(-db_z, p0, hz[v]);
                     hy[v] = fma(db_y, p1, hy[v]);
                 }
-                if ((sym >> v & 1) && k >= S1.other.lo[2] && k < S1.other.hi[2]) {
+                if (GY && (sym >> v & 1) && s1k) {
                     T *__restrict__ q0 = a.psi[1][0] + shot * a.pshot[1];
                     T *__restrict__ q1 = a.psi[1][1] + shot * a.pshot[1];
                     const int o = (k * S1.width + ly) * py + i0 + v;
@@ -511,7 +523,7 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
                     hx[v] = fma(-db_x, p0, hx[v]);
                     hz[v] = fma(db_z, p1, hz[v]);
                 }
-                if ((szm >> v & 1) && lz >= 0) {
+                if (GZ && (szm >> v & 1) && lz >= 0) {
                     T *__restrict__ q0 = a.psi[2][0] + shot * a.pshot[2];
                     T *__restrict__ q1 = a.psi[2][1] + shot * a.pshot[2];
                     const int o = (lz * ny + j) * py + i0 + v;
@@ -533,8 +545,8 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
 
 // Locate this CTA's box and tile (tile index b over all boxes).
 template <int VX, int BX, int BY, int KZ>
-__device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int b, int &i0, int &j, int &kb, int &khi,
-                                       bool &inside) {
+__device__ __forceinline__ int locate(const TileMap *__restrict__ tm, int b, int &i0, int &j, int &kb, int &khi,
+                                      bool &inside) {
     const int nbox = __ldg(&tm->nbox);
     int q = 0;
     for (int t = 1; t < nbox; t++)
@@ -548,60 +560,53 @@ __device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int b, in
     kb = __ldg(&tm->lo[q][2]) + tz * KZ;
     khi = __ldg(&tm->hi[q][2]);
     inside = i0 < __ldg(&tm->hi[q][0]) && j < __ldg(&tm->hi[q][1]);
+    return __ldg(&tm->kind[q]);
 }
 
-// Interior tiles (box 0 when tm->interior): straight-line body, own register budget.
-template <typename T, int VX, int BX, int BY, int KZ>
-__global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, KZ, BX *BY))
-    e_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {
-    int i0, j, kb, khi;
-    bool inside;
-    locate<VX, BX, BY, KZ>(tm, blockIdx.x, i0, j, kb, khi, inside);
-    e_cells<T, VX, KZ, true>(a, blockIdx.y, i0, j, kb, kb + KZ);
-}
-template <typename T, int VX, int BX, int BY, int KZ>
-__global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, KZ, BX *BY))
-    h_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {
-    int i0, j, kb, khi;
-    bool inside;
-    locate<VX, BX, BY, KZ>(tm, blockIdx.x, i0, j, kb, khi, inside);
-    h_cells<T, VX, KZ, true>(a, blockIdx.y, i0, j, kb, kb + KZ);
-}
+#define MITTET_PHASE_KERNELS(PH)                                                                             \
+    template <typename T, int VX, int BX, int BY, int KZ>                                                    \
+    __global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, KZ, BX *BY))                                \
+        PH##_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {                         \
+        int i0, j, kb, khi;                                                                                  \
+        bool inside;                                                                                         \
+        locate<VX, BX, BY, KZ>(tm, blockIdx.x, i0, j, kb, khi, inside);                                     \
+        PH##_cells<T, VX, KZ, 0>(a, blockIdx.y, i0, j, kb, kb + KZ);                                         \
+    }                                                                                                        \
+    template <typename T, int VX, int BX, int BY, int KZ>                                                    \
+    __global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))                                               \
+        PH##_face_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {            \
+        int i0, j, kb, khi;                                                                                  \
+        bool inside;                                                                                         \
+        const int kind = locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);       \
+        if (!inside) return;                                                                                 \
+        if (kind == 1) PH##_cells<T, VX, KZ, 1>(a, blockIdx.y, i0, j, kb, khi);                             \
+        else if (kind == 2) PH##_cells<T, VX, KZ, 2>(a, blockIdx.y, i0, j, kb, khi);                        \
+        else PH##_cells<T, VX, KZ, 4>(a, blockIdx.y, i0, j, kb, khi);                                        \
+    }                                                                                                        \
+    template <typename T, int VX, int BX, int BY, int KZ>                                                    \
+    __global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))                                               \
+        PH##_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {           \
+        int i0, j, kb, khi;                                                                                  \
+        bool inside;                                                                                         \
+        locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);                        \
+        if (inside) PH##_cells<T, VX, KZ, 7>(a, blockIdx.y, i0, j, kb, khi);                                 \
+    }
 
-// Shell tiles (every box after the interior one): the general body.
-template <typename T, int VX, int BX, int BY, int KZ>
-__global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))
-    e_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {
-    int i0, j, kb, khi;
-    bool inside;
-    locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);
-    if (inside) e_cells<T, VX, KZ, false>(a, blockIdx.y, i0, j, kb, khi);
-}
-template <typename T, int VX, int BX, int BY, int KZ>
-__global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))
-    h_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {
-    int i0, j, kb, khi;
-    bool inside;
-    locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);
-    if (inside) h_cells<T, VX, KZ, false>(a, blockIdx.y, i0, j, kb, khi);
-}
+// e_interior_kernel / e_face_kernel / e_shell_kernel and the h_ ones.
+MITTET_PHASE_KERNELS(e)
+MITTET_PHASE_KERNELS(h)
 
 // Variants the autotuner chooses from: (VX, BX, BY, KZ).
 #define MITTET_STENCIL_VARIANTS_F32(X) \
     X(2, 32, 4, 1)                     \
-    X(2, 32, 8, 1)                     \
     X(2, 16, 8, 1)                     \
-    X(2, 64, 2, 1)                     \
-    X(4, 32, 4, 1)                     \
     X(4, 16, 8, 1)                     \
     X(4, 8, 16, 1)                     \
     X(2, 32, 4, 2)                     \
     X(4, 16, 4, 2)
 #define MITTET_STENCIL_VARIANTS_F64(X) \
     X(2, 32, 4, 1)                     \
-    X(2, 32, 8, 1)                     \
     X(2, 16, 8, 1)                     \
-    X(2, 64, 2, 1)                     \
     X(2, 32, 4, 2)                     \
     X(2, 16, 4, 2)
 
