@@ -1,0 +1,210 @@
+"""Request loop: continuous batching of forward and gradient solves on one GPU.
+
+Requests (each its own model, grid, shots, receivers and time base) arrive
+over time.  The server keeps ``n_slots`` worker slots; a waiting request is
+admitted as soon as a slot is free and its device-memory estimate fits what
+is left of the HBM budget (first come first served, but a request that does
+not fit lets later, smaller ones go ahead).  Each slot owns a solver handle,
+and with it a CUDA stream, so admitted requests run concurrently on the GPU;
+a slot keeps its handle (model, fields and psi slabs resident on the device)
+and reuses it for the next request of the same grid.  The C-ABI calls release
+the GIL, so slots are host threads.
+
+Latency = completion - arrival.  ``serial_latencies`` gives the plain path
+for comparison: one request at a time, in arrival order, on one handle.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Optional
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float               # seconds after the start of the run
+    workload: object             # workloads.Workload
+    mode: str = "forward"        # "forward" or "gradient"
+    obs: Optional[np.ndarray] = None
+    checkpoint_every: int = 200
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    start: float
+    done: float
+    slot: int
+    output: object = None
+    error: Optional[str] = None
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def estimate_bytes(wl, mode: str = "forward", checkpoint_every: int = 200) -> int:
+    """Device memory a request needs on a fresh handle (fields, psi slabs,
+    model, traces, DFT ring/accumulators; for gradients the checkpoint and
+    segment-history buffers)."""
+    cp = wl.cp
+    esz = 8 if cp.precision == 1 else 4
+    px = -(-cp.nx // 32) * 32
+    fshot = px * cp.ny * cp.nz
+    ns = len(wl.shots)
+    nc = cp.ncpml
+    slab = 2 * (nc * cp.ny * cp.nz + cp.nz * nc * px + nc * cp.ny * px)  # both slab groups, rough
+    b = ns * (6 * fshot + 4 * slab) * esz + 2 * fshot * esz
+    b += ns * len(wl.receivers) * wl.nt * esz + ns * len(wl.receivers) * len(wl.omega) * 16
+    if wl.volume_dft:
+        b += 32 * 3 * ns * fshot * esz + ns * 3 * len(wl.omega) * fshot * 16
+    if mode == "gradient":
+        K = checkpoint_every
+        ncheck = -(-wl.nt // K)
+        b += ns * esz * ((K + 1) * 6 * fshot + ncheck * (6 * fshot + 4 * slab) + 19 * fshot) + ns * 8 * fshot
+    return int(b)
+
+
+def run_request(solver_cache: dict, req: Request):
+    """Default executor: solve one request on a cached handle of its grid."""
+    from dataclasses import replace
+
+    from .solver import MittetSolver
+
+    wl = req.workload
+    key = (wl.cp.nx, wl.cp.ny, wl.cp.nz, wl.cp.precision, wl.cp.flavor, wl.cp.dx, wl.cp.dt, wl.cp.cmax,
+           wl.cp.ncpml, wl.cp.device)
+    s = solver_cache.get(key)
+    if s is None:
+        for k in list(solver_cache):
+            solver_cache.pop(k).close()
+        s = MittetSolver(wl.cp)
+        solver_cache[key] = s
+    s.set_model(wl.sigma, wl.mu)
+    s.set_shots(wl.shots)
+    s.set_wavelet(wl.wavelet)
+    s.set_receivers(wl.receivers)
+    s.set_freqs(wl.omega)
+    s.set_volume_dft(wl.volume_dft) if wl.volume_dft else s.set_volume_dft("")
+    if req.mode == "gradient":
+        return s.gradient(wl.nt, req.obs, req.checkpoint_every)
+    spec, _ = s.forward(wl.nt)
+    return spec
+
+
+class MittetServer:
+    def __init__(self, n_slots: int = 4, hbm_budget: float = 150e9,
+                 executor: Optional[Callable] = None, estimator: Optional[Callable] = None):
+        self.n_slots = n_slots
+        self.budget = float(hbm_budget)
+        self.executor = executor or run_request
+        self.estimator = estimator or (lambda r: estimate_bytes(r.workload, r.mode, r.checkpoint_every))
+        self._lock = threading.Condition()
+        self.peak_in_use = 0.0
+        self.max_concurrent = 0
+
+    def run(self, requests: list, realtime: bool = True) -> list:
+        """Serve ``requests`` (sorted by arrival); returns one Result per request."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            if self.estimator(r) > self.budget:
+                raise ValueError(f"request {r.rid} needs more than the whole HBM budget")
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+        waiting: list = []
+        results: dict = {}
+        free_slots = list(range(self.n_slots))
+        caches = [dict() for _ in range(self.n_slots)]
+        state = {"in_use": 0.0, "running": 0}
+        threads = []
+
+        def worker(slot, req, need, start):
+            out, err = None, None
+            try:
+                out = self.executor(caches[slot], req)
+            except Exception as ex:  # reported per request
+                err = f"{type(ex).__name__}: {ex}"
+            done = now()
+            with self._lock:
+                results[req.rid] = Result(req.rid, req.arrival, start, done, slot, out, err)
+                state["in_use"] -= need
+                state["running"] -= 1
+                free_slots.append(slot)
+                self._lock.notify_all()
+
+        pending = list(reqs)
+        with self._lock:
+            while pending or waiting or state["running"] > 0:
+                t = now()
+                while pending and (not realtime or pending[0].arrival <= t):
+                    waiting.append(pending.pop(0))
+                # admit in arrival order; a request that does not fit lets smaller ones pass
+                admitted = True
+                while admitted:
+                    admitted = False
+                    for r in list(waiting):
+                        if not free_slots:
+                            break
+                        need = self.estimator(r)
+                        if state["in_use"] + need <= self.budget:
+                            waiting.remove(r)
+                            slot = free_slots.pop(0)
+                            state["in_use"] += need
+                            state["running"] += 1
+                            self.peak_in_use = max(self.peak_in_use, state["in_use"])
+                            self.max_concurrent = max(self.max_concurrent, state["running"])
+                            th = threading.Thread(target=worker, args=(slot, r, need, now()), daemon=True)
+                            threads.append(th)
+                            th.start()
+                            admitted = True
+                            break
+                if not pending and not waiting and state["running"] == 0:
+                    break
+                timeout = None
+                if pending and realtime:
+                    timeout = max(0.0, pending[0].arrival - now())
+                self._lock.wait(timeout=timeout if timeout is not None else 0.5)
+        for th in threads:
+            th.join()
+        for c in caches:
+            for s in c.values():
+                s.close()
+        return [results[r.rid] for r in reqs]
+
+
+def serial_latencies(requests: list, service_times: dict) -> dict:
+    """Plain path: one request at a time in arrival order; returns rid -> latency."""
+    t = 0.0
+    out = {}
+    for r in sorted(requests, key=lambda r: r.arrival):
+        start = max(t, r.arrival)
+        t = start + service_times[r.rid]
+        out[r.rid] = t - r.arrival
+    return out
+
+
+def percentile(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=float), q)) if len(xs) else float("nan")
+
+
+def poisson_requests(n: int, rate: float, make_workload: Callable[[int, np.random.Generator], object],
+                     seed: int = 2026, gradient_every: int = 4) -> list:
+    """n requests with Poisson arrivals at ``rate`` per second; every
+    ``gradient_every``-th request is a gradient (forward:gradient = 3:1)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        wl = make_workload(i, rng)
+        mode = "gradient" if gradient_every and i % gradient_every == gradient_every - 1 else "forward"
+        obs = None
+        if mode == "gradient":
+            obs = np.zeros((len(wl.shots), len(wl.receivers), len(wl.omega)), dtype=complex)
+        out.append(Request(i, t, wl, mode, obs, checkpoint_every=max(1, min(200, wl.nt // 4))))
+    return out

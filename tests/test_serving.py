@@ -1,0 +1,70 @@
+"""CPU tests of the serving loop's admission logic with a stand-in executor
+(no GPU): the HBM budget is never exceeded, every request completes once,
+requests overlap when slots and memory allow, and a request too large to fit
+lets smaller later ones through."""
+import threading
+import time
+
+import pytest
+
+from mittet_main_b200.serving import MittetServer, Request, percentile, serial_latencies
+
+
+class FakeWL:
+    pass
+
+
+def make(rid, arrival, size):
+    r = Request(rid, arrival, FakeWL())
+    r.size = size
+    return r
+
+
+def test_budget_respected_and_all_complete():
+    lock = threading.Lock()
+    live = {"bytes": 0, "peak": 0}
+
+    def execu(cache, req):
+        with lock:
+            live["bytes"] += req.size
+            live["peak"] = max(live["peak"], live["bytes"])
+        time.sleep(0.02)
+        with lock:
+            live["bytes"] -= req.size
+        return req.rid * 10
+
+    reqs = [make(i, 0.002 * i, size=(30 if i % 3 else 70)) for i in range(24)]
+    srv = MittetServer(n_slots=4, hbm_budget=100, executor=execu, estimator=lambda r: r.size)
+    res = srv.run(reqs)
+    assert sorted(r.rid for r in res) == list(range(24))
+    assert all(r.output == r.rid * 10 and r.error is None for r in res)
+    assert live["peak"] <= 100 and srv.peak_in_use <= 100
+    assert srv.max_concurrent >= 2
+
+
+def test_small_requests_pass_a_blocked_large_one():
+    order = []
+
+    def execu(cache, req):
+        order.append(req.rid)
+        time.sleep(0.05 if req.rid == 0 else 0.01)
+        return None
+
+    reqs = [make(0, 0.0, 60), make(1, 0.001, 60), make(2, 0.002, 10), make(3, 0.003, 10)]
+    srv = MittetServer(n_slots=4, hbm_budget=100, executor=execu, estimator=lambda r: r.size)
+    res = {r.rid: r for r in srv.run(reqs)}
+    # request 1 (60) cannot start while 0 (60) runs; 2 and 3 (10 each) can
+    assert res[2].start < res[1].start and res[3].start < res[1].start
+
+
+def test_oversized_request_is_rejected():
+    srv = MittetServer(n_slots=2, hbm_budget=10, executor=lambda c, r: None, estimator=lambda r: r.size)
+    with pytest.raises(ValueError):
+        srv.run([make(0, 0.0, 11)])
+
+
+def test_serial_latency_model():
+    reqs = [make(0, 0.0, 1), make(1, 0.5, 1), make(2, 0.6, 1)]
+    lat = serial_latencies(reqs, {0: 1.0, 1: 1.0, 2: 1.0})
+    assert lat == {0: 1.0, 1: 1.5, 2: 2.4}
+    assert percentile([1, 2, 3, 4], 50) == 2.5
