@@ -115,18 +115,15 @@ _lock = threading.Lock()
 
 
 def load(build_if_missing: bool = True):
-    """Load the in-tree library, building it first if it is missing or stale."""
+    """Load the in-tree library, building it first only if it does not exist
+    (rebuilds are explicit: ``python mittet_main_b200/build.py``)."""
     global _lib
     with _lock:
         if _lib is not None:
             return _lib
-        if build_if_missing:
+        if build_if_missing and not os.path.exists(LIB_PATH):
             from . import build as _build
-            try:
-                _build.build()
-            except Exception:
-                if not os.path.exists(LIB_PATH):
-                    raise
+            _build.build(force=True)
         lib = ctypes.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(lib, name)
