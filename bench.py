@@ -157,6 +157,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain_gpu", choices=["plain_gpu", "batched", "plain_cpu"])
+    ap.add_argument("--mode", default="solve", choices=["solve", "batching", "gradient", "serving"],
+                    help="solve: the headline line; batching/gradient/serving: the other workloads' reports")
+    ap.add_argument("--requests", type=int, default=24, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate per second")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--nt", type=int, default=0, help="override Nt (0 = workload default)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -187,6 +191,10 @@ def main():
         if rank != 0:
             return
         print(json.dumps(run_reference(args, wl)), flush=True)
+        return
+    if args.mode != "solve":
+        from mittet_main_b200 import benchmarks
+        print(json.dumps(getattr(benchmarks, args.mode)(args)), flush=True)
         return
 
     import torch

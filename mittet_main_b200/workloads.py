@@ -150,6 +150,21 @@ def gradient_case(nt: int = 4000, nx=128, ny=128, nz=96, nshot=16, precision=FP3
                     2 * np.pi * np.array([0.25, 0.5, 1.0]), fmax=fmax)
 
 
+def serving_case(nx, ny, nz, nshot, nt, seed=2026, precision=FP32) -> Workload:
+    """One serving request: its own seeded log-normal model on a grid whose
+    domain is 6.4 km wide (dx = 6400/nx), nshot surface dipoles, Nt steps."""
+    d = 6400.0 / nx
+    sig = c2_model(nx, ny, nz, seed)
+    cp, fmax = _time_base(sig, d, precision=precision, nx=nx, ny=ny, nz=nz, ncpml=min(16, nx // 6))
+    kz = cp.ncpml + 3
+    m = max(1, int(np.ceil(np.sqrt(nshot))))
+    pos = surface_grid(nx, ny, cp.ncpml, m)[:nshot]
+    shots = [Shot(points=[(x, y, kz, "ex" if s % 2 == 0 else "ey", SRC_ELECTRIC, 1.0)]) for s, (x, y) in enumerate(pos)]
+    rec = [(x, y, kz, comp) for (x, y) in surface_grid(nx, ny, cp.ncpml, 6) for comp in ("ex", "ey")]
+    w = firstderiv_gauss(nt + 1, cp.dt, fmax)
+    return Workload(f"serve_{nx}x{ny}x{nz}x{nshot}", cp, sig, shots, rec, nt, w, 2 * np.pi * FREQS4, fmax=fmax)
+
+
 def small_case(n=(40, 36, 32), ncpml=8, nt=200, precision=FP32, flavor=FLAVOR_NCVER0027, seed=7,
                magnetic=False) -> Workload:
     """A random small case for parity tests (every slab and corner populated)."""
