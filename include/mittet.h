@@ -199,10 +199,15 @@ int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *
  * H phase, sampling, volume-DFT flush (0 where a kernel did not run). */
 int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms);
 
-/* Stencil variant the autotuner chose for the E and H phases at the last
- * forward: {VX, BX, BY, KZ} = x cells per thread, thread tile in x and y,
- * z cells per thread. */
+/* Stencil variant the autotuner chose for the interior launch of the E and
+ * H phases at the last forward: {VX, BX, BY, ZC} = x cells per thread,
+ * thread block in x and y, z planes each thread marches through. */
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
+
+/* All chosen variants: cfg[24] = [phase E, H][launch interior, faces,
+ * edges][VX, BX, BY, ZC].  VX = 0 marks the TMA-staged interior kernel, whose
+ * BX x BY is then its tile in cells. */
+int mittet_tuned_variants(mittet_handle *h, int32_t *cfg);
 
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);

@@ -224,70 +224,59 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 
 // ---------------------------------------------------- full-volume f_to_d
 //
-// Every ring_k steps the E phase has left the last ring_k values of each
+// Every ring_k (= 32) steps the E phase has left the last values of each
 // selected E component in the ring; this kernel folds them into the FP64
 // accumulators:
 //   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring(vc, shot*fshot + cell, s),
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
-// One thread per (component, shot, cell).  The sum over the ring is formed in
-// the field precision T (at most 32 terms; for FP32 fields the partial sum
-// carries ~1e-7 relative error) and added to the FP64 accumulator once per
-// flush.  Ring values are loaded 16 at a time before any arithmetic; the
-// weights of the flush sit in shared memory.
+// Grid (cells, component, shot), one thread per cell.  A thread issues its
+// 32 ring loads (one 128-byte line per warp each) before any arithmetic, forms
+// the sum over the ring in the field precision T (at most 32 terms; for FP32
+// fields the partial sum carries ~1e-7 relative error) and adds it to the FP64
+// accumulators once per flush.  The weights of one group of up to four
+// frequencies are a by-value kernel parameter (zero for s >= cnt), so every
+// multiply reads its weight from the constant bank.
+constexpr int kFlushRing = 32;
+constexpr int kFlushFreqs = 4;
+template <typename T>
+struct FlushWeights {
+    T wr[kFlushRing][kFlushFreqs];
+    T wi[kFlushRing][kFlushFreqs];
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int ring_k,
-                                                         int nvc, int3 vcs, long long fshot, int cnt, int n0,
-                                                         const double2 *__restrict__ wt, int nf,
+                                                         int3 vcs, long long fshot, int cnt, int f0, int nf,
+                                                         const __grid_constant__ FlushWeights<T> w,
                                                          double2 *__restrict__ acc) {
-    extern __shared__ unsigned char sw_raw[];
-    T *swr = reinterpret_cast<T *>(sw_raw);  // [cnt][nf] real parts
-    T *swi = swr + cnt * nf;                 // [cnt][nf] imaginary parts
-    for (int q = threadIdx.x; q < cnt * nf; q += blockDim.x) {
-        const double2 w = wt[(long long)n0 * nf + q];
-        swr[q] = (T)w.x;
-        swi[q] = (T)w.y;
-    }
-    __syncthreads();
-    const long long tot = ring_comp * nvc;
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < tot; g += (long long)gridDim.x * blockDim.x) {
-        const int vi = (int)(g / ring_comp);
-        const long long e = g - (long long)vi * ring_comp;
-        const int vc = vi == 0 ? vcs.x : (vi == 1 ? vcs.y : vcs.z);
-        const long long shot = e / fshot;
-        const long long cell = e - shot * fshot;
-        double2 *__restrict__ ap = acc + ((shot * 3 + vc) * nf) * fshot + cell;
-        const T *__restrict__ rp = ring + ring_index(ring_comp, ring_k, vc, e, 0);
-        for (int f0 = 0; f0 < nf; f0 += 8) {
-            const int fn = min(8, nf - f0);
-            T pr[8], pi[8];
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= fshot) return;
+    const int vi = blockIdx.y, shot = blockIdx.z;
+    const int vc = vi == 0 ? vcs.x : (vi == 1 ? vcs.y : vcs.z);
+    const long long e = (long long)shot * fshot + cell;
+    const T *__restrict__ rp = ring + ring_index(ring_comp, ring_k, vc, e, 0);
+    T xs[kFlushRing];
 #pragma unroll
-            for (int f = 0; f < 8; f++) { pr[f] = T(0); pi[f] = T(0); }
-            for (int s0 = 0; s0 < cnt; s0 += 16) {
-                T xs[16];
+    for (int s = 0; s < kFlushRing; s++) xs[s] = s < cnt ? __ldg(rp + s * 32) : T(0);
+    T pr[kFlushFreqs], pi[kFlushFreqs];
 #pragma unroll
-                for (int s = 0; s < 16; s++)
-                    xs[s] = (s0 + s < cnt) ? __ldg(rp + (long long)(s0 + s) * 32) : T(0);
+    for (int f = 0; f < kFlushFreqs; f++) { pr[f] = T(0); pi[f] = T(0); }
 #pragma unroll
-                for (int s = 0; s < 16; s++) {
-                    if (s0 + s < cnt) {
-                        const T *wr = swr + (s0 + s) * nf + f0;
-                        const T *wi = swi + (s0 + s) * nf + f0;
+    for (int s = 0; s < kFlushRing; s++)
 #pragma unroll
-                        for (int f = 0; f < 8; f++)
-                            if (f < fn) { pr[f] = fma(wr[f], xs[s], pr[f]); pi[f] = fma(wi[f], xs[s], pi[f]); }
-                    }
-                }
-            }
-#pragma unroll
-            for (int f = 0; f < 8; f++)
-                if (f < fn) {
-                    double2 v = ap[(long long)(f0 + f) * fshot];
-                    v.x += (double)pr[f];
-                    v.y += (double)pi[f];
-                    ap[(long long)(f0 + f) * fshot] = v;
-                }
+        for (int f = 0; f < kFlushFreqs; f++) {
+            pr[f] = fma(w.wr[s][f], xs[s], pr[f]);
+            pi[f] = fma(w.wi[s][f], xs[s], pi[f]);
         }
-    }
+    double2 *__restrict__ ap = acc + (((long long)shot * 3 + vc) * nf + f0) * fshot + cell;
+#pragma unroll
+    for (int f = 0; f < kFlushFreqs; f++)
+        if (f0 + f < nf) {
+            double2 v = ap[(long long)f * fshot];
+            v.x += (double)pr[f];
+            v.y += (double)pi[f];
+            ap[(long long)f * fshot] = v;
+        }
 }
 
 // Non-finite check of the receiver traces: sets *flag if any sample is NaN/Inf.

@@ -6,6 +6,8 @@
 // full-volume DFT ring and accumulators.  mittet_forward() runs the time loop
 // as one CUDA graph of G steps replayed nt/G times, then the f_to_d
 // transform of the receiver traces.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -15,14 +17,17 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/mittet.h"
 #include "kernels.cuh"
+#include "tma_interior.cuh"
 #include "adjoint.cuh"
 #include "setup_host.h"
 
@@ -126,14 +131,23 @@ struct mittet_handle_s {
     DevBuf d_omega;
 
     uint32_t vmask = 0;
-    int ring_k = 32;
-    int var_e = 0, var_h = 0;  // stencil variants (index into variants<T>())
+    int ring_k = kFlushRing;  // ring depth = steps per graph and per volume-DFT flush
+    int var_e[3] = {0, 0, 0};  // stencil variant (index into variants<T>()) of the
+    int var_h[3] = {0, 0, 0};  // interior, face and edge launches of each phase;
+                               // var[0] = -1 - c selects TMA interior config c
+    TmaMaps tma_maps[2];       // tensor maps of the E and H interior (current buffers)
+    int tma_nown[2] = {0, 0};
+    bool tma_ok = false;
+    int ibox[2][6] = {{0}};    // interior box of each phase: lo xyz, hi xyz
+    bool has_ibox[2] = {false, false};
+    int ldg_int[2] = {0, 0};   // best plain-load interior variant of each phase
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
     int tiles[64] = {0};       // tiles per (variant, phase)
     int tiles_int[64] = {0};   // tiles [0, tiles_int) interior
     int tiles_face[64] = {0};  // tiles [tiles_int, tiles_face) faces
     bool tuned = false;
-    DevBuf ring, acc, wtab;
+    DevBuf ring, acc;
+    std::vector<double> wt_host;  // volume-DFT weights [n][f] (re, im)
 
     DevBuf fields[6], psiE[3][2], psiH[3][2];
     int alloc_shots = -1;
@@ -229,11 +243,11 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
     return a;
 }
 
-// Stencil variants (VX x cells and KZ z cells per thread, BX x BY threads)
+// Stencil variants (VX x cells per thread, BX x BY threads, ZC z planes per thread)
 // the autotuner picks from.
 template <typename T>
 struct Variant {
-    int vx, bx, by, kz;
+    int vx, bx, by, zc;
     void (*ei)(PhaseArgs<T>, const TileMap *);
     void (*hi)(PhaseArgs<T>, const TileMap *);
     void (*ef)(PhaseArgs<T>, const TileMap *, int);
@@ -248,10 +262,10 @@ const std::vector<Variant<T>> &variants();
 template <>
 const std::vector<Variant<float>> &variants<float>() {
     static const std::vector<Variant<float>> v = {
-#define MITTET_X(vx, bx, by, kz)                                                                      \
-    {vx, bx, by, kz, e_interior_kernel<float, vx, bx, by, kz>, h_interior_kernel<float, vx, bx, by, kz>, \
-     e_face_kernel<float, vx, bx, by, kz>, h_face_kernel<float, vx, bx, by, kz>,                         \
-     e_shell_kernel<float, vx, bx, by, kz>, h_shell_kernel<float, vx, bx, by, kz>},
+#define MITTET_X(vx, bx, by, zc)                                                              \
+    {vx, bx, by, zc, e_interior_kernel<float, vx, bx, by>, h_interior_kernel<float, vx, bx, by>, \
+     e_face_kernel<float, vx, bx, by>, h_face_kernel<float, vx, bx, by>,                         \
+     e_shell_kernel<float, vx, bx, by>, h_shell_kernel<float, vx, bx, by>},
         MITTET_STENCIL_VARIANTS_F32(MITTET_X)
 #undef MITTET_X
     };
@@ -260,10 +274,10 @@ const std::vector<Variant<float>> &variants<float>() {
 template <>
 const std::vector<Variant<double>> &variants<double>() {
     static const std::vector<Variant<double>> v = {
-#define MITTET_X(vx, bx, by, kz)                                                                        \
-    {vx, bx, by, kz, e_interior_kernel<double, vx, bx, by, kz>, h_interior_kernel<double, vx, bx, by, kz>, \
-     e_face_kernel<double, vx, bx, by, kz>, h_face_kernel<double, vx, bx, by, kz>,                         \
-     e_shell_kernel<double, vx, bx, by, kz>, h_shell_kernel<double, vx, bx, by, kz>},
+#define MITTET_X(vx, bx, by, zc)                                                                \
+    {vx, bx, by, zc, e_interior_kernel<double, vx, bx, by>, h_interior_kernel<double, vx, bx, by>, \
+     e_face_kernel<double, vx, bx, by>, h_face_kernel<double, vx, bx, by>,                         \
+     e_shell_kernel<double, vx, bx, by>, h_shell_kernel<double, vx, bx, by>},
         MITTET_STENCIL_VARIANTS_F64(MITTET_X)
 #undef MITTET_X
     };
@@ -301,18 +315,20 @@ void interior_box(const mittet_handle *h, bool e, int lo[3], int hi[3]) {
     }
 }
 
-TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int kz) {
+TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int zc) {
     TileMap t;
     memset(&t, 0, sizeof(t));
+    t.zc = zc;
     const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
     const int TX = bx * vx;
     int lo[3], hi[3];
     interior_box(h, e, lo, hi);
-    // x box edges are multiples of 4 cells, so every vector width divides them
-    const int X0 = (lo[0] + 3) / 4 * 4;
-    const int ntx = hi[0] > X0 ? (hi[0] - X0) / TX : 0;
-    const int nty = hi[1] > lo[1] ? (hi[1] - lo[1]) / by : 0;
-    const int ntz = hi[2] > lo[2] ? (hi[2] - lo[2]) / kz : 0;
+    // The boxes do not depend on the variant: x box edges are multiples of 4
+    // cells (every vector width divides them); partial tiles in x and y are
+    // masked and the last z chunk of a box is cut at the box edge.
+    const int X0 = (lo[0] + 3) / 4 * 4, X1 = hi[0] / 4 * 4;
+    const int Y0 = lo[1], Y1 = hi[1];
+    const int Z0 = lo[2], Z1 = hi[2];
     auto add = [&](int kind, int x0, int y0, int z0, int x1, int y1, int z1) {
         if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
         const int q = t.nbox++;
@@ -321,11 +337,10 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
         t.hi[q][0] = x1; t.hi[q][1] = y1; t.hi[q][2] = z1;
         t.ntx[q] = (x1 - x0 + TX - 1) / TX;
         t.nty[q] = (y1 - y0 + by - 1) / by;
-        const int nzt = (z1 - z0 + kz - 1) / kz;
+        const int nzt = (z1 - z0 + zc - 1) / zc;
         t.start[q + 1] = t.start[q] + t.ntx[q] * t.nty[q] * nzt;
     };
-    if (ntx > 0 && nty > 0 && ntz > 0) {
-        const int X1 = X0 + ntx * TX, Y0 = lo[1], Y1 = lo[1] + nty * by, Z0 = lo[2], Z1 = lo[2] + ntz * kz;
+    if (X1 > X0 && Y1 > Y0 && Z1 > Z0) {
         add(0, X0, Y0, Z0, X1, Y1, Z1);
         t.g0 = t.start[t.nbox];
         add(1, 0, Y0, Z0, X0, Y1, Z1);   // x faces
@@ -359,8 +374,8 @@ int upload_tilemaps(mittet_handle *h) {
     const auto &vs = variants<T>();
     std::vector<TileMap> maps(2 * vs.size());
     for (size_t v = 0; v < vs.size(); v++) {
-        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].kz);
-        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].kz);
+        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc);
+        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc);
         for (int p = 0; p < 2; p++) {
             const TileMap &t = maps[2 * v + p];
             h->tiles[2 * v + p] = t.start[t.nbox];
@@ -368,40 +383,189 @@ int upload_tilemaps(mittet_handle *h) {
             h->tiles_face[2 * v + p] = t.g1;
         }
     }
+    for (int p = 0; p < 2; p++) {  // the interior box (identical in every variant's map)
+        const TileMap &t = maps[p];
+        h->has_ibox[p] = t.g0 > 0;
+        for (int q = 0; q < 3; q++) {
+            h->ibox[p][q] = t.lo[0][q];
+            h->ibox[p][3 + q] = t.hi[0][q];
+        }
+    }
     CK(h->tmaps.ensure(maps.size() * sizeof(TileMap)));
     CK(cudaMemcpy(h->tmaps.p, maps.data(), maps.size() * sizeof(TileMap), cudaMemcpyHostToDevice));
     return MITTET_OK;
 }
 
-// One phase = the interior kernel over the interior tiles, then the shell
-// kernel over the rest (two launches; the first is skipped on grids too
-// small to have an interior).  Returns the number of launches.
+// ------------------------------------------------- TMA-staged interior
+// Configurations of interior_tma_kernel the autotuner may pick for part 0:
+// tile TX x TY (TX = 64 FP32 / 32 FP64 cells, TY = 8 rows), ring depth of
+// the E and H phases, z planes per CTA.
 template <typename T>
-int launch_phase(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a) {
+struct TmaCfg {
+    int zc;
+    void (*ek)(PhaseArgs<T>, TmaTiling, TmaMaps, int, int *);
+    void (*hk)(PhaseArgs<T>, TmaTiling, TmaMaps, int, int *);
+};
+template <typename T>
+struct TmaShape {
+    static constexpr int TX = sizeof(T) == 4 ? 64 : 32, TY = 8, SE = 4, SH = 5;
+};
+
+template <typename T>
+const std::vector<TmaCfg<T>> &tma_cfgs() {
+    using S = TmaShape<T>;
+    static const std::vector<TmaCfg<T>> v = {
+        {8, interior_tma_kernel<T, S::TX, S::TY, S::SE, true>, interior_tma_kernel<T, S::TX, S::TY, S::SH, false>},
+        {16, interior_tma_kernel<T, S::TX, S::TY, S::SE, true>, interior_tma_kernel<T, S::TX, S::TY, S::SH, false>},
+        {32, interior_tma_kernel<T, S::TX, S::TY, S::SE, true>, interior_tma_kernel<T, S::TX, S::TY, S::SH, false>},
+    };
+    return v;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 3-D map of one padded field array [nzs][ny][px] with a bx x by x 1 box.
+bool encode_map(CUtensorMap *m, const void *base, bool fp64, int px, int ny, long long nzs, int bx, int by) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tma_encoder();
+    if (!fn || !base) return false;
+    const cuuint64_t esz = fp64 ? 8 : 4;
+    const cuuint64_t dims[3] = {(cuuint64_t)px, (cuuint64_t)ny, (cuuint64_t)nzs};
+    const cuuint64_t strides[2] = {(cuuint64_t)px * esz, (cuuint64_t)px * ny * esz};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base),
+              dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Encodes the tensor maps of both phases for the handle's current field and
+// model buffers; a change of any map invalidates the captured graph.
+template <typename T>
+int build_tma_maps(mittet_handle *h) {
+    using S = TmaShape<T>;
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        for (const auto &c : tma_cfgs<T>()) {
+            cudaError_t e1 = cudaFuncSetAttribute(c.ek, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)TmaStage<T, S::TX, S::TY>::bytes(S::SE));
+            cudaError_t e2 = cudaFuncSetAttribute(c.hk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)TmaStage<T, S::TX, S::TY>::bytes(S::SH));
+            if (e1 != cudaSuccess) attr_err = e1;
+            if (e2 != cudaSuccess) attr_err = e2;
+        }
+    });
+    const char *mode = std::getenv("MITTET_INTERIOR");
+    if (attr_err != cudaSuccess || (mode && std::string(mode) == "ldg")) {
+        h->tma_ok = false;
+        return MITTET_OK;
+    }
+    const int px = h->px, ny = h->g.ny, nz = h->g.nz, TX = S::TX, TY = S::TY, PA = TX + 8;
+    const long long nzs = (long long)nz * h->nshot;
+    const bool f64 = h->fp64;
+    TmaMaps me, mh;
+    memset(&me, 0, sizeof(me));
+    memset(&mh, 0, sizeof(mh));
+    auto F = [&](int c) { return h->fields[c].p; };
+    bool ok = encode_map(&me.map[0], F(5), f64, px, ny, nzs, PA, TY + 3) &&   // Hz, x and y halo
+              encode_map(&me.map[1], F(4), f64, px, ny, nzs, PA, TY) &&       // Hy, x halo
+              encode_map(&me.map[2], F(3), f64, px, ny, nzs, TX, TY + 3) &&   // Hx, y halo
+              encode_map(&me.map[3], h->m.p, f64, px, ny, nz, TX, TY) &&      // m
+              encode_map(&me.map[4], F(0), f64, px, ny, nzs, TX, TY) &&
+              encode_map(&me.map[5], F(1), f64, px, ny, nzs, TX, TY) &&
+              encode_map(&me.map[6], F(2), f64, px, ny, nzs, TX, TY) &&
+              encode_map(&mh.map[0], F(2), f64, px, ny, nzs, PA, TY + 3) &&   // Ez, x and y halo
+              encode_map(&mh.map[1], F(1), f64, px, ny, nzs, PA, TY) &&       // Ey, x halo
+              encode_map(&mh.map[2], F(0), f64, px, ny, nzs, TX, TY + 3) &&   // Ex, y halo
+              encode_map(&mh.map[3], F(3), f64, px, ny, nzs, TX, TY) &&
+              encode_map(&mh.map[4], F(4), f64, px, ny, nzs, TX, TY) &&
+              encode_map(&mh.map[5], F(5), f64, px, ny, nzs, TX, TY);
+    if (ok && h->has_mu) ok = encode_map(&mh.map[6], h->dtmu.p, f64, px, ny, nz, TX, TY);
+    if (ok && (!h->tma_ok || memcmp(&me, &h->tma_maps[0], sizeof(me)) || memcmp(&mh, &h->tma_maps[1], sizeof(mh))))
+        drop_graph(h);
+    h->tma_ok = ok;
+    h->tma_maps[0] = me;
+    h->tma_maps[1] = mh;
+    h->tma_nown[0] = 4;
+    h->tma_nown[1] = h->has_mu ? 4 : 3;
+    return MITTET_OK;
+}
+
+// The interior of one phase with TMA config ci.
+template <typename T>
+int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a) {
+    using S = TmaShape<T>;
+    const int p = e ? 0 : 1;
+    if (!h->has_ibox[p]) return 0;
+    const TmaCfg<T> &c = tma_cfgs<T>()[ci];
+    const int *ib = h->ibox[p];
+    TmaTiling tl;
+    tl.x0 = ib[0]; tl.y0 = ib[1]; tl.z0 = ib[2];
+    tl.x1 = ib[3]; tl.y1 = ib[4]; tl.z1 = ib[5];
+    tl.ntx = (tl.x1 - tl.x0 + S::TX - 1) / S::TX;
+    tl.nty = (tl.y1 - tl.y0 + S::TY - 1) / S::TY;
+    tl.zc = c.zc;
+    const int nzc = (tl.z1 - tl.z0 + c.zc - 1) / c.zc;
+    const dim3 grid(tl.ntx * tl.nty * nzc, h->nshot), block(S::TX / 2, S::TY);
+    const size_t smem = TmaStage<T, S::TX, S::TY>::bytes(e ? S::SE : S::SH);
+    (e ? c.ek : c.hk)<<<grid, block, smem, h->st>>>(a, tl, h->tma_maps[p], h->tma_nown[p], h->d_flag.as<int>());
+    return 1;
+}
+
+// True when a phase's arguments are the handle's own buffers (the ones the
+// tensor maps describe).
+template <typename T>
+bool tma_usable(const mittet_handle *h, const PhaseArgs<T> &a) {
+    return h->tma_ok && a.f[0] == h->fields[0].as<T>() && a.m == h->m.as<T>();
+}
+
+// One part of a phase (0 interior, 1 faces, 2 edges and corners) with
+// variant vi (vi < 0: TMA interior config -1 - vi); returns 1 if it
+// launched a kernel.
+template <typename T>
+int launch_part(mittet_handle *h, bool e, int part, int vi, const PhaseArgs<T> &a) {
+    if (vi < 0) {
+        if (part == 0 && tma_usable<T>(h, a)) return launch_tma<T>(h, e, -1 - vi, a);
+        vi = h->ldg_int[e ? 0 : 1];  // other buffers (gradient replays): best plain-load body
+    }
     const Variant<T> &v = variants<T>()[vi];
     const int slot = 2 * vi + (e ? 0 : 1);
     const TileMap *tm = h->tmaps.as<TileMap>() + slot;
     const int g0 = h->tiles_int[slot], g1 = h->tiles_face[slot], n_all = h->tiles[slot];
-    dim3 block(v.bx, v.by);
-    int n = 0;
-    if (g0 > 0) {
-        dim3 grid(g0, h->nshot);
+    const int first = part == 0 ? 0 : (part == 1 ? g0 : g1);
+    const int last = part == 0 ? g0 : (part == 1 ? g1 : n_all);
+    if (last <= first) return 0;
+    dim3 block(v.bx, v.by), grid(last - first, h->nshot);
+    if (part == 0) {
         if (e) v.ei<<<grid, block, 0, h->st>>>(a, tm);
         else v.hi<<<grid, block, 0, h->st>>>(a, tm);
-        n++;
+    } else if (part == 1) {
+        if (e) v.ef<<<grid, block, 0, h->st>>>(a, tm, first);
+        else v.hf<<<grid, block, 0, h->st>>>(a, tm, first);
+    } else {
+        if (e) v.es<<<grid, block, 0, h->st>>>(a, tm, first);
+        else v.hs<<<grid, block, 0, h->st>>>(a, tm, first);
     }
-    if (g1 > g0) {
-        dim3 grid(g1 - g0, h->nshot);
-        if (e) v.ef<<<grid, block, 0, h->st>>>(a, tm, g0);
-        else v.hf<<<grid, block, 0, h->st>>>(a, tm, g0);
-        n++;
-    }
-    if (n_all > g1) {
-        dim3 grid(n_all - g1, h->nshot);
-        if (e) v.es<<<grid, block, 0, h->st>>>(a, tm, g1);
-        else v.hs<<<grid, block, 0, h->st>>>(a, tm, g1);
-        n++;
-    }
+    return 1;
+}
+
+// One phase = interior, faces, edges (up to three launches, each part with
+// its own variant).  Returns the number of launches.
+template <typename T>
+int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a) {
+    int n = 0;
+    for (int part = 0; part < 3; part++) n += launch_part<T>(h, e, part, vi[part], a);
     return n;
 }
 
@@ -422,17 +586,23 @@ void launch_step(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &h
 // fields, so the state is untouched apart from the ring slot written by the
 // E phase).  Results are cached for the process.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 8>> g_tune_cache;
 
 template <typename T>
 int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
-    const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0);
+    const char *imode = std::getenv("MITTET_INTERIOR");  // "ldg" / "tma": restrict the interior body
+    const bool only_ldg = imode && std::string(imode) == "ldg";
+    const bool only_tma = imode && std::string(imode) == "tma" && tma_usable<T>(h, ea) && tma_usable<T>(h, ha);
+    const bool try_tma = !only_ldg && tma_usable<T>(h, ea) && tma_usable<T>(h, ha);
+    const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0,
+                                     (try_tma ? 1 : 0) + (only_tma ? 2 : 0));
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            h->var_e = it->second.first;
-            h->var_h = it->second.second;
+            for (int p = 0; p < 3; p++) { h->var_e[p] = it->second[p]; h->var_h[p] = it->second[3 + p]; }
+            h->ldg_int[0] = it->second[6];
+            h->ldg_int[1] = it->second[7];
             return MITTET_OK;
         }
     }
@@ -440,53 +610,89 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     const int nv = (int)variants<T>().size();
     if (fix) {
         const int v = std::atoi(fix);
-        if (v >= 0 && v < nv) { h->var_e = h->var_h = v; return MITTET_OK; }
+        if (v >= 0 && v < nv) {
+            for (int p = 0; p < 3; p++) h->var_e[p] = h->var_h[p] = v;
+            h->ldg_int[0] = h->ldg_int[1] = v;
+            if (only_tma) h->var_e[0] = h->var_h[0] = -1;
+            return MITTET_OK;
+        }
     }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     const long long cells = (long long)h->nshot * h->g.nx * h->g.ny * h->g.nz;
-    const int reps = cells > (1LL << 24) ? 2 : (cells > (1LL << 20) ? 5 : 20);
-    float best[2] = {1e30f, 1e30f};
-    for (int v = 0; v < nv; v++) {
-        for (int ph = 0; ph < 2; ph++) {
-            const PhaseArgs<T> &a = ph == 0 ? ea : ha;
-            launch_phase<T>(h, ph == 0, v, a);  // warm-up
-            CK(cudaEventRecord(e0, h->st));
-            for (int r = 0; r < reps; r++) launch_phase<T>(h, ph == 0, v, a);
-            CK(cudaEventRecord(e1, h->st));
-            CK(cudaEventSynchronize(e1));
-            CK(cudaGetLastError());
-            float ms = 0;
-            CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (std::getenv("MITTET_TUNE_LOG"))
-                fprintf(stderr, "autotune %s vx%d %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", variants<T>()[v].vx,
-                        variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].kz, ms / reps);
-            if (ms < best[ph]) {
-                best[ph] = ms;
-                (ph == 0 ? h->var_e : h->var_h) = v;
+    const int reps = cells > (1LL << 24) ? 3 : (cells > (1LL << 20) ? 8 : 20);
+    static const char *pname[3] = {"interior", "faces", "edges"};
+    for (int ph = 0; ph < 2; ph++) {
+        const PhaseArgs<T> &a = ph == 0 ? ea : ha;
+        int *var = ph == 0 ? h->var_e : h->var_h;
+        for (int part = 0; part < 3; part++) {
+            // candidates: TMA interior configs (v < 0, part 0 only), then the plain-load variants
+            float best = 1e30f, best_ldg = 1e30f;
+            var[part] = 0;
+            if (part == 0) h->ldg_int[ph] = 0;
+            const int ntma = (part == 0 && try_tma) ? (int)tma_cfgs<T>().size() : 0;
+            for (int v = -ntma; v < nv; v++) {
+                if (!launch_part<T>(h, ph == 0, part, v, a)) break;  // warm-up; part is empty
+                CK(cudaEventRecord(e0, h->st));
+                for (int r = 0; r < reps; r++) launch_part<T>(h, ph == 0, part, v, a);
+                CK(cudaEventRecord(e1, h->st));
+                CK(cudaEventSynchronize(e1));
+                CK(cudaGetLastError());
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (std::getenv("MITTET_TUNE_LOG")) {
+                    if (v < 0)
+                        fprintf(stderr, "autotune %s %s tma %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", pname[part],
+                                TmaShape<T>::TX, TmaShape<T>::TY, tma_cfgs<T>()[-1 - v].zc, ms / reps);
+                    else
+                        fprintf(stderr, "autotune %s %s vx%d %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", pname[part],
+                                variants<T>()[v].vx, variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].zc,
+                                ms / reps);
+                }
+                const bool eligible = !(only_tma && part == 0 && v >= 0);
+                if (eligible && ms < best) {
+                    best = ms;
+                    var[part] = v;
+                }
+                if (part == 0 && v >= 0 && ms < best_ldg) {
+                    best_ldg = ms;
+                    h->ldg_int[ph] = v;
+                }
             }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = std::make_pair(h->var_e, h->var_h);
+    g_tune_cache[key] = {h->var_e[0], h->var_e[1], h->var_e[2], h->var_h[0], h->var_h[1], h->var_h[2],
+                         h->ldg_int[0], h->ldg_int[1]};
     return MITTET_OK;
 }
 
+// Folds the last cnt ring steps (time steps n0 .. n0+cnt-1) into the volume
+// accumulators: one launch per group of up to four frequencies.
 template <typename T>
 void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
-    const long long tot = (long long)h->nshot * h->fshot;
     const int nf = (int)h->omega.size();
     int vc[3] = {0, 0, 0}, nvc = 0;
     for (int c = 0; c < 3; c++)
         if (h->vmask >> c & 1) vc[nvc++] = c;
-    int blocks = (int)std::min<long long>((tot * nvc + 255) / 256, 148LL * 16);
-    volume_dft_kernel<T><<<blocks, 256, (size_t)cnt * nf * 2 * sizeof(T), h->st>>>(
-        h->ring.as<T>(), tot, h->ring_k, nvc, make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, n0, h->wtab.as<double2>(), nf,
-        h->acc.as<double2>());
-    h->launches++;
+    const dim3 grid((unsigned)((h->fshot + 255) / 256), nvc, h->nshot);
+    for (int f0 = 0; f0 < nf; f0 += kFlushFreqs) {
+        FlushWeights<T> w;
+        memset(&w, 0, sizeof(w));
+        for (int s = 0; s < cnt; s++)
+            for (int f = 0; f < kFlushFreqs && f0 + f < nf; f++) {
+                const size_t q = ((size_t)(n0 + s) * nf + f0 + f) * 2;
+                w.wr[s][f] = (T)h->wt_host[q];
+                w.wi[s][f] = (T)h->wt_host[q + 1];
+            }
+        volume_dft_kernel<T><<<grid, 256, 0, h->st>>>(h->ring.as<T>(), (long long)h->nshot * h->fshot, h->ring_k,
+                                                      make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, f0, nf, w,
+                                                      h->acc.as<double2>());
+        h->launches++;
+    }
 }
 
 template <typename T>
@@ -509,7 +715,8 @@ int run_forward(mittet_handle *h, int nt) {
         CK(h->acc.ensure(acc_b));
         CK(cudaMemsetAsync(h->acc.p, 0, acc_b, h->st));
         // weights wt[n][f] = dt exp((i-1) sqrt(w0 w) n dt)
-        std::vector<double> wt((size_t)nt * nf * 2);
+        std::vector<double> &wt = h->wt_host;
+        wt.assign((size_t)nt * nf * 2, 0.0);
         for (int n = 0; n < nt; n++)
             for (int f = 0; f < nf; f++) {
                 const double xa = std::sqrt(h->ph.omega0 * h->omega[f]) * (double)n * h->ph.dt;
@@ -517,8 +724,6 @@ int run_forward(mittet_handle *h, int nt) {
                 wt[((size_t)n * nf + f) * 2] = e * std::cos(xa);
                 wt[((size_t)n * nf + f) * 2 + 1] = e * std::sin(xa);
             }
-        CK(h->wtab.ensure(wt.size() * sizeof(double)));
-        CK(cudaMemcpyAsync(h->wtab.p, wt.data(), wt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
     }
 
     PhaseArgs<T> ea = phase_args<T>(h, true);
@@ -552,6 +757,8 @@ int run_forward(mittet_handle *h, int nt) {
     sa.nt = nt;
     sa.d_step = h->d_step.as<int>();
 
+    rc = build_tma_maps<T>(h);
+    if (rc) return rc;
     if (!h->tuned) {
         rc = autotune<T>(h, ea, ha);
         if (rc) return rc;
@@ -613,6 +820,8 @@ int run_forward(mittet_handle *h, int nt) {
 template <typename T>
 int time_kernels(mittet_handle *h, int nsteps, double *ms) {
     int rc = ensure_state(h);
+    if (rc) return rc;
+    rc = build_tma_maps<T>(h);
     if (rc) return rc;
     CK(cudaMemsetAsync(h->d_step.p, 0, sizeof(int), h->st));
     const int nt = h->last_nt;
@@ -1384,6 +1593,7 @@ int mittet_forward(mittet_handle *h, int32_t nt, double *rec_fd, double *rec_td)
     int flag = 0;
     CK(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    if (flag & 2) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded wait for a TMA copy gave up");
     if (flag) return fail(MITTET_ERR_DIVERGED, "non-finite receiver samples (unstable time step or model)");
     return MITTET_OK;
 }
@@ -1481,13 +1691,34 @@ int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1
 
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg) {
     if (!h || !e_cfg || !h_cfg) return fail(MITTET_ERR_INVALID_ARG, "null argument");
-    auto fill = [&](auto &v) {
-        const auto &a = v[h->var_e], &b = v[h->var_h];
-        e_cfg[0] = a.vx; e_cfg[1] = a.bx; e_cfg[2] = a.by; e_cfg[3] = a.kz;
-        h_cfg[0] = b.vx; h_cfg[1] = b.bx; h_cfg[2] = b.by; h_cfg[3] = b.kz;
+    int32_t all[24];
+    int rc = mittet_tuned_variants(h, all);
+    if (rc) return rc;
+    for (int q = 0; q < 4; q++) {
+        e_cfg[q] = all[q];
+        h_cfg[q] = all[12 + q];
+    }
+    return MITTET_OK;
+}
+
+int mittet_tuned_variants(mittet_handle *h, int32_t *cfg) {
+    if (!h || !cfg) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    auto fill = [&](auto tag) {
+        using T = decltype(tag);
+        for (int ph = 0; ph < 2; ph++)
+            for (int p = 0; p < 3; p++) {
+                const int vi = (ph == 0 ? h->var_e : h->var_h)[p];
+                int32_t *c = cfg + (ph * 3 + p) * 4;
+                if (vi < 0) {  // TMA-staged interior: VX = 0, then the tile and z planes per CTA
+                    c[0] = 0; c[1] = TmaShape<T>::TX; c[2] = TmaShape<T>::TY; c[3] = tma_cfgs<T>()[-1 - vi].zc;
+                } else {
+                    const auto &a = variants<T>()[vi];
+                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.zc;
+                }
+            }
     };
-    if (h->fp64) fill(variants<double>());
-    else fill(variants<float>());
+    if (h->fp64) fill(double());
+    else fill(float());
     return MITTET_OK;
 }
 

@@ -50,7 +50,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[MITTET_NOALLOC_
 namespace {
 
 constexpr int NA_MAX_AXIS = 256, NA_MAX_POINTS = 64, NA_MAX_REC = 2048, NA_MAX_FREQ = 256, NA_MAX_DEV = 64;
-constexpr int NA_VX = 2, NA_BX = 32, NA_BY = 4, NA_KZ = 1;
+constexpr int NA_VX = 2, NA_BX = 32, NA_BY = 4, NA_ZC = 4;
 
 std::mutex g_na_mu;
 void *g_na_ptr[NA_MAX_DEV] = {nullptr};
@@ -238,12 +238,13 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
     TileMap tm;
     memset(&tm, 0, sizeof(tm));
     tm.nbox = 1;
+    tm.zc = NA_ZC;
     tm.g0 = tm.g1 = 0;
     tm.kind[0] = 7;
     tm.hi[0][0] = nx; tm.hi[0][1] = ny; tm.hi[0][2] = nz;
     tm.ntx[0] = (nx + NA_BX * NA_VX - 1) / (NA_BX * NA_VX);
     tm.nty[0] = (ny + NA_BY - 1) / NA_BY;
-    tm.start[1] = tm.ntx[0] * tm.nty[0] * ((nz + NA_KZ - 1) / NA_KZ);
+    tm.start[1] = tm.ntx[0] * tm.nty[0] * ((nz + NA_ZC - 1) / NA_ZC);
 
     // ---- device work, all on the caller's stream, all inside the array
     int dev = 0;
@@ -346,9 +347,9 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
     const dim3 grid(tm.start[1], 1), block(NA_BX, NA_BY);
     for (int s = 0; s < nt; s++) {
         if (has_mag) inject_kernel<float><<<1, 128, 0, st>>>(ia_m);
-        e_shell_kernel<float, NA_VX, NA_BX, NA_BY, NA_KZ><<<grid, block, 0, st>>>(pa[0], dtm, 0);
+        e_shell_kernel<float, NA_VX, NA_BX, NA_BY><<<grid, block, 0, st>>>(pa[0], dtm, 0);
         if (has_ele) inject_kernel<float><<<1, 128, 0, st>>>(ia_e);
-        h_shell_kernel<float, NA_VX, NA_BX, NA_BY, NA_KZ><<<grid, block, 0, st>>>(pa[1], dtm, 0);
+        h_shell_kernel<float, NA_VX, NA_BX, NA_BY><<<grid, block, 0, st>>>(pa[1], dtm, 0);
         sample_kernel<float><<<1, 1024, 0, st>>>(sa);
     }
     trace_dft_kernel<float><<<nf, 256, 0, st>>>((const float *)(base + o_tr), nrec, nt, (const double *)(base + o_om), nf,

@@ -8,18 +8,23 @@
 // is one template specialised by a mask GM of the axes handled generally, so
 // the interior (GM = 0) is straight-line code, a face carries one axis's
 // CPML terms, and only edges and corners (GM = 7) pay for all of them.
-// Three launches per phase (interior, faces, general); blockIdx.x
-// enumerates tiles through a TileMap in global memory, blockIdx.y is the
-// shot.  Every body uses the same explicit fma forms, so a cell gets
+// Three launches per phase (interior, faces, general), each with its own
+// thread-tile shape; blockIdx.x enumerates tiles through a TileMap in global
+// memory, blockIdx.y is the shot.  The interior box is the exact interior
+// (x edges on multiples of 4 cells), so its last tile in x and y may be
+// partial.  Every body uses the same explicit fma forms, so a cell gets
 // bit-identical results whichever body computes it.
 //
 // Thread mapping: a BX x BY block covers one tile in (x, y); each thread owns
 // VX consecutive x cells (one aligned float2/float4/double2 per field and
-// plane) of KZ consecutive z planes.  x neighbours come from the aligned
-// vectors at i0-VX, i0, i0+VX; y and z neighbours are whole vectors.  All
-// loads of a thread are issued before its first store (every pointer is
-// __restrict__, fields read in a phase are never written in it), so a warp
-// keeps ~20 independent 8-16 byte loads in flight.
+// plane) and marches through the tile's ZC z planes, keeping the four planes
+// of the two fields it differentiates along z in a rolling register window,
+// so each plane costs one new load of each.  x neighbours come from the
+// aligned vectors at i0-VX, i0, i0+VX; y neighbours are whole vectors.  All
+// loads of a plane are issued before its first store (every pointer is
+// __restrict__, fields read in a phase are never written in it), and the
+// psi slabs are loaded with the fields, so a warp keeps ~17 independent
+// 8-16 byte loads in flight per plane.
 //
 // E half step (ncver0027/cpu_eh_field_cpml42.f90:114-158, cpu_cpml4.f90:271-361):
 //   Ex = ca_x Ex + s cb_x (Dy(Hz)/kedy - Dz(Hy)/kedz),  cyclic for Ey, Ez,
@@ -40,6 +45,7 @@ namespace mittet {
 // need general handling (0 interior, 1/2/4 faces, 7 general).
 struct TileMap {
     int nbox;
+    int zc;           // z planes per tile (each thread marches through them)
     int g0, g1;       // tiles [0, g0) interior, [g0, g1) faces, [g1, start[nbox]) general
     int start[25];    // first tile of each box
     int kind[24];
@@ -84,6 +90,28 @@ __device__ __forceinline__ void zerov(T (&d)[VX]) {
     for (int q = 0; q < VX; q++) d[q] = T(0);
 }
 
+// psi values o .. o+VX-1 of the lanes in mask: one vector access when every
+// lane is active, else one scalar access per active lane.
+template <typename T, int VX>
+__device__ __forceinline__ void ld_psi(T (&d)[VX], const T *__restrict__ p, int o, unsigned mask) {
+    if (mask == (1u << VX) - 1u) {
+        ldv_rw<T, VX>(d, p + o);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VX; v++) d[v] = (mask >> v & 1) ? p[o + v] : T(0);
+    }
+}
+template <typename T, int VX>
+__device__ __forceinline__ void st_psi(T *__restrict__ p, int o, const T (&s)[VX], unsigned mask) {
+    if (mask == (1u << VX) - 1u) {
+        stv<T, VX>(p + o, s);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VX; v++)
+            if (mask >> v & 1) p[o + v] = s[v];
+    }
+}
+
 template <int VX>
 __device__ __forceinline__ unsigned xmask(int i0, int lo, int hi) {
     unsigned m = 0;
@@ -106,11 +134,14 @@ __device__ __forceinline__ T leap(T ca, T sgcb, T x, T e) {  // ca e + (s cb) x
     return fma(sgcb, x, ca * e);
 }
 
-#define MITTET_MINB(T, VX, KZ, NT) ((sizeof(T) == 4 && VX == 2 && KZ == 1) ? 768 / (NT) : 512 / (NT))
+#define MITTET_MINB(T, VX, NT) ((sizeof(T) == 4 && VX == 2) ? 768 / (NT) : 512 / (NT))
+// Face and edge bodies carry psi and profile state: the wide ones get up to
+// 168 registers (3 x 128 threads per SM) instead of spilling.
+#define MITTET_MINB_GEN(T, VX, NT) ((sizeof(T) == 4 && VX == 2) ? 512 / (NT) : 384 / (NT))
 
 // ------------------------------------------------------------------ E phase
-template <typename T, int VX, int KZ, int GM>
-__device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int khi) {
+template <typename T, int VX, int GM>
+__device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
     const long long sb = (long long)shot * a.fshot;
     T *__restrict__ Ex = a.f[0] + sb;
     T *__restrict__ Ey = a.f[1] + sb;
@@ -169,10 +200,32 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
     const unsigned szm = GZ ? ((!GY || (j >= S2.other.lo[1] && j < S2.other.hi[1])) ? (GX ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : all) : 0u) : 0u;
     const int col = j * py + i0;
 
-    // z window: planes kb-2 .. kb+KZ of Hx and Hy
-    T wx[KZ + 3][VX], wy[KZ + 3][VX];
+    // psi recurrence coefficients of the x and y slabs (fixed along z) and
+    // this shot's psi slabs.
+    T be_x[VX], ced_x[VX];
+    int lx[VX];
+    T be_y = T(0), ced_y = T(0);
+    if constexpr (GX) {
+        ldv<T, VX>(be_x, P + 2 * ps + i0);
+        ldv<T, VX>(ced_x, P + 3 * ps + i0);
 #pragma unroll
-    for (int q = 0; q < KZ + 3; q++) {
+        for (int v = 0; v < VX; v++) lx[v] = slab_local(S0, i0 + v);
+    }
+    if constexpr (GY) {
+        be_y = __ldg(P + 10 * ps + j);
+        ced_y = __ldg(P + 11 * ps + j);
+    }
+    T *__restrict__ sx0 = a.psi[0][0] + shot * a.pshot[0];
+    T *__restrict__ sx1 = a.psi[0][1] + shot * a.pshot[0];
+    T *__restrict__ sy0 = a.psi[1][0] + shot * a.pshot[1];
+    T *__restrict__ sy1 = a.psi[1][1] + shot * a.pshot[1];
+    T *__restrict__ sz0 = a.psi[2][0] + shot * a.pshot[2];
+    T *__restrict__ sz1 = a.psi[2][1] + shot * a.pshot[2];
+
+    // rolling z window: wx/wy[0..3] = planes k-2 .. k+1 of Hx and Hy
+    T wx[4][VX], wy[4][VX];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
         const int kk = kb - 2 + q;
         if (!GZ || (kk >= 0 && kk < nz)) {
             ldv<T, VX>(wx[q], Hx + kk * pz + col);
@@ -184,17 +237,25 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
     }
     const int slot = a.ring_k > 0 ? (*a.d_step) % a.ring_k : 0;
 
-#pragma unroll
-    for (int q = 0; q < KZ; q++) {
-        const int k = kb + q;
-        if (GM != 0 && k >= khi) break;
+#pragma unroll 2
+    for (int k = kb; k < ke; k++) {
+        {
+            const int kk = k + 1;
+            if (!GZ || kk < nz) {
+                ldv<T, VX>(wx[3], Hx + kk * pz + col);
+                ldv<T, VX>(wy[3], Hy + kk * pz + col);
+            } else {
+                zerov<T, VX>(wx[3]);
+                zerov<T, VX>(wy[3]);
+            }
+        }
         const int c = k * pz + col;
         T hzx[3 * VX], hyx[3 * VX];
         {
             T t[VX];
             ldv<T, VX>(t, Hz + c);
 #pragma unroll
-            for (int v = 0; v < VX; v++) { hzx[VX + v] = t[v]; hyx[VX + v] = wy[q + 2][v]; }
+            for (int v = 0; v < VX; v++) { hzx[VX + v] = t[v]; hyx[VX + v] = wy[2][v]; }
             if (has_l) {
                 ldv<T, VX>(t, Hz + c - VX);
 #pragma unroll
@@ -255,15 +316,42 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         const bool s0k = !GZ || (k >= S0.other.lo[2] && k < S0.other.hi[2]);
         const bool s1k = !GZ || (k >= S1.other.lo[2] && k < S1.other.hi[2]);
 
+        // psi of the slabs this row crosses, loaded together with the fields
+        const unsigned mx = (GX && s0k) ? sxm : 0u;
+        const unsigned my = (GY && s1k) ? sym : 0u;
+        const unsigned mz = (GZ && lz >= 0) ? szm : 0u;
+        const int ox = (k * ny + j) * S0.width;
+        const int oy = (k * S1.width + ly) * py + i0;
+        const int oz = (lz * ny + j) * py + i0;
+        T qx0[VX], qx1[VX], qy0[VX], qy1[VX], qz0[VX], qz1[VX];
+        T be_z = T(0), ced_z = T(0);
+        if constexpr (GX) {
+#pragma unroll
+            for (int v = 0; v < VX; v++) {
+                qx0[v] = (mx >> v & 1) ? sx0[ox + lx[v]] : T(0);
+                qx1[v] = (mx >> v & 1) ? sx1[ox + lx[v]] : T(0);
+            }
+        }
+        if constexpr (GY) {
+            ld_psi<T, VX>(qy0, sy0, oy, my);
+            ld_psi<T, VX>(qy1, sy1, oy, my);
+        }
+        if constexpr (GZ) {
+            ld_psi<T, VX>(qz0, sz0, oz, mz);
+            ld_psi<T, VX>(qz1, sz1, oz, mz);
+            be_z = __ldg(P + 18 * ps + k);
+            ced_z = __ldg(P + 19 * ps + k);
+        }
+
 #pragma unroll
         for (int v = 0; v < VX; v++) {
             const bool vx = vxm >> v & 1;
             const T dyHz = vy ? d4(c1, c2, hzx[VX + v], hzm1[v], hzp1[v], hzm2[v]) : T(0);
-            const T dyHx = vy ? d4(c1, c2, wx[q + 2][v], hxm1[v], hxp1[v], hxm2[v]) : T(0);
+            const T dyHx = vy ? d4(c1, c2, wx[2][v], hxm1[v], hxp1[v], hxm2[v]) : T(0);
             const T dxHz = vx ? d4(c1, c2, hzx[VX + v], hzx[VX + v - 1], hzx[VX + v + 1], hzx[VX + v - 2]) : T(0);
             const T dxHy = vx ? d4(c1, c2, hyx[VX + v], hyx[VX + v - 1], hyx[VX + v + 1], hyx[VX + v - 2]) : T(0);
-            const T dzHy = vz ? d4(c1, c2, wy[q + 2][v], wy[q + 1][v], wy[q + 3][v], wy[q][v]) : T(0);
-            const T dzHx = vz ? d4(c1, c2, wx[q + 2][v], wx[q + 1][v], wx[q + 3][v], wx[q][v]) : T(0);
+            const T dzHy = vz ? d4(c1, c2, wy[2][v], wy[1][v], wy[3][v], wy[0][v]) : T(0);
+            const T dzHx = vz ? d4(c1, c2, wx[2][v], wx[1][v], wx[3][v], wx[0][v]) : T(0);
             const T mv = m[v];
             T ca_x = T(1), cb_x = mv, ca_y = T(1), cb_y = mv, ca_z = T(1), cb_z = mv;
             if (GX && esh_x[v] != T(0)) { const T h = esh_x[v] * mv; const T r = rcp(T(1) + h); ca_x = (T(1) - h) * r; cb_x = mv * r; }
@@ -273,44 +361,34 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
             if (ky && (uy >> v & 1)) ey[v] = leap(ca_y, sg * cb_y, curl2(dzHx, ik_z, dxHz, ik_x[v]), ey[v]);
             if (kz && (uz >> v & 1)) ez[v] = leap(ca_z, sg * cb_z, curl2(dxHy, ik_x[v], dyHx, ik_y), ez[v]);
 
-            {
-                if (GX && (sxm >> v & 1) && s0k) {
-                    T *__restrict__ q0 = a.psi[0][0] + shot * a.pshot[0];
-                    T *__restrict__ q1 = a.psi[0][1] + shot * a.pshot[0];
-                    const int o = (k * ny + j) * S0.width + slab_local(S0, i0 + v);
-                    const T be = __ldg(P + 2 * ps + i0 + v), ced = __ldg(P + 3 * ps + i0 + v);
-                    const T p0 = fma(be, q0[o], ced * dxHy);  // psi_Ezx
-                    const T p1 = fma(be, q1[o], ced * dxHz);  // psi_Eyx
-                    q0[o] = p0;
-                    q1[o] = p1;
-                    ez[v] = fma(cb_z, p0, ez[v]);
-                    ey[v] = fma(-cb_y, p1, ey[v]);
-                }
-                if (GY && (sym >> v & 1) && s1k) {
-                    T *__restrict__ q0 = a.psi[1][0] + shot * a.pshot[1];
-                    T *__restrict__ q1 = a.psi[1][1] + shot * a.pshot[1];
-                    const int o = (k * S1.width + ly) * py + i0 + v;
-                    const T be = __ldg(P + 10 * ps + j), ced = __ldg(P + 11 * ps + j);
-                    const T p0 = fma(be, q0[o], ced * dyHz);  // psi_Exy
-                    const T p1 = fma(be, q1[o], ced * dyHx);  // psi_Ezy
-                    q0[o] = p0;
-                    q1[o] = p1;
-                    ex[v] = fma(cb_x, p0, ex[v]);
-                    ez[v] = fma(-cb_z, p1, ez[v]);
-                }
-                if (GZ && (szm >> v & 1) && lz >= 0) {
-                    T *__restrict__ q0 = a.psi[2][0] + shot * a.pshot[2];
-                    T *__restrict__ q1 = a.psi[2][1] + shot * a.pshot[2];
-                    const int o = (lz * ny + j) * py + i0 + v;
-                    const T be = __ldg(P + 18 * ps + k), ced = __ldg(P + 19 * ps + k);
-                    const T p0 = fma(be, q0[o], ced * dzHx);  // psi_Eyz
-                    const T p1 = fma(be, q1[o], ced * dzHy);  // psi_Exz
-                    q0[o] = p0;
-                    q1[o] = p1;
-                    ey[v] = fma(cb_y, p0, ey[v]);
-                    ex[v] = fma(-cb_x, p1, ex[v]);
-                }
+            if (GX && (mx >> v & 1)) {
+                const T p0 = fma(be_x[v], qx0[v], ced_x[v] * dxHy);  // psi_Ezx
+                const T p1 = fma(be_x[v], qx1[v], ced_x[v] * dxHz);  // psi_Eyx
+                sx0[ox + lx[v]] = p0;
+                sx1[ox + lx[v]] = p1;
+                ez[v] = fma(cb_z, p0, ez[v]);
+                ey[v] = fma(-cb_y, p1, ey[v]);
             }
+            if (GY && (my >> v & 1)) {
+                qy0[v] = fma(be_y, qy0[v], ced_y * dyHz);  // psi_Exy
+                qy1[v] = fma(be_y, qy1[v], ced_y * dyHx);  // psi_Ezy
+                ex[v] = fma(cb_x, qy0[v], ex[v]);
+                ez[v] = fma(-cb_z, qy1[v], ez[v]);
+            }
+            if (GZ && (mz >> v & 1)) {
+                qz0[v] = fma(be_z, qz0[v], ced_z * dzHx);  // psi_Eyz
+                qz1[v] = fma(be_z, qz1[v], ced_z * dzHy);  // psi_Exz
+                ey[v] = fma(cb_y, qz0[v], ey[v]);
+                ex[v] = fma(-cb_x, qz1[v], ex[v]);
+            }
+        }
+        if constexpr (GY) {
+            st_psi<T, VX>(sy0, oy, qy0, my);
+            st_psi<T, VX>(sy1, oy, qy1, my);
+        }
+        if constexpr (GZ) {
+            st_psi<T, VX>(sz0, oz, qz0, mz);
+            st_psi<T, VX>(sz1, oz, qz1, mz);
         }
         stv<T, VX>(Ex + c, ex);
         stv<T, VX>(Ey + c, ey);
@@ -321,12 +399,17 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
             if (a.vmask & 2) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
             if (a.vmask & 4) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
         }
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            wx[0][v] = wx[1][v]; wx[1][v] = wx[2][v]; wx[2][v] = wx[3][v];
+            wy[0][v] = wy[1][v]; wy[1][v] = wy[2][v]; wy[2][v] = wy[3][v];
+        }
     }
 }
 
 // ------------------------------------------------------------------ H phase
-template <typename T, int VX, int KZ, int GM>
-__device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int khi) {
+template <typename T, int VX, int GM>
+__device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
     const long long sb = (long long)shot * a.fshot;
     const T *__restrict__ Ex = a.f[0] + sb;
     const T *__restrict__ Ey = a.f[1] + sb;
@@ -386,10 +469,32 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
     const unsigned szm = GZ ? ((!GY || (j >= S2.other.lo[1] && j < S2.other.hi[1])) ? (GX ? xmask<VX>(i0, S2.other.lo[0], S2.other.hi[0]) : all) : 0u) : 0u;
     const int col = j * py + i0;
 
-    // z window: planes kb-1 .. kb+KZ+1 of Ex and Ey
-    T wx[KZ + 3][VX], wy[KZ + 3][VX];
+    // psi recurrence coefficients of the x and y slabs (fixed along z) and
+    // this shot's psi slabs.
+    T bh_x[VX], chd_x[VX];
+    int lx[VX];
+    T bh_y = T(0), chd_y = T(0);
+    if constexpr (GX) {
+        ldv<T, VX>(bh_x, P + 4 * ps + i0);
+        ldv<T, VX>(chd_x, P + 5 * ps + i0);
 #pragma unroll
-    for (int q = 0; q < KZ + 3; q++) {
+        for (int v = 0; v < VX; v++) lx[v] = slab_local(S0, i0 + v);
+    }
+    if constexpr (GY) {
+        bh_y = __ldg(P + 12 * ps + j);
+        chd_y = __ldg(P + 13 * ps + j);
+    }
+    T *__restrict__ sx0 = a.psi[0][0] + shot * a.pshot[0];
+    T *__restrict__ sx1 = a.psi[0][1] + shot * a.pshot[0];
+    T *__restrict__ sy0 = a.psi[1][0] + shot * a.pshot[1];
+    T *__restrict__ sy1 = a.psi[1][1] + shot * a.pshot[1];
+    T *__restrict__ sz0 = a.psi[2][0] + shot * a.pshot[2];
+    T *__restrict__ sz1 = a.psi[2][1] + shot * a.pshot[2];
+
+    // rolling z window: wx/wy[0..3] = planes k-1 .. k+2 of Ex and Ey
+    T wx[4][VX], wy[4][VX];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
         const int kk = kb - 1 + q;
         if (!GZ || (kk >= 0 && kk < nz)) {
             ldv<T, VX>(wx[q], Ex + kk * pz + col);
@@ -400,17 +505,25 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         }
     }
 
-#pragma unroll
-    for (int q = 0; q < KZ; q++) {
-        const int k = kb + q;
-        if (GM != 0 && k >= khi) break;
+#pragma unroll 2
+    for (int k = kb; k < ke; k++) {
+        {
+            const int kk = k + 2;
+            if (!GZ || kk < nz) {
+                ldv<T, VX>(wx[3], Ex + kk * pz + col);
+                ldv<T, VX>(wy[3], Ey + kk * pz + col);
+            } else {
+                zerov<T, VX>(wx[3]);
+                zerov<T, VX>(wy[3]);
+            }
+        }
         const int c = k * pz + col;
         T ezx[3 * VX], eyx[3 * VX];
         {
             T t[VX];
             ldv<T, VX>(t, Ez + c);
 #pragma unroll
-            for (int v = 0; v < VX; v++) { ezx[VX + v] = t[v]; eyx[VX + v] = wy[q + 1][v]; }
+            for (int v = 0; v < VX; v++) { ezx[VX + v] = t[v]; eyx[VX + v] = wy[1][v]; }
             if (has_l) {
                 ldv<T, VX>(t, Ez + c - VX);
 #pragma unroll
@@ -477,16 +590,43 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         const bool s0k = !GZ || (k >= S0.other.lo[2] && k < S0.other.hi[2]);
         const bool s1k = !GZ || (k >= S1.other.lo[2] && k < S1.other.hi[2]);
 
+        // psi of the slabs this row crosses, loaded together with the fields
+        const unsigned mx = (GX && s0k) ? sxm : 0u;
+        const unsigned my = (GY && s1k) ? sym : 0u;
+        const unsigned mz = (GZ && lz >= 0) ? szm : 0u;
+        const int ox = (k * ny + j) * S0.width;
+        const int oy = (k * S1.width + ly) * py + i0;
+        const int oz = (lz * ny + j) * py + i0;
+        T qx0[VX], qx1[VX], qy0[VX], qy1[VX], qz0[VX], qz1[VX];
+        T bh_z = T(0), chd_z = T(0);
+        if constexpr (GX) {
+#pragma unroll
+            for (int v = 0; v < VX; v++) {
+                qx0[v] = (mx >> v & 1) ? sx0[ox + lx[v]] : T(0);
+                qx1[v] = (mx >> v & 1) ? sx1[ox + lx[v]] : T(0);
+            }
+        }
+        if constexpr (GY) {
+            ld_psi<T, VX>(qy0, sy0, oy, my);
+            ld_psi<T, VX>(qy1, sy1, oy, my);
+        }
+        if constexpr (GZ) {
+            ld_psi<T, VX>(qz0, sz0, oz, mz);
+            ld_psi<T, VX>(qz1, sz1, oz, mz);
+            bh_z = __ldg(P + 20 * ps + k);
+            chd_z = __ldg(P + 21 * ps + k);
+        }
+
 #pragma unroll
         for (int v = 0; v < VX; v++) {
             const bool vx = vxm >> v & 1;
             const T ez = ezx[VX + v];
             const T dyEz = vy ? d4(c1, c2, ezp1[v], ez, ezp2[v], ezm1[v]) : T(0);
-            const T dyEx = vy ? d4(c1, c2, exp1[v], wx[q + 1][v], exp2[v], exm1[v]) : T(0);
+            const T dyEx = vy ? d4(c1, c2, exp1[v], wx[1][v], exp2[v], exm1[v]) : T(0);
             const T dxEz = vx ? d4(c1, c2, ezx[VX + v + 1], ez, ezx[VX + v + 2], ezx[VX + v - 1]) : T(0);
             const T dxEy = vx ? d4(c1, c2, eyx[VX + v + 1], eyx[VX + v], eyx[VX + v + 2], eyx[VX + v - 1]) : T(0);
-            const T dzEy = vz ? d4(c1, c2, wy[q + 2][v], wy[q + 1][v], wy[q + 3][v], wy[q][v]) : T(0);
-            const T dzEx = vz ? d4(c1, c2, wx[q + 2][v], wx[q + 1][v], wx[q + 3][v], wx[q][v]) : T(0);
+            const T dzEy = vz ? d4(c1, c2, wy[2][v], wy[1][v], wy[3][v], wy[0][v]) : T(0);
+            const T dzEx = vz ? d4(c1, c2, wx[2][v], wx[1][v], wx[3][v], wx[0][v]) : T(0);
             const T mv = m[v], dmv = dm[v];
             T da_x = T(1), db_x = dmv, da_y = T(1), db_y = dmv, da_z = T(1), db_z = dmv;
             if (GX && msh_x[v] != T(0)) { const T h = msh_x[v] * mv; const T r = rcp(T(1) + h); da_x = (T(1) - h) * r; db_x = dmv * r; }
@@ -496,118 +636,131 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
             if (ky && (uy >> v & 1)) hy[v] = leap(da_y, -sg * db_y, curl2(dzEx, ik_z, dxEz, ik_x[v]), hy[v]);
             if (kz && (uz >> v & 1)) hz[v] = leap(da_z, -sg * db_z, curl2(dxEy, ik_x[v], dyEx, ik_y), hz[v]);
 
-            {
-                if (GX && (sxm >> v & 1) && s0k) {
-                    T *__restrict__ q0 = a.psi[0][0] + shot * a.pshot[0];
-                    T *__restrict__ q1 = a.psi[0][1] + shot * a.pshot[0];
-                    const int o = (k * ny + j) * S0.width + slab_local(S0, i0 + v);
-                    const T bh = __ldg(P + 4 * ps + i0 + v), chd = __ldg(P + 5 * ps + i0 + v);
-                    // psi_Hyx stencil (cpu_cpml4.f90:400): c1 Ez(i+1) - c2t Ez(i) + c2 Ez(i+2) - c2 Ez(i-1)
-                    const T dxEzt = vx ? fma(c1, ezx[VX + v + 1], -(c2t * ez)) + c2 * (ezx[VX + v + 2] - ezx[VX + v - 1]) : T(0);
-                    const T p0 = fma(bh, q0[o], chd * dxEy);   // psi_Hzx
-                    const T p1 = fma(bh, q1[o], chd * dxEzt);  // psi_Hyx
-                    q0[o] = p0;
-                    q1[o] = p1;
-                    hz[v] = fma(-db_z, p0, hz[v]);
-                    hy[v] = fma(db_y, p1, hy[v]);
-                }
-                if (GY && (sym >> v & 1) && s1k) {
-                    T *__restrict__ q0 = a.psi[1][0] + shot * a.pshot[1];
-                    T *__restrict__ q1 = a.psi[1][1] + shot * a.pshot[1];
-                    const int o = (k * S1.width + ly) * py + i0 + v;
-                    const T bh = __ldg(P + 12 * ps + j), chd = __ldg(P + 13 * ps + j);
-                    const T p0 = fma(bh, q0[o], chd * dyEz);  // psi_Hxy
-                    const T p1 = fma(bh, q1[o], chd * dyEx);  // psi_Hzy
-                    q0[o] = p0;
-                    q1[o] = p1;
-                    hx[v] = fma(-db_x, p0, hx[v]);
-                    hz[v] = fma(db_z, p1, hz[v]);
-                }
-                if (GZ && (szm >> v & 1) && lz >= 0) {
-                    T *__restrict__ q0 = a.psi[2][0] + shot * a.pshot[2];
-                    T *__restrict__ q1 = a.psi[2][1] + shot * a.pshot[2];
-                    const int o = (lz * ny + j) * py + i0 + v;
-                    const T bh = __ldg(P + 20 * ps + k), chd = __ldg(P + 21 * ps + k);
-                    const T p0 = fma(bh, q0[o], chd * dzEx);  // psi_Hyz
-                    const T p1 = fma(bh, q1[o], chd * dzEy);  // psi_Hxz
-                    q0[o] = p0;
-                    q1[o] = p1;
-                    hy[v] = fma(-db_y, p0, hy[v]);
-                    hx[v] = fma(db_x, p1, hx[v]);
-                }
+            if (GX && (mx >> v & 1)) {
+                // psi_Hyx stencil (cpu_cpml4.f90:400): c1 Ez(i+1) - c2t Ez(i) + c2 Ez(i+2) - c2 Ez(i-1)
+                const T dxEzt = vx ? fma(c1, ezx[VX + v + 1], -(c2t * ez)) + c2 * (ezx[VX + v + 2] - ezx[VX + v - 1]) : T(0);
+                const T p0 = fma(bh_x[v], qx0[v], chd_x[v] * dxEy);   // psi_Hzx
+                const T p1 = fma(bh_x[v], qx1[v], chd_x[v] * dxEzt);  // psi_Hyx
+                sx0[ox + lx[v]] = p0;
+                sx1[ox + lx[v]] = p1;
+                hz[v] = fma(-db_z, p0, hz[v]);
+                hy[v] = fma(db_y, p1, hy[v]);
             }
+            if (GY && (my >> v & 1)) {
+                qy0[v] = fma(bh_y, qy0[v], chd_y * dyEz);  // psi_Hxy
+                qy1[v] = fma(bh_y, qy1[v], chd_y * dyEx);  // psi_Hzy
+                hx[v] = fma(-db_x, qy0[v], hx[v]);
+                hz[v] = fma(db_z, qy1[v], hz[v]);
+            }
+            if (GZ && (mz >> v & 1)) {
+                qz0[v] = fma(bh_z, qz0[v], chd_z * dzEx);  // psi_Hyz
+                qz1[v] = fma(bh_z, qz1[v], chd_z * dzEy);  // psi_Hxz
+                hy[v] = fma(-db_y, qz0[v], hy[v]);
+                hx[v] = fma(db_x, qz1[v], hx[v]);
+            }
+        }
+        if constexpr (GY) {
+            st_psi<T, VX>(sy0, oy, qy0, my);
+            st_psi<T, VX>(sy1, oy, qy1, my);
+        }
+        if constexpr (GZ) {
+            st_psi<T, VX>(sz0, oz, qz0, mz);
+            st_psi<T, VX>(sz1, oz, qz1, mz);
         }
         stv<T, VX>(Hx + c, hx);
         stv<T, VX>(Hy + c, hy);
         stv<T, VX>(Hz + c, hz);
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            wx[0][v] = wx[1][v]; wx[1][v] = wx[2][v]; wx[2][v] = wx[3][v];
+            wy[0][v] = wy[1][v]; wy[1][v] = wy[2][v]; wy[2][v] = wy[3][v];
+        }
     }
 }
 
-// Locate this CTA's box and tile (tile index b over all boxes).
-template <int VX, int BX, int BY, int KZ>
-__device__ __forceinline__ int locate(const TileMap *__restrict__ tm, int b, int &i0, int &j, int &kb, int &khi,
-                                      bool &inside) {
+// Locate this CTA's box and tile (tile index b over boxes [q0, nbox)): the
+// thread's first x cell i0, its row j and its z planes [kb, ke).
+template <int VX, int BX, int BY>
+__device__ __forceinline__ int locate(const TileMap *__restrict__ tm, int q0, int b, int &i0, int &j, int &kb,
+                                      int &ke, bool &inside) {
     const int nbox = __ldg(&tm->nbox);
-    int q = 0;
-    for (int t = 1; t < nbox; t++)
+    int q = q0;
+    for (int t = q0 + 1; t < nbox; t++)
         if (b >= __ldg(&tm->start[t])) q = t;
     const int local = b - __ldg(&tm->start[q]);
-    const int ntx = __ldg(&tm->ntx[q]), nty = __ldg(&tm->nty[q]);
+    const int ntx = __ldg(&tm->ntx[q]), nty = __ldg(&tm->nty[q]), zc = __ldg(&tm->zc);
     const int tx = local % ntx, r = local / ntx;
     const int ty = r % nty, tz = r / nty;
     i0 = __ldg(&tm->lo[q][0]) + (tx * BX + (int)threadIdx.x) * VX;
     j = __ldg(&tm->lo[q][1]) + ty * BY + (int)threadIdx.y;
-    kb = __ldg(&tm->lo[q][2]) + tz * KZ;
-    khi = __ldg(&tm->hi[q][2]);
+    kb = __ldg(&tm->lo[q][2]) + tz * zc;
+    ke = min(kb + zc, __ldg(&tm->hi[q][2]));
     inside = i0 < __ldg(&tm->hi[q][0]) && j < __ldg(&tm->hi[q][1]);
     return __ldg(&tm->kind[q]);
 }
 
 #define MITTET_PHASE_KERNELS(PH)                                                                             \
-    template <typename T, int VX, int BX, int BY, int KZ>                                                    \
-    __global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, KZ, BX *BY))                                \
+    template <typename T, int VX, int BX, int BY>                                                            \
+    __global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, BX *BY))                                    \
         PH##_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {                         \
-        int i0, j, kb, khi;                                                                                  \
+        int i0, j, kb, ke;                                                                                   \
         bool inside;                                                                                         \
-        locate<VX, BX, BY, KZ>(tm, blockIdx.x, i0, j, kb, khi, inside);                                     \
-        PH##_cells<T, VX, KZ, 0>(a, blockIdx.y, i0, j, kb, kb + KZ);                                         \
+        locate<VX, BX, BY>(tm, 0, blockIdx.x, i0, j, kb, ke, inside);                                        \
+        if (inside) PH##_cells<T, VX, 0>(a, blockIdx.y, i0, j, kb, ke);                                      \
     }                                                                                                        \
-    template <typename T, int VX, int BX, int BY, int KZ>                                                    \
-    __global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))                                               \
+    template <typename T, int VX, int BX, int BY>                                                            \
+    __global__ void __launch_bounds__(BX *BY, MITTET_MINB_GEN(T, VX, BX *BY))                                \
         PH##_face_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {            \
-        int i0, j, kb, khi;                                                                                  \
+        int i0, j, kb, ke;                                                                                   \
         bool inside;                                                                                         \
-        const int kind = locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);       \
+        const int kind = locate<VX, BX, BY>(tm, 1, first_tile + blockIdx.x, i0, j, kb, ke, inside);          \
         if (!inside) return;                                                                                 \
-        if (kind == 1) PH##_cells<T, VX, KZ, 1>(a, blockIdx.y, i0, j, kb, khi);                             \
-        else if (kind == 2) PH##_cells<T, VX, KZ, 2>(a, blockIdx.y, i0, j, kb, khi);                        \
-        else PH##_cells<T, VX, KZ, 4>(a, blockIdx.y, i0, j, kb, khi);                                        \
+        if (kind == 1) PH##_cells<T, VX, 1>(a, blockIdx.y, i0, j, kb, ke);                                   \
+        else if (kind == 2) PH##_cells<T, VX, 2>(a, blockIdx.y, i0, j, kb, ke);                              \
+        else PH##_cells<T, VX, 4>(a, blockIdx.y, i0, j, kb, ke);                                             \
     }                                                                                                        \
-    template <typename T, int VX, int BX, int BY, int KZ>                                                    \
-    __global__ void __launch_bounds__(BX *BY, 512 / (BX * BY))                                               \
+    template <typename T, int VX, int BX, int BY>                                                            \
+    __global__ void __launch_bounds__(BX *BY, MITTET_MINB_GEN(T, VX, BX *BY))                                \
         PH##_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {           \
-        int i0, j, kb, khi;                                                                                  \
+        int i0, j, kb, ke;                                                                                   \
         bool inside;                                                                                         \
-        locate<VX, BX, BY, KZ>(tm, first_tile + blockIdx.x, i0, j, kb, khi, inside);                        \
-        if (inside) PH##_cells<T, VX, KZ, 7>(a, blockIdx.y, i0, j, kb, khi);                                 \
+        locate<VX, BX, BY>(tm, 0, first_tile + blockIdx.x, i0, j, kb, ke, inside);                           \
+        if (inside) PH##_cells<T, VX, 7>(a, blockIdx.y, i0, j, kb, ke);                                      \
     }
 
 // e_interior_kernel / e_face_kernel / e_shell_kernel and the h_ ones.
 MITTET_PHASE_KERNELS(e)
 MITTET_PHASE_KERNELS(h)
 
-// Variants the autotuner chooses from: (VX, BX, BY, KZ).
+// Variants the autotuner chooses from: (VX, BX, BY, ZC) = x cells per
+// thread, thread block, z planes each thread marches through.  ZC is a
+// run-time tile parameter (the same kernel serves every ZC): short chunks give
+// small boxes enough CTAs, long ones amortise the window preload.  The
+// narrow blocks (x tile of 8 or 16 cells) suit the thin x faces.
 #define MITTET_STENCIL_VARIANTS_F32(X) \
-    X(2, 32, 4, 1)                     \
-    X(2, 16, 8, 1)                     \
-    X(4, 16, 8, 1)                     \
-    X(4, 8, 16, 1)                     \
     X(2, 32, 4, 2)                     \
-    X(4, 16, 4, 2)
+    X(2, 32, 4, 4)                     \
+    X(2, 32, 4, 8)                     \
+    X(2, 32, 4, 16)                    \
+    X(2, 16, 8, 2)                     \
+    X(2, 16, 8, 4)                     \
+    X(2, 16, 8, 8)                     \
+    X(4, 16, 8, 2)                     \
+    X(4, 16, 8, 4)                     \
+    X(4, 16, 8, 8)                     \
+    X(4, 8, 16, 4)                     \
+    X(4, 16, 4, 4)                     \
+    X(2, 8, 16, 4)                     \
+    X(2, 8, 16, 8)                     \
+    X(2, 4, 32, 4)
 #define MITTET_STENCIL_VARIANTS_F64(X) \
-    X(2, 32, 4, 1)                     \
-    X(2, 16, 8, 1)                     \
     X(2, 32, 4, 2)                     \
-    X(2, 16, 4, 2)
+    X(2, 32, 4, 4)                     \
+    X(2, 32, 4, 8)                     \
+    X(2, 16, 8, 2)                     \
+    X(2, 16, 8, 4)                     \
+    X(2, 16, 8, 8)                     \
+    X(2, 16, 4, 4)                     \
+    X(2, 8, 16, 4)
 
 }  // namespace mittet

@@ -242,10 +242,12 @@ class MittetSolver:
         return dict(zip(["inject_magnetic", "e_phase", "inject_electric", "h_phase", "sample", "volume_dft"], ms.tolist()))
 
     def tuned_variant(self) -> dict:
-        e = (ctypes.c_int32 * 4)()
-        h = (ctypes.c_int32 * 4)()
-        check(self._lib.mittet_tuned_variant(self._h, e, h))
-        return {"e_phase": list(e), "h_phase": list(h)}
+        """[VX, BX, BY, ZC] the autotuner chose per phase and launch."""
+        c = (ctypes.c_int32 * 24)()
+        check(self._lib.mittet_tuned_variants(self._h, c))
+        v = list(c)
+        return {f"{ph}_{part}": v[(i * 3 + p) * 4:(i * 3 + p + 1) * 4]
+                for i, ph in enumerate(("e", "h")) for p, part in enumerate(("interior", "faces", "edges"))}
 
     def launch_count(self) -> int:
         return int(self._lib.mittet_last_launch_count(self._h))

@@ -209,3 +209,34 @@ def test_single_step():
     with W.make_solver(wl) as s:
         _, td = s.forward(1, want_traces=True)
     assert np.allclose(td[0], ref, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("prec", [FP32, FP64])
+@pytest.mark.parametrize("flavor", [FLAVOR_NCVER0027, FLAVOR_SATAN_I])
+def test_tma_interior_is_bit_identical_to_plain_loads(monkeypatch, prec, flavor):
+    """The TMA-staged interior kernel and the plain-load interior body use the
+    same fma forms, so fields, traces and volume spectra agree bit for bit.
+    The grid gives the interior partial tiles in x and y, several z chunks
+    and two shots."""
+    wl = W.small_case(n=(150, 44, 40), ncpml=8, nt=70, precision=prec, flavor=flavor, magnetic=True)
+    nx, ny, nz = wl.cp.nx, wl.cp.ny, wl.cp.nz
+    second = Shot(points=[(nx // 3, ny // 2 + 3, nz // 2 - 4, "ey", SRC_ELECTRIC, 0.7)])
+    wl = replace(wl, volume_dft="xyz", shots=[wl.shots[0], second])
+    out = {}
+    for mode in ("ldg", "tma"):
+        monkeypatch.setenv("MITTET_INTERIOR", mode)
+        with W.make_solver(wl) as s:
+            spec, td = s.forward(wl.nt, want_traces=True)
+            var = s.tuned_variant()
+            vols = [s.volume_dft(k, c) for k in (0, 1) for c in ("ex", "ey", "ez")]
+            fields = [s.fields(k) for k in (0, 1)]
+        out[mode] = (spec, td, vols, fields, var)
+    assert out["tma"][4]["e_interior"][0] == 0 and out["tma"][4]["h_interior"][0] == 0, out["tma"][4]
+    assert out["ldg"][4]["e_interior"][0] != 0 and out["ldg"][4]["h_interior"][0] != 0, out["ldg"][4]
+    a, b = out["ldg"], out["tma"]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for va, vb in zip(a[2], b[2]):
+        assert np.array_equal(va, vb)
+    for fa, fb in zip(a[3], b[3]):
+        for c in range(6):
+            assert np.array_equal(fa[c], fb[c]), NAMES[c]
