@@ -107,6 +107,20 @@ def stencil_bytes(wl, esz):
     return b * len(wl.shots)
 
 
+def e_phase_traffic(wl, esz):
+    """DRAM bytes of one E-phase launch set, from the committed ncu capture of
+    the same kernels (bytes per cell of the 256x256x96 twin, scaled by the
+    cells of this launch).  Only FP32 fields with the 3-component volume DFT
+    were captured; other configurations return None."""
+    import re
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        "plain_gpu_256x256x192_launches_and_dram.md")
+    if esz != 4 or wl.volume_dft != "xyz" or not os.path.exists(path):
+        return None
+    m = re.search(r"e_phase_dram_bytes_per_cell:\s*([0-9.]+)", open(path).read())
+    return float(m.group(1)) * wl.ncell * len(wl.shots) if m else None
+
+
 def run_cpu_baseline(wl, budget_s=20.0):
     """Oracle (FP64 CPU restatement, all host threads) on a bounded sample of the
     workload: a few time steps of the same grid.  Returns (Gcell/s, sample text, threads)."""
@@ -304,7 +318,7 @@ def main():
             "kernel_ms": kt,
             "stencil_variant": solver.tuned_variant(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "e_phase_kernel",
+                         "frac": achieved / peak, "traffic": e_phase_traffic(wl, esz), "kernel": "E phase (e_part_kernel x5 / interior_tma_kernel)",
                          "alg_bytes_per_launch": ebytes, "peak_source": peak_kind},
             "clocks": clocks,
             "e2e": e2e,

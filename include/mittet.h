@@ -184,6 +184,26 @@ int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double 
 int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t checkpoint_every,
                     double *misfit, double *grad);
 
+/* One satan_i model update after a gradient (fwi3d_cpu_inv_fwi_v1.4.c:85-107):
+ *   calc_phi (fwi3d_cpu_function_v1.4.c:2565-2603): scaler = 0.01f * max sigma /
+ *     max grad over the cells with 0-based k <= iseabed (both maxima start at
+ *     cell 0); trial model sigma2 = sigma - scaler * grad everywhere;
+ *   one forward of every shot on sigma2 (receivers and frequencies of the
+ *     handle, volume DFT off);
+ *   calc_alpha (:2757-2785): k1 = sum dE (E2 - Ecal), k2 = sum (E2 - Ecal)^2
+ *     (complex products, no conjugate) over shots, receivers and frequencies,
+ *     dE = obs - Ecal;
+ *   update_para2 (:2787-2832): alpha = 3 |k1| / |k2|; inside [ncpml, n-ncpml)
+ *     sigma += alpha * scaler * grad where k <= iseabed, then every inside
+ *     cell is clamped to [minval, maxval].
+ * obs, ecal: [nshot][nrec][nf] complex (ecal = the current model's rec_fd);
+ * grad: mittet_gradient's output; sigma: in/out [nz][ny][nx] (x fastest).
+ * step[0] = scaler, step[1] = alpha.  The handle's model is left at the new
+ * sigma.  A trial model with a non-positive conductivity, a zero largest
+ * gradient or k2 = 0 is rejected with MITTET_ERR_INVALID_ARG. */
+int mittet_fwi_update(mittet_handle *h, int32_t nt, const double *obs, const double *ecal, const double *grad,
+                      int32_t iseabed, double minval, double maxval, double *sigma, double *step);
+
 /* Device-resident variants for callers that keep data on the GPU (the
  * PyTorch front end).  Pointers are device pointers of the handle's device;
  * stream is the caller's cudaStream_t (NULL = the legacy default stream): the
@@ -204,9 +224,9 @@ int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms);
  * thread block in x and y, z planes each thread marches through. */
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
 
-/* All chosen variants: cfg[24] = [phase E, H][launch interior, faces,
- * edges][VX, BX, BY, ZC].  VX = 0 marks the TMA-staged interior kernel, whose
- * BX x BY is then its tile in cells. */
+/* All chosen variants: cfg[40] = [phase E, H][launch interior, x faces,
+ * y faces, z faces, edges][VX, BX, BY, ZC].  VX = 0 marks the TMA-staged
+ * interior kernel, whose BX x BY is then its tile in cells. */
 int mittet_tuned_variants(mittet_handle *h, int32_t *cfg);
 
 /* Number of kernels the last forward launched (for launch accounting). */

@@ -1,11 +1,15 @@
 // kernels.cuh -- sm_100a kernels of the Mittet fictitious-wave FDTD step.
 //
-// One time step of one batch of shots is four launches on one stream:
+// One time step of one batch of shots runs on one stream:
 //   inject_kernel (magnetic points, before E)   ncver0027/cpu_waveform.f90:46-50
-//   e_phase_kernel  E update + CPML psi_E        cpu_eh_field_cpml42.f90:114-158, cpu_cpml4.f90:271-361
+//   E phase: e_part_kernel x 5 (interior, x/y/z faces, edges) or
+//            interior_tma_kernel for the interior
+//                   E update + CPML psi_E        cpu_eh_field_cpml42.f90:114-158, cpu_cpml4.f90:271-361
 //   inject_kernel (electric points, after E)    satan_i/fwi3d_cpu_function_v1.4.c:526-527
-//   h_phase_kernel  H update + CPML psi_H        cpu_eh_field_cpml42.f90:210-253, cpu_cpml4.f90:384-474
+//   H phase: h_part_kernel x 5 / interior_tma_kernel
+//                   H update + CPML psi_H        cpu_eh_field_cpml42.f90:210-253, cpu_cpml4.f90:384-474
 //   sample_kernel   receiver gather + step++     cpu_output.f90:20-30
+// and every 32 steps volume_dft_kernel folds the E ring into the spectra.
 // The step index lives in device memory (d_step) so a block of steps can be
 // captured once in a CUDA graph and replayed.
 //
@@ -15,7 +19,7 @@
 // plus dt/mu per cell only when a permeability volume is given.  CPML psi
 // variables exist only inside their slabs (compact [shot][...] boxes).
 //
-// The two half-step kernels are in stencil.cuh.
+// The half-step kernels are in stencil.cuh and tma_interior.cuh.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>

@@ -107,6 +107,10 @@ struct mittet_handle_s {
     bool fp64 = false;
     size_t esz = 4;
     cudaStream_t st = nullptr;
+    // side streams and events of the concurrent phase parts (fork/join,
+    // captured as parallel branches of the step graph)
+    cudaStream_t pst[kParts] = {nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[kParts] = {nullptr};
 
     DevBuf prof, m, dtmu;
     bool has_model = false, has_mu = false;
@@ -132,8 +136,8 @@ struct mittet_handle_s {
 
     uint32_t vmask = 0;
     int ring_k = kFlushRing;  // ring depth = steps per graph and per volume-DFT flush
-    int var_e[3] = {0, 0, 0};  // stencil variant (index into variants<T>()) of the
-    int var_h[3] = {0, 0, 0};  // interior, face and edge launches of each phase;
+    int var_e[kParts] = {0};   // stencil variant (index into variants<T>()) of the interior,
+    int var_h[kParts] = {0};   // x/y/z face and edge launches of each phase;
                                // var[0] = -1 - c selects TMA interior config c
     TmaMaps tma_maps[2];       // tensor maps of the E and H interior (current buffers)
     int tma_nown[2] = {0, 0};
@@ -142,9 +146,8 @@ struct mittet_handle_s {
     bool has_ibox[2] = {false, false};
     int ldg_int[2] = {0, 0};   // best plain-load interior variant of each phase
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
-    int tiles[64] = {0};       // tiles per (variant, phase)
-    int tiles_int[64] = {0};   // tiles [0, tiles_int) interior
-    int tiles_face[64] = {0};  // tiles [tiles_int, tiles_face) faces
+    std::vector<TileMap> tmaps_host;
+    int ptile[64][kParts + 1] = {{0}};  // per (variant, phase): part p is tiles [ptile[p], ptile[p+1])
     bool tuned = false;
     DevBuf ring, acc;
     std::vector<double> wt_host;  // volume-DFT weights [n][f] (re, im)
@@ -244,17 +247,18 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
 }
 
 // Stencil variants (VX x cells per thread, BX x BY threads, ZC z planes per thread)
-// the autotuner picks from.
+// the autotuner picks from; k[phase][part] are the kernels of the five bodies.
+template <typename T>
+using PartKernel = void (*)(PhaseArgs<T>, const TileMap *, int, int, int);
 template <typename T>
 struct Variant {
     int vx, bx, by, zc;
-    void (*ei)(PhaseArgs<T>, const TileMap *);
-    void (*hi)(PhaseArgs<T>, const TileMap *);
-    void (*ef)(PhaseArgs<T>, const TileMap *, int);
-    void (*hf)(PhaseArgs<T>, const TileMap *, int);
-    void (*es)(PhaseArgs<T>, const TileMap *, int);
-    void (*hs)(PhaseArgs<T>, const TileMap *, int);
+    PartKernel<T> k[2][kParts];
 };
+
+#define MITTET_PARTS(PH, T, vx, bx, by)                                                                      \
+    {PH##_part_kernel<T, vx, bx, by, 0>, PH##_part_kernel<T, vx, bx, by, 1>, PH##_part_kernel<T, vx, bx, by, 2>, \
+     PH##_part_kernel<T, vx, bx, by, 4>, PH##_part_kernel<T, vx, bx, by, 7>}
 
 template <typename T>
 const std::vector<Variant<T>> &variants();
@@ -262,10 +266,8 @@ const std::vector<Variant<T>> &variants();
 template <>
 const std::vector<Variant<float>> &variants<float>() {
     static const std::vector<Variant<float>> v = {
-#define MITTET_X(vx, bx, by, zc)                                                              \
-    {vx, bx, by, zc, e_interior_kernel<float, vx, bx, by>, h_interior_kernel<float, vx, bx, by>, \
-     e_face_kernel<float, vx, bx, by>, h_face_kernel<float, vx, bx, by>,                         \
-     e_shell_kernel<float, vx, bx, by>, h_shell_kernel<float, vx, bx, by>},
+#define MITTET_X(vx, bx, by, zc) \
+    {vx, bx, by, zc, {MITTET_PARTS(e, float, vx, bx, by), MITTET_PARTS(h, float, vx, bx, by)}},
         MITTET_STENCIL_VARIANTS_F32(MITTET_X)
 #undef MITTET_X
     };
@@ -274,10 +276,8 @@ const std::vector<Variant<float>> &variants<float>() {
 template <>
 const std::vector<Variant<double>> &variants<double>() {
     static const std::vector<Variant<double>> v = {
-#define MITTET_X(vx, bx, by, zc)                                                                \
-    {vx, bx, by, zc, e_interior_kernel<double, vx, bx, by>, h_interior_kernel<double, vx, bx, by>, \
-     e_face_kernel<double, vx, bx, by>, h_face_kernel<double, vx, bx, by>,                         \
-     e_shell_kernel<double, vx, bx, by>, h_shell_kernel<double, vx, bx, by>},
+#define MITTET_X(vx, bx, by, zc) \
+    {vx, bx, by, zc, {MITTET_PARTS(e, double, vx, bx, by), MITTET_PARTS(h, double, vx, bx, by)}},
         MITTET_STENCIL_VARIANTS_F64(MITTET_X)
 #undef MITTET_X
     };
@@ -341,15 +341,18 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
         t.start[q + 1] = t.start[q] + t.ntx[q] * t.nty[q] * nzt;
     };
     if (X1 > X0 && Y1 > Y0 && Z1 > Z0) {
+        t.pbox[0] = t.nbox;
         add(0, X0, Y0, Z0, X1, Y1, Z1);
-        t.g0 = t.start[t.nbox];
+        t.pbox[1] = t.nbox;
         add(1, 0, Y0, Z0, X0, Y1, Z1);   // x faces
         add(1, X1, Y0, Z0, nx, Y1, Z1);
+        t.pbox[2] = t.nbox;
         add(2, X0, 0, Z0, X1, Y0, Z1);   // y faces
         add(2, X0, Y1, Z0, X1, ny, Z1);
+        t.pbox[3] = t.nbox;
         add(4, X0, Y0, 0, X1, Y1, Z0);   // z faces
         add(4, X0, Y0, Z1, X1, Y1, nz);
-        t.g1 = t.start[t.nbox];
+        t.pbox[4] = t.nbox;
         const int zr[2][2] = {{0, Z0}, {Z1, nz}};
         for (int zz = 0; zz < 2; zz++) {  // rings around the z faces
             const int za = zr[zz][0], zb = zr[zz][1];
@@ -363,9 +366,9 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
         add(7, 0, Y1, Z0, X0, ny, Z1);
         add(7, X1, Y1, Z0, nx, ny, Z1);
     } else {
-        t.g0 = t.g1 = 0;
         add(7, 0, 0, 0, nx, ny, nz);
     }
+    t.pbox[kParts] = t.nbox;  // without an interior every box is part 4 (pbox[0..4] = 0)
     return t;
 }
 
@@ -378,19 +381,18 @@ int upload_tilemaps(mittet_handle *h) {
         maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc);
         for (int p = 0; p < 2; p++) {
             const TileMap &t = maps[2 * v + p];
-            h->tiles[2 * v + p] = t.start[t.nbox];
-            h->tiles_int[2 * v + p] = t.g0;
-            h->tiles_face[2 * v + p] = t.g1;
+            for (int q = 0; q <= kParts; q++) h->ptile[2 * v + p][q] = t.start[t.pbox[q]];
         }
     }
     for (int p = 0; p < 2; p++) {  // the interior box (identical in every variant's map)
         const TileMap &t = maps[p];
-        h->has_ibox[p] = t.g0 > 0;
+        h->has_ibox[p] = t.pbox[1] > t.pbox[0];
         for (int q = 0; q < 3; q++) {
             h->ibox[p][q] = t.lo[0][q];
             h->ibox[p][3 + q] = t.hi[0][q];
         }
     }
+    h->tmaps_host = maps;
     CK(h->tmaps.ensure(maps.size() * sizeof(TileMap)));
     CK(cudaMemcpy(h->tmaps.p, maps.data(), maps.size() * sizeof(TileMap), cudaMemcpyHostToDevice));
     return MITTET_OK;
@@ -504,7 +506,7 @@ int build_tma_maps(mittet_handle *h) {
 
 // The interior of one phase with TMA config ci.
 template <typename T>
-int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a) {
+int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a, cudaStream_t st) {
     using S = TmaShape<T>;
     const int p = e ? 0 : 1;
     if (!h->has_ibox[p]) return 0;
@@ -519,7 +521,7 @@ int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a) {
     const int nzc = (tl.z1 - tl.z0 + c.zc - 1) / c.zc;
     const dim3 grid(tl.ntx * tl.nty * nzc, h->nshot), block(S::TX / 2, S::TY);
     const size_t smem = TmaStage<T, S::TX, S::TY>::bytes(e ? S::SE : S::SH);
-    (e ? c.ek : c.hk)<<<grid, block, smem, h->st>>>(a, tl, h->tma_maps[p], h->tma_nown[p], h->d_flag.as<int>());
+    (e ? c.ek : c.hk)<<<grid, block, smem, st>>>(a, tl, h->tma_maps[p], h->tma_nown[p], h->d_flag.as<int>());
     return 1;
 }
 
@@ -534,38 +536,55 @@ bool tma_usable(const mittet_handle *h, const PhaseArgs<T> &a) {
 // variant vi (vi < 0: TMA interior config -1 - vi); returns 1 if it
 // launched a kernel.
 template <typename T>
-int launch_part(mittet_handle *h, bool e, int part, int vi, const PhaseArgs<T> &a) {
+int launch_part(mittet_handle *h, bool e, int part, int vi, const PhaseArgs<T> &a, cudaStream_t st = nullptr) {
+    if (!st) st = h->st;
     if (vi < 0) {
-        if (part == 0 && tma_usable<T>(h, a)) return launch_tma<T>(h, e, -1 - vi, a);
+        if (part == 0 && tma_usable<T>(h, a)) return launch_tma<T>(h, e, -1 - vi, a, st);
         vi = h->ldg_int[e ? 0 : 1];  // other buffers (gradient replays): best plain-load body
     }
     const Variant<T> &v = variants<T>()[vi];
     const int slot = 2 * vi + (e ? 0 : 1);
     const TileMap *tm = h->tmaps.as<TileMap>() + slot;
-    const int g0 = h->tiles_int[slot], g1 = h->tiles_face[slot], n_all = h->tiles[slot];
-    const int first = part == 0 ? 0 : (part == 1 ? g0 : g1);
-    const int last = part == 0 ? g0 : (part == 1 ? g1 : n_all);
+    const int first = h->ptile[slot][part], last = h->ptile[slot][part + 1];
     if (last <= first) return 0;
+    const TileMap &th = h->tmaps_host[slot];
     dim3 block(v.bx, v.by), grid(last - first, h->nshot);
-    if (part == 0) {
-        if (e) v.ei<<<grid, block, 0, h->st>>>(a, tm);
-        else v.hi<<<grid, block, 0, h->st>>>(a, tm);
-    } else if (part == 1) {
-        if (e) v.ef<<<grid, block, 0, h->st>>>(a, tm, first);
-        else v.hf<<<grid, block, 0, h->st>>>(a, tm, first);
-    } else {
-        if (e) v.es<<<grid, block, 0, h->st>>>(a, tm, first);
-        else v.hs<<<grid, block, 0, h->st>>>(a, tm, first);
-    }
+    v.k[e ? 0 : 1][part]<<<grid, block, 0, st>>>(a, tm, first, th.pbox[part], th.pbox[part + 1]);
     return 1;
 }
 
-// One phase = interior, faces, edges (up to three launches, each part with
-// its own variant).  Returns the number of launches.
+// Side streams and events of the concurrent parts, created once per handle.
+int ensure_part_streams(mittet_handle *h) {
+    if (h->ev_fork) return MITTET_OK;
+    for (int p = 1; p < kParts; p++) {
+        CK(cudaStreamCreateWithFlags(&h->pst[p], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->ev_join[p], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    return MITTET_OK;
+}
+
+// One phase = interior, x/y/z faces and edges, each part with its own variant.
+// The parts write disjoint cells (and their own psi and ring entries) and
+// only read the other field, so the x/y/z faces and edges run on side streams
+// concurrently with the interior, forked from and joined back to the
+// handle's stream (inside a capture these become parallel graph branches,
+// and each part's tail overlaps the others).  Returns the number of launches.
 template <typename T>
 int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a) {
     int n = 0;
-    for (int part = 0; part < 3; part++) n += launch_part<T>(h, e, part, vi[part], a);
+    if (!h->ev_fork || std::getenv("MITTET_SERIAL_PARTS")) {
+        for (int part = 0; part < kParts; part++) n += launch_part<T>(h, e, part, vi[part], a);
+        return n;
+    }
+    cudaEventRecord(h->ev_fork, h->st);
+    for (int p = 1; p < kParts; p++) cudaStreamWaitEvent(h->pst[p], h->ev_fork, 0);
+    n += launch_part<T>(h, e, 0, vi[0], a, h->st);
+    for (int p = 1; p < kParts; p++) n += launch_part<T>(h, e, p, vi[p], a, h->pst[p]);
+    for (int p = 1; p < kParts; p++) {
+        cudaEventRecord(h->ev_join[p], h->pst[p]);
+        cudaStreamWaitEvent(h->st, h->ev_join[p], 0);
+    }
     return n;
 }
 
@@ -586,7 +605,7 @@ void launch_step(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &h
 // fields, so the state is untouched apart from the ring slot written by the
 // E phase).  Results are cached for the process.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 8>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 2>> g_tune_cache;
 
 template <typename T>
 int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
@@ -600,10 +619,49 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            for (int p = 0; p < 3; p++) { h->var_e[p] = it->second[p]; h->var_h[p] = it->second[3 + p]; }
-            h->ldg_int[0] = it->second[6];
-            h->ldg_int[1] = it->second[7];
+            for (int p = 0; p < kParts; p++) {
+                h->var_e[p] = it->second[p];
+                h->var_h[p] = it->second[kParts + p];
+            }
+            h->ldg_int[0] = it->second[2 * kParts];
+            h->ldg_int[1] = it->second[2 * kParts + 1];
             return MITTET_OK;
+        }
+    }
+    // A tune file (MITTET_TUNE_CACHE) carries choices across processes, e.g. so
+    // that a profiled run launches the kernels a plain run chose.
+    const char *tfile = std::getenv("MITTET_TUNE_CACHE");
+    auto key_text = [&]() {
+        char b[128];
+        snprintf(b, sizeof(b), "%d %d %d %d %d %d %d", std::get<0>(key), std::get<1>(key), std::get<2>(key),
+                 std::get<3>(key), std::get<4>(key), std::get<5>(key), std::get<6>(key));
+        return std::string(b);
+    };
+    if (tfile) {
+        if (FILE *f = fopen(tfile, "r")) {
+            char line[512];
+            const std::string kt = key_text();
+            while (fgets(line, sizeof(line), f)) {
+                if (strncmp(line, kt.c_str(), kt.size()) != 0 || line[kt.size()] != ':') continue;
+                std::array<int, 2 * kParts + 2> e;
+                int n = 0, off = (int)kt.size() + 1, used = 0;
+                while (n < (int)e.size() && sscanf(line + off, "%d%n", &e[n], &used) == 1) {
+                    off += used;
+                    n++;
+                }
+                if (n != (int)e.size()) continue;
+                for (int p = 0; p < kParts; p++) {
+                    h->var_e[p] = e[p];
+                    h->var_h[p] = e[kParts + p];
+                }
+                h->ldg_int[0] = e[2 * kParts];
+                h->ldg_int[1] = e[2 * kParts + 1];
+                fclose(f);
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tune_cache[key] = e;
+                return MITTET_OK;
+            }
+            fclose(f);
         }
     }
     const char *fix = std::getenv("MITTET_VARIANT");
@@ -611,7 +669,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     if (fix) {
         const int v = std::atoi(fix);
         if (v >= 0 && v < nv) {
-            for (int p = 0; p < 3; p++) h->var_e[p] = h->var_h[p] = v;
+            for (int p = 0; p < kParts; p++) h->var_e[p] = h->var_h[p] = v;
             h->ldg_int[0] = h->ldg_int[1] = v;
             if (only_tma) h->var_e[0] = h->var_h[0] = -1;
             return MITTET_OK;
@@ -622,11 +680,11 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     CK(cudaEventCreate(&e1));
     const long long cells = (long long)h->nshot * h->g.nx * h->g.ny * h->g.nz;
     const int reps = cells > (1LL << 24) ? 3 : (cells > (1LL << 20) ? 8 : 20);
-    static const char *pname[3] = {"interior", "faces", "edges"};
+    static const char *pname[kParts] = {"interior", "xfaces", "yfaces", "zfaces", "edges"};
     for (int ph = 0; ph < 2; ph++) {
         const PhaseArgs<T> &a = ph == 0 ? ea : ha;
         int *var = ph == 0 ? h->var_e : h->var_h;
-        for (int part = 0; part < 3; part++) {
+        for (int part = 0; part < kParts; part++) {
             // candidates: TMA interior configs (v < 0, part 0 only), then the plain-load variants
             float best = 1e30f, best_ldg = 1e30f;
             var[part] = 0;
@@ -665,8 +723,22 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = {h->var_e[0], h->var_e[1], h->var_e[2], h->var_h[0], h->var_h[1], h->var_h[2],
-                         h->ldg_int[0], h->ldg_int[1]};
+    std::array<int, 2 * kParts + 2> entry;
+    for (int p = 0; p < kParts; p++) {
+        entry[p] = h->var_e[p];
+        entry[kParts + p] = h->var_h[p];
+    }
+    entry[2 * kParts] = h->ldg_int[0];
+    entry[2 * kParts + 1] = h->ldg_int[1];
+    g_tune_cache[key] = entry;
+    if (tfile) {
+        if (FILE *f = fopen(tfile, "a")) {
+            fprintf(f, "%s:", key_text().c_str());
+            for (int v : entry) fprintf(f, " %d", v);
+            fprintf(f, "\n");
+            fclose(f);
+        }
+    }
     return MITTET_OK;
 }
 
@@ -699,6 +771,8 @@ template <typename T>
 int run_forward(mittet_handle *h, int nt) {
     const int ns = h->nshot;
     int rc = ensure_state(h);
+    if (rc) return rc;
+    rc = ensure_part_streams(h);
     if (rc) return rc;
     CK(h->d_step.ensure(sizeof(int)));
     CK(h->d_flag.ensure(sizeof(int)));
@@ -820,6 +894,8 @@ int run_forward(mittet_handle *h, int nt) {
 template <typename T>
 int time_kernels(mittet_handle *h, int nsteps, double *ms) {
     int rc = ensure_state(h);
+    if (rc) return rc;
+    rc = ensure_part_streams(h);
     if (rc) return rc;
     rc = build_tma_maps<T>(h);
     if (rc) return rc;
@@ -1379,6 +1455,11 @@ void mittet_destroy(mittet_handle *h) {
     cudaSetDevice(h->ph.device);
     drop_graph(h);
     if (h->st) cudaStreamSynchronize(h->st);
+    for (int p = 0; p < kParts; p++) {
+        if (h->pst[p]) cudaStreamDestroy(h->pst[p]);
+        if (h->ev_join[p]) cudaEventDestroy(h->ev_join[p]);
+    }
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -1691,12 +1772,12 @@ int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1
 
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg) {
     if (!h || !e_cfg || !h_cfg) return fail(MITTET_ERR_INVALID_ARG, "null argument");
-    int32_t all[24];
+    int32_t all[2 * kParts * 4];
     int rc = mittet_tuned_variants(h, all);
     if (rc) return rc;
     for (int q = 0; q < 4; q++) {
         e_cfg[q] = all[q];
-        h_cfg[q] = all[12 + q];
+        h_cfg[q] = all[kParts * 4 + q];
     }
     return MITTET_OK;
 }
@@ -1706,9 +1787,9 @@ int mittet_tuned_variants(mittet_handle *h, int32_t *cfg) {
     auto fill = [&](auto tag) {
         using T = decltype(tag);
         for (int ph = 0; ph < 2; ph++)
-            for (int p = 0; p < 3; p++) {
+            for (int p = 0; p < kParts; p++) {
                 const int vi = (ph == 0 ? h->var_e : h->var_h)[p];
-                int32_t *c = cfg + (ph * 3 + p) * 4;
+                int32_t *c = cfg + (ph * kParts + p) * 4;
                 if (vi < 0) {  // TMA-staged interior: VX = 0, then the tile and z planes per CTA
                     c[0] = 0; c[1] = TmaShape<T>::TX; c[2] = TmaShape<T>::TY; c[3] = tma_cfgs<T>()[-1 - vi].zc;
                 } else {
@@ -1749,6 +1830,70 @@ int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t che
     rc = set_device(h);
     if (rc) return rc;
     return h->fp64 ? run_gradient<double>(h, nt, obs, K, misfit, grad) : run_gradient<float>(h, nt, obs, K, misfit, grad);
+}
+
+int mittet_fwi_update(mittet_handle *h, int32_t nt, const double *obs, const double *ecal, const double *grad,
+                      int32_t iseabed, double minval, double maxval, double *sigma, double *step) {
+    if (!h || !obs || !ecal || !grad || !sigma || !step) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    int rc = validate_ready(h, nt);
+    if (rc) return rc;
+    if (h->nrec <= 0 || h->omega.empty()) return fail(MITTET_ERR_STATE, "the update needs receivers and frequencies");
+    if (!(minval <= maxval)) return fail(MITTET_ERR_INVALID_ARG, "minval must not exceed maxval");
+    const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz, nc = h->g.ncpml;
+    const size_t n = (size_t)nx * ny * nz;
+    // calc_phi (satan_i/fwi3d_cpu_function_v1.4.c:2565-2603): maxima of sigma
+    // and grad over k <= iseabed, starting from cell 0; trial sigma2.
+    double sigmax2 = sigma[0], gradmax = grad[0];
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                const size_t ijk = ((size_t)k * ny + j) * nx + i;
+                if (k <= iseabed) {
+                    if (sigma[ijk] > sigmax2) sigmax2 = sigma[ijk];
+                    if (grad[ijk] > gradmax) gradmax = grad[ijk];
+                }
+            }
+    if (!(gradmax != 0.0) || !std::isfinite(gradmax))
+        return fail(MITTET_ERR_INVALID_ARG, "largest gradient above the seabed is %g: no step scale", gradmax);
+    const double scaler = (double)0.01f * sigmax2 / gradmax;
+    std::vector<double> sig2(n);
+    for (size_t q = 0; q < n; q++) sig2[q] = sigma[q] - scaler * grad[q];
+    // trial forward of every shot (media_coeff_sig_tmp + fwdpropagation + laplaceToFreq_3)
+    std::vector<double> mu_keep = h->mu_h;
+    const double *mu = mu_keep.empty() ? nullptr : mu_keep.data();
+    rc = mittet_set_model(h, sig2.data(), mu);
+    if (rc) return rc;
+    const int nf = (int)h->omega.size();
+    const size_t nspec = (size_t)h->nshot * h->nrec * nf;
+    std::vector<double> e2(2 * nspec);
+    const uint32_t vmask_saved = h->vmask;
+    if (h->vmask) { h->vmask = 0; drop_graph(h); }
+    rc = mittet_forward(h, nt, e2.data(), nullptr);
+    h->vmask = vmask_saved;
+    if (vmask_saved) drop_graph(h);
+    if (rc) return rc;
+    // calc_alpha (function.c:2757-2785): k1 = sum dE (E2 - Ecal), k2 = sum (E2 - Ecal)^2
+    std::complex<double> k1 = 0.0, k2 = 0.0;
+    for (size_t q = 0; q < nspec; q++) {
+        const std::complex<double> d(obs[2 * q] - ecal[2 * q], obs[2 * q + 1] - ecal[2 * q + 1]);
+        const std::complex<double> c(e2[2 * q] - ecal[2 * q], e2[2 * q + 1] - ecal[2 * q + 1]);
+        k1 += d * c;
+        k2 += c * c;
+    }
+    if (!(std::abs(k2) > 0)) return fail(MITTET_ERR_INVALID_ARG, "trial model changes no receiver value (k2 = 0)");
+    // update_para2 (function.c:2787-2832)
+    const double alpha = 3.0f * std::abs(k1) / std::abs(k2);
+    for (int k = nc; k < nz - nc; k++)
+        for (int j = nc; j < ny - nc; j++)
+            for (int i = nc; i < nx - nc; i++) {
+                const size_t ijk = ((size_t)k * ny + j) * nx + i;
+                if (k <= iseabed) sigma[ijk] += alpha * scaler * grad[ijk];
+                if (sigma[ijk] < minval) sigma[ijk] = minval;
+                if (sigma[ijk] > maxval) sigma[ijk] = maxval;
+            }
+    step[0] = scaler;
+    step[1] = alpha;
+    return mittet_set_model(h, sigma, mu);
 }
 
 }  // extern "C"

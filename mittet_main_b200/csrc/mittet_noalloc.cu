@@ -239,7 +239,7 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
     memset(&tm, 0, sizeof(tm));
     tm.nbox = 1;
     tm.zc = NA_ZC;
-    tm.g0 = tm.g1 = 0;
+    tm.pbox[kParts] = 1;  // one general box: part 4 (edges body) covers the grid
     tm.kind[0] = 7;
     tm.hi[0][0] = nx; tm.hi[0][1] = ny; tm.hi[0][2] = nz;
     tm.ntx[0] = (nx + NA_BX * NA_VX - 1) / (NA_BX * NA_VX);
@@ -347,9 +347,9 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
     const dim3 grid(tm.start[1], 1), block(NA_BX, NA_BY);
     for (int s = 0; s < nt; s++) {
         if (has_mag) inject_kernel<float><<<1, 128, 0, st>>>(ia_m);
-        e_shell_kernel<float, NA_VX, NA_BX, NA_BY><<<grid, block, 0, st>>>(pa[0], dtm, 0);
+        e_part_kernel<float, NA_VX, NA_BX, NA_BY, 7><<<grid, block, 0, st>>>(pa[0], dtm, 0, 0, 1);
         if (has_ele) inject_kernel<float><<<1, 128, 0, st>>>(ia_e);
-        h_shell_kernel<float, NA_VX, NA_BX, NA_BY><<<grid, block, 0, st>>>(pa[1], dtm, 0);
+        h_part_kernel<float, NA_VX, NA_BX, NA_BY, 7><<<grid, block, 0, st>>>(pa[1], dtm, 0, 0, 1);
         sample_kernel<float><<<1, 1024, 0, st>>>(sa);
     }
     trace_dft_kernel<float><<<nf, 256, 0, st>>>((const float *)(base + o_tr), nrec, nt, (const double *)(base + o_om), nf,

@@ -8,8 +8,8 @@
 // is one template specialised by a mask GM of the axes handled generally, so
 // the interior (GM = 0) is straight-line code, a face carries one axis's
 // CPML terms, and only edges and corners (GM = 7) pay for all of them.
-// Three launches per phase (interior, faces, general), each with its own
-// thread-tile shape; blockIdx.x enumerates tiles through a TileMap in global
+// Five launches per phase (interior, x faces, y faces, z faces, edges), each
+// with its own thread-tile shape; blockIdx.x enumerates tiles through a TileMap in global
 // memory, blockIdx.y is the shot.  The interior box is the exact interior
 // (x edges on multiples of 4 cells), so its last tile in x and y may be
 // partial.  Every body uses the same explicit fma forms, so a cell gets
@@ -40,14 +40,18 @@
 namespace mittet {
 
 // Boxes of one phase, in the order their tiles are enumerated: the interior
-// box, then six faces (CPML / range handling along one axis only), then the
-// edge and corner boxes (general handling).  kind = mask of the axes that
-// need general handling (0 interior, 1/2/4 faces, 7 general).
+// box, the two x faces, the two y faces, the two z faces (CPML / range
+// handling along one axis only), then the edge and corner boxes (general
+// handling).  kind = mask of the axes that need general handling (0
+// interior, 1/2/4 faces, 7 general).  Part p (0 interior, 1 x faces, 2 y
+// faces, 3 z faces, 4 edges) is boxes [pbox[p], pbox[p+1]), tiles
+// [start[pbox[p]], start[pbox[p+1]]).
+constexpr int kParts = 5;
 struct TileMap {
     int nbox;
-    int zc;           // z planes per tile (each thread marches through them)
-    int g0, g1;       // tiles [0, g0) interior, [g0, g1) faces, [g1, start[nbox]) general
-    int start[25];    // first tile of each box
+    int zc;            // z planes per tile (each thread marches through them)
+    int pbox[kParts + 1];
+    int start[25];     // first tile of each box
     int kind[24];
     int lo[24][3], hi[24][3];
     int ntx[24], nty[24];
@@ -678,14 +682,13 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
     }
 }
 
-// Locate this CTA's box and tile (tile index b over boxes [q0, nbox)): the
+// Locate this CTA's box and tile (tile index b, boxes [q0, q1)): the
 // thread's first x cell i0, its row j and its z planes [kb, ke).
 template <int VX, int BX, int BY>
-__device__ __forceinline__ int locate(const TileMap *__restrict__ tm, int q0, int b, int &i0, int &j, int &kb,
-                                      int &ke, bool &inside) {
-    const int nbox = __ldg(&tm->nbox);
+__device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int q0, int q1, int b, int &i0, int &j,
+                                       int &kb, int &ke, bool &inside) {
     int q = q0;
-    for (int t = q0 + 1; t < nbox; t++)
+    for (int t = q0 + 1; t < q1; t++)
         if (b >= __ldg(&tm->start[t])) q = t;
     const int local = b - __ldg(&tm->start[q]);
     const int ntx = __ldg(&tm->ntx[q]), nty = __ldg(&tm->nty[q]), zc = __ldg(&tm->zc);
@@ -696,41 +699,24 @@ __device__ __forceinline__ int locate(const TileMap *__restrict__ tm, int q0, in
     kb = __ldg(&tm->lo[q][2]) + tz * zc;
     ke = min(kb + zc, __ldg(&tm->hi[q][2]));
     inside = i0 < __ldg(&tm->hi[q][0]) && j < __ldg(&tm->hi[q][1]);
-    return __ldg(&tm->kind[q]);
 }
 
-#define MITTET_PHASE_KERNELS(PH)                                                                             \
-    template <typename T, int VX, int BX, int BY>                                                            \
-    __global__ void __launch_bounds__(BX *BY, MITTET_MINB(T, VX, BX *BY))                                    \
-        PH##_interior_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm) {                         \
+// One kernel per body: GM = 0 interior, 1/2/4 the x/y/z faces, 7 edges and
+// corners.  Tiles [first_tile, first_tile + gridDim.x) of boxes [q0, q1).
+#define MITTET_PHASE_KERNEL(PH)                                                                              \
+    template <typename T, int VX, int BX, int BY, int GM>                                                    \
+    __global__ void __launch_bounds__(BX *BY, GM == 0 ? MITTET_MINB(T, VX, BX *BY)                           \
+                                                      : MITTET_MINB_GEN(T, VX, BX *BY))                      \
+        PH##_part_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile, int q0, int q1) { \
         int i0, j, kb, ke;                                                                                   \
         bool inside;                                                                                         \
-        locate<VX, BX, BY>(tm, 0, blockIdx.x, i0, j, kb, ke, inside);                                        \
-        if (inside) PH##_cells<T, VX, 0>(a, blockIdx.y, i0, j, kb, ke);                                      \
-    }                                                                                                        \
-    template <typename T, int VX, int BX, int BY>                                                            \
-    __global__ void __launch_bounds__(BX *BY, MITTET_MINB_GEN(T, VX, BX *BY))                                \
-        PH##_face_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {            \
-        int i0, j, kb, ke;                                                                                   \
-        bool inside;                                                                                         \
-        const int kind = locate<VX, BX, BY>(tm, 1, first_tile + blockIdx.x, i0, j, kb, ke, inside);          \
-        if (!inside) return;                                                                                 \
-        if (kind == 1) PH##_cells<T, VX, 1>(a, blockIdx.y, i0, j, kb, ke);                                   \
-        else if (kind == 2) PH##_cells<T, VX, 2>(a, blockIdx.y, i0, j, kb, ke);                              \
-        else PH##_cells<T, VX, 4>(a, blockIdx.y, i0, j, kb, ke);                                             \
-    }                                                                                                        \
-    template <typename T, int VX, int BX, int BY>                                                            \
-    __global__ void __launch_bounds__(BX *BY, MITTET_MINB_GEN(T, VX, BX *BY))                                \
-        PH##_shell_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile) {           \
-        int i0, j, kb, ke;                                                                                   \
-        bool inside;                                                                                         \
-        locate<VX, BX, BY>(tm, 0, first_tile + blockIdx.x, i0, j, kb, ke, inside);                           \
-        if (inside) PH##_cells<T, VX, 7>(a, blockIdx.y, i0, j, kb, ke);                                      \
+        locate<VX, BX, BY>(tm, q0, q1, first_tile + blockIdx.x, i0, j, kb, ke, inside);                      \
+        if (inside) PH##_cells<T, VX, GM>(a, blockIdx.y, i0, j, kb, ke);                                     \
     }
 
-// e_interior_kernel / e_face_kernel / e_shell_kernel and the h_ ones.
-MITTET_PHASE_KERNELS(e)
-MITTET_PHASE_KERNELS(h)
+// e_part_kernel and h_part_kernel.
+MITTET_PHASE_KERNEL(e)
+MITTET_PHASE_KERNEL(h)
 
 // Variants the autotuner chooses from: (VX, BX, BY, ZC) = x cells per
 // thread, thread block, z planes each thread marches through.  ZC is a

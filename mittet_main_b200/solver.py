@@ -235,6 +235,25 @@ class MittetSolver:
         check(self._lib.mittet_gradient(self._h, nt, _dptr(o), checkpoint_every, _dptr(misfit), _dptr(grad)))
         return float(misfit[0]), grad
 
+    def fwi_update(self, nt: int, obs: np.ndarray, ecal: np.ndarray, grad: np.ndarray, sigma: np.ndarray,
+                   iseabed: int, minval: float, maxval: float):
+        """satan_i's model update (calc_phi, trial forward, calc_alpha,
+        update_para2; fwi3d_cpu_inv_fwi_v1.4.c:85-107).  Returns
+        (new sigma [nz, ny, nx], scaler, alpha); the solver's model becomes
+        the new sigma."""
+        def cplx(a):
+            o = np.zeros(a.shape + (2,), dtype=np.float64)
+            o[..., 0] = a.real
+            o[..., 1] = a.imag
+            return np.ascontiguousarray(o)
+        o, e = cplx(np.asarray(obs)), cplx(np.asarray(ecal))
+        g = np.ascontiguousarray(grad, dtype=np.float64)
+        sig = np.array(sigma, dtype=np.float64, order="C", copy=True)
+        step = np.zeros(2, dtype=np.float64)
+        check(self._lib.mittet_fwi_update(self._h, nt, _dptr(o), _dptr(e), _dptr(g), int(iseabed), float(minval),
+                                          float(maxval), _dptr(sig), _dptr(step)))
+        return sig, float(step[0]), float(step[1])
+
     def time_kernels(self, nsteps: int) -> dict:
         """Mean device ms per launch of each kernel over nsteps separately launched steps."""
         ms = np.zeros(6, dtype=np.float64)
@@ -243,11 +262,12 @@ class MittetSolver:
 
     def tuned_variant(self) -> dict:
         """[VX, BX, BY, ZC] the autotuner chose per phase and launch."""
-        c = (ctypes.c_int32 * 24)()
+        parts = ("interior", "xfaces", "yfaces", "zfaces", "edges")
+        c = (ctypes.c_int32 * (2 * len(parts) * 4))()
         check(self._lib.mittet_tuned_variants(self._h, c))
         v = list(c)
-        return {f"{ph}_{part}": v[(i * 3 + p) * 4:(i * 3 + p + 1) * 4]
-                for i, ph in enumerate(("e", "h")) for p, part in enumerate(("interior", "faces", "edges"))}
+        return {f"{ph}_{part}": v[(i * len(parts) + p) * 4:(i * len(parts) + p + 1) * 4]
+                for i, ph in enumerate(("e", "h")) for p, part in enumerate(parts)}
 
     def launch_count(self) -> int:
         return int(self._lib.mittet_last_launch_count(self._h))

@@ -321,3 +321,43 @@ def misfit(p: Params, sigma, mu, sources, wavelet, receivers, nt, omega, obs, h_
         S = dft(tr[r], p.dt, p.omega0, omega, h_factor=h_factor and rec[3].startswith("h"))
         J += 0.5 * float(np.sum(np.abs(S - obs[r]) ** 2))
     return J
+
+
+def calc_phi(sigma, grad, iseabed):
+    """satan_i calc_phi (fwi3d_cpu_function_v1.4.c:2565-2603): maxima of sigma
+    and grad over 0-based k <= iseabed, both starting from cell 0;
+    scaler = 0.01f * sigmax / gradmax; trial sigma2 = sigma - scaler * grad.
+    Arrays are [nz, ny, nx].  Returns (scaler, sigma2)."""
+    sigma = np.asarray(sigma, dtype=np.float64)
+    grad = np.asarray(grad, dtype=np.float64)
+    sigmax, gradmax = float(sigma.flat[0]), float(grad.flat[0])
+    top = slice(0, iseabed + 1)
+    if sigma[top].size:
+        sigmax = max(sigmax, float(sigma[top].max()))
+        gradmax = max(gradmax, float(grad[top].max()))
+    scaler = float(np.float32(0.01)) * sigmax / gradmax
+    return scaler, sigma - scaler * grad
+
+
+def update_para2(sigma, grad, obs, ecal, e2, scaler, iseabed, minval, maxval, ncpml):
+    """satan_i calc_alpha + update_para2 (fwi3d_cpu_function_v1.4.c:2757-2832):
+    k1 = sum dE (E2 - Ecal), k2 = sum (E2 - Ecal)^2 with dE = obs - Ecal, in
+    the order shot, receiver, frequency; alpha = 3 |k1| / |k2|; inside
+    [ncpml, n - ncpml) sigma += alpha * scaler * grad where k <= iseabed, then
+    clamp to [minval, maxval].  Returns (new sigma, alpha)."""
+    d = (np.asarray(obs) - np.asarray(ecal)).ravel()
+    c = (np.asarray(e2) - np.asarray(ecal)).ravel()
+    k1 = 0j
+    k2 = 0j
+    for q in range(d.size):
+        k1 += d[q] * c[q]
+        k2 += c[q] * c[q]
+    alpha = 3.0 * abs(k1) / abs(k2)
+    out = np.array(sigma, dtype=np.float64, copy=True)
+    nz, ny, nx = out.shape
+    inner = out[ncpml:nz - ncpml, ncpml:ny - ncpml, ncpml:nx - ncpml]
+    g = np.asarray(grad, dtype=np.float64)[ncpml:nz - ncpml, ncpml:ny - ncpml, ncpml:nx - ncpml]
+    ks = np.arange(ncpml, nz - ncpml)[:, None, None]
+    inner += np.where(ks <= iseabed, (alpha * scaler) * g, 0.0)
+    np.clip(inner, minval, maxval, out=inner)
+    return out, alpha

@@ -49,3 +49,26 @@ def test_oracle_gradient_is_zero_for_matching_data():
     _, _, spec = O.gradient(p, sig, mu, src, w, rec, nt, omega, np.zeros((len(rec), omega.size)))
     J, g, _ = O.gradient(p, sig, mu, src, w, rec, nt, omega, spec)
     assert J == 0.0 and np.abs(g).max() == 0.0
+
+
+def test_restated_model_update_on_a_hand_case():
+    """oracle.calc_phi / oracle.update_para2 on a 4x4x4 case worked by hand."""
+    sig = np.full((4, 4, 4), 0.5)
+    sig[0, 0, 0] = 0.25
+    sig[1, 1, 1] = 2.0
+    grad = np.zeros((4, 4, 4))
+    grad[1, 1, 1] = 4.0
+    grad[2, 2, 2] = 8.0   # below the seabed (k = 2 > 1): not in the maxima
+    scaler, sig2 = O.calc_phi(sig, grad, iseabed=1)
+    assert scaler == float(np.float32(0.01)) * 2.0 / 4.0
+    assert sig2[1, 1, 1] == 2.0 - scaler * 4.0 and sig2[2, 2, 2] == 0.5 - scaler * 8.0
+    obs = np.array([[[1 + 1j]]])
+    ecal = np.array([[[0.5 + 0j]]])
+    e2 = np.array([[[0.5 + 0.5j]]])
+    new, alpha = O.update_para2(sig, grad, obs, ecal, e2, scaler, iseabed=1, minval=0.1, maxval=1.9, ncpml=1)
+    k1 = (0.5 + 1j) * 0.5j
+    k2 = (0.5j) ** 2
+    assert alpha == 3.0 * abs(k1) / abs(k2)
+    assert new[1, 1, 1] == 1.9                       # clamped to maxval
+    assert new[2, 2, 2] == 0.5                       # below the seabed: only clamped
+    assert new[0, 0, 0] == 0.25                      # CPML frame untouched
