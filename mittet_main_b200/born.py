@@ -17,7 +17,12 @@ normalisation of satan_i (E / J times the FFT of its "true" wavelet) is
 replaced by the plain Green's-function form that makes the formula the
 first-order derivative of this library's misfit 0.5 sum |Ecal - Eobs|^2:
 
-  grad_w(x) = Re [ (1/J_w) sum_c E_ff,c(x) E_back,c(x) ] * dx dy dz,
+  gamma_w(x) = Re [ (1/J_w) sum_c E_ff,c(x) E_back,c(x) ] * dx dy dz,
+
+which, like satan_i's gamma, is the descent direction -dJ/dsigma: the
+scattering current of a conductivity perturbation, (dsigma / 2 w0) dE'/dt' in
+the fictitious domain, enters Ampere's law as the source current does, and
+its transform is -i w' (dsigma / 2 w0) E = E dsigma / sqrt(-2 w0 / (i w)),
 
 J_w = the diffusive-domain spectrum of the injected source current: the
 f_to_d transform of the wavelet times sqrt(-2 w0 / (i w)), as satan_i's

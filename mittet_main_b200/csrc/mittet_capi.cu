@@ -403,24 +403,34 @@ int upload_tilemaps(mittet_handle *h) {
 // tile TX x TY (TX = 64 FP32 / 32 FP64 cells, TY = 8 rows), ring depth of
 // the E and H phases, z planes per CTA.
 template <typename T>
+struct TmaShape {
+    static constexpr int TX = sizeof(T) == 4 ? 64 : 32, TY = 8;
+};
+
+template <typename T>
 struct TmaCfg {
     int zc;
+    bool own_smem;  // own-cell tiles staged by TMA (else loaded by the threads)
+    int se, sh;     // ring depth of the E and H kernels
     void (*ek)(PhaseArgs<T>, TmaTiling, TmaMaps, int, int *);
     void (*hk)(PhaseArgs<T>, TmaTiling, TmaMaps, int, int *);
-};
-template <typename T>
-struct TmaShape {
-    static constexpr int TX = sizeof(T) == 4 ? 64 : 32, TY = 8, SE = 4, SH = 5;
+    size_t smem(bool e) const {
+        using S = TmaShape<T>;
+        return own_smem ? TmaStage<T, S::TX, S::TY, 4>::bytes(e ? se : sh)
+                        : TmaStage<T, S::TX, S::TY, 0>::bytes(e ? se : sh);
+    }
 };
 
 template <typename T>
 const std::vector<TmaCfg<T>> &tma_cfgs() {
-    using S = TmaShape<T>;
+    constexpr int TX = TmaShape<T>::TX, TY = TmaShape<T>::TY;
+#define MITTET_TMA(ZC, OWN, SE, SH) \
+    {ZC, OWN, SE, SH, interior_tma_kernel<T, TX, TY, SE, true, OWN>, interior_tma_kernel<T, TX, TY, SH, false, OWN>}
     static const std::vector<TmaCfg<T>> v = {
-        {8, interior_tma_kernel<T, S::TX, S::TY, S::SE, true>, interior_tma_kernel<T, S::TX, S::TY, S::SH, false>},
-        {16, interior_tma_kernel<T, S::TX, S::TY, S::SE, true>, interior_tma_kernel<T, S::TX, S::TY, S::SH, false>},
-        {32, interior_tma_kernel<T, S::TX, S::TY, S::SE, true>, interior_tma_kernel<T, S::TX, S::TY, S::SH, false>},
+        MITTET_TMA(8, true, 4, 5),  MITTET_TMA(16, true, 4, 5),  MITTET_TMA(32, true, 4, 5),
+        MITTET_TMA(8, false, 6, 6), MITTET_TMA(16, false, 6, 6), MITTET_TMA(32, false, 6, 6),
     };
+#undef MITTET_TMA
     return v;
 }
 
@@ -460,10 +470,8 @@ int build_tma_maps(mittet_handle *h) {
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(attr_once, [] {
         for (const auto &c : tma_cfgs<T>()) {
-            cudaError_t e1 = cudaFuncSetAttribute(c.ek, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)TmaStage<T, S::TX, S::TY>::bytes(S::SE));
-            cudaError_t e2 = cudaFuncSetAttribute(c.hk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)TmaStage<T, S::TX, S::TY>::bytes(S::SH));
+            cudaError_t e1 = cudaFuncSetAttribute(c.ek, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem(true));
+            cudaError_t e2 = cudaFuncSetAttribute(c.hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem(false));
             if (e1 != cudaSuccess) attr_err = e1;
             if (e2 != cudaSuccess) attr_err = e2;
         }
@@ -520,7 +528,7 @@ int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a, cudaStre
     tl.zc = c.zc;
     const int nzc = (tl.z1 - tl.z0 + c.zc - 1) / c.zc;
     const dim3 grid(tl.ntx * tl.nty * nzc, h->nshot), block(S::TX / 2, S::TY);
-    const size_t smem = TmaStage<T, S::TX, S::TY>::bytes(e ? S::SE : S::SH);
+    const size_t smem = c.smem(e);
     (e ? c.ek : c.hk)<<<grid, block, smem, st>>>(a, tl, h->tma_maps[p], h->tma_nown[p], h->d_flag.as<int>());
     return 1;
 }
@@ -613,8 +621,13 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     const bool only_ldg = imode && std::string(imode) == "ldg";
     const bool only_tma = imode && std::string(imode) == "tma" && tma_usable<T>(h, ea) && tma_usable<T>(h, ha);
     const bool try_tma = !only_ldg && tma_usable<T>(h, ea) && tma_usable<T>(h, ha);
+    // MITTET_TMA_CFG=<c> with MITTET_INTERIOR=tma pins the interior of both
+    // phases to TMA configuration c (the other parts are still tuned).
+    const char *tcfg = std::getenv("MITTET_TMA_CFG");
+    const int pin_tma = (only_tma && tcfg) ? std::atoi(tcfg) : -1;
+    const bool pinned = pin_tma >= 0 && pin_tma < (int)tma_cfgs<T>().size();
     const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0,
-                                     (try_tma ? 1 : 0) + (only_tma ? 2 : 0));
+                                     (try_tma ? 1 : 0) + (only_tma ? 2 : 0) + (pinned ? 4 * (pin_tma + 1) : 0));
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
@@ -708,7 +721,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
                                 variants<T>()[v].vx, variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].zc,
                                 ms / reps);
                 }
-                const bool eligible = !(only_tma && part == 0 && v >= 0);
+                const bool eligible = !(only_tma && part == 0 && v >= 0) && !(pinned && part == 0 && v != -1 - pin_tma);
                 if (eligible && ms < best) {
                     best = ms;
                     var[part] = v;
@@ -1221,6 +1234,12 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
             ae.slab[ax] = to_dslab(h->su.se[ax]);
             ah.upd[ax] = to_dbox(h->su.upd[3 + ax]);
             ae.upd[ax] = to_dbox(h->su.upd[ax]);
+            ah.ik[ax] = ae.ik[ax] = (T)(1.0 / (ax == 0 ? h->g.dx : (ax == 1 ? h->g.dy : h->g.dz)));
+            // the forward's interior boxes (empty when the grid has none)
+            ae.ibox.lo[ax] = h->has_ibox[0] ? h->ibox[0][ax] : 0;
+            ae.ibox.hi[ax] = h->has_ibox[0] ? h->ibox[0][3 + ax] : 0;
+            ah.ibox.lo[ax] = h->has_ibox[1] ? h->ibox[1][ax] : 0;
+            ah.ibox.hi[ax] = h->has_ibox[1] ? h->ibox[1][3 + ax] : 0;
             for (int w = 0; w < 2; w++) { ah.lpsi[ax][w] = lph[ax][w].as<T>(); ae.lpsi[ax][w] = lpe[ax][w].as<T>(); }
         }
         ah.sgn = (T)h->ph.h_sign;

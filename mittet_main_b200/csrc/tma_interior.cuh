@@ -11,6 +11,8 @@
 //   B  the field differentiated along x  E: Hy         H: Ey
 //   C  the field differentiated along y  E: Hx         H: Ex
 //   own-cell tiles                        E: m Ex Ey Ez H: Hx Hy Hz [dt/mu]
+//      (OWN_SMEM; otherwise each thread loads its own cells directly,
+//      before waiting for the plane, and the ring stage is half the size)
 // B and C are also differentiated along z: their centre values of planes
 // k-L .. k+U ride in a rolling register window, so a plane's stage is needed
 // only while it is the window's newest plane and while it is plane k.  After
@@ -49,14 +51,15 @@ struct TmaTiling {
     int ntx, nty, zc;            // tiles in x and y, z planes per chunk
 };
 
-// Stage geometry shared by the host (shared-memory size) and the kernel.
-template <typename T, int TX, int TY>
+// Stage geometry shared by the host (shared-memory size) and the kernel;
+// OWN = own-cell tiles staged per plane (4) or loaded by the threads (0).
+template <typename T, int TX, int TY, int OWN>
 struct TmaStage {
     static constexpr int PA = TX + 8;  // pitch of the A and B tiles
     static constexpr int NA = PA * (TY + 3), NB = PA * TY, NC = TX * (TY + 3), NO = TX * TY;
     static constexpr int r32(int n) { return (n + 31) / 32 * 32; }
     static constexpr int OA = 0, OB = r32(NA), OC = OB + r32(NB), OO = OC + r32(NC);
-    static constexpr int ELEMS = OO + 4 * NO;  // stage size in elements (multiple of 32)
+    static constexpr int ELEMS = OO + OWN * NO;  // stage size in elements (multiple of 32)
     static constexpr size_t bytes(int S) { return (size_t)S * ELEMS * sizeof(T) + (size_t)S * 8; }
 };
 
@@ -91,12 +94,12 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 constexpr int kMbarSpinLimit = 1 << 20;   // try_wait polls before a wait gives up
 constexpr int kMbarDrainLimit = 1 << 16;  // polls per in-flight copy when draining
 
-template <typename T, int TX, int TY, int S, bool EPH>
+template <typename T, int TX, int TY, int S, bool EPH, bool OWN_SMEM>
 __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const PhaseArgs<T> a, const TmaTiling tl,
                                                                      const __grid_constant__ TmaMaps maps, int nown,
                                                                      int *__restrict__ err) {
     constexpr int VX = 2;
-    using G = TmaStage<T, TX, TY>;
+    using G = TmaStage<T, TX, TY, OWN_SMEM ? 4 : 0>;
     constexpr int PA = G::PA, L = EPH ? 2 : 1, U = EPH ? 1 : 2, YH = EPH ? 2 : 1;
     static_assert(S >= U + 2, "ring too shallow for the window");
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
     const int i0 = X0 + lx, j = Y0 + ly;
     const bool inside = i0 < tl.x1 && j < tl.y1;
     const int zs = shot * a.nz;
-    const uint32_t bytes = (uint32_t)((G::NA + G::NB + G::NC + nown * G::NO) * sizeof(T));
+    const uint32_t bytes = (uint32_t)((G::NA + G::NB + G::NC + (OWN_SMEM ? nown * G::NO : 0)) * sizeof(T));
 
     // s_abort lets a wait that gave up release the CTA's other waits at once;
     // every decision to leave is taken through __syncthreads_or, so it is the
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
         tma_load_3d(smem_addr(st + G::OA), &maps.map[0], X0 - 4, Y0 - YH, zs + p, bar);
         tma_load_3d(smem_addr(st + G::OB), &maps.map[1], X0 - 4, Y0, zs + p, bar);
         tma_load_3d(smem_addr(st + G::OC), &maps.map[2], X0, Y0 - YH, zs + p, bar);
-        for (int q = 0; q < nown; q++) {
+        for (int q = 0; q < (OWN_SMEM ? nown : 0); q++) {
             const bool model = EPH ? q == 0 : q == 3;
             tma_load_3d(smem_addr(st + G::OO + q * G::NO), &maps.map[3 + q], X0, Y0, model ? p : zs + p, bar);
         }
@@ -185,6 +188,31 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
     for (int i = 0; i < ke - kb; i++) {
         const int k = kb + i;
         const int rn = i + L + U, ro = i + L;
+        const int c = k * pz + j * py + i0;
+        // own cells of plane k: staged tiles, or plain loads issued before the wait
+        T o0[VX], o1[VX], o2[VX], o3[VX];
+        if constexpr (!OWN_SMEM) {
+            if (inside) {
+                if constexpr (EPH) {
+                    ldv<T, VX>(o0, a.m + c);
+                    ldv_rw<T, VX>(o1, a.f[0] + sb + c);
+                    ldv_rw<T, VX>(o2, a.f[1] + sb + c);
+                    ldv_rw<T, VX>(o3, a.f[2] + sb + c);
+                } else {
+                    ldv_rw<T, VX>(o0, a.f[3] + sb + c);
+                    ldv_rw<T, VX>(o1, a.f[4] + sb + c);
+                    ldv_rw<T, VX>(o2, a.f[5] + sb + c);
+                    if (a.dtmu) {
+                        ldv<T, VX>(o3, a.dtmu + c);
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < VX; v++) o3[v] = a.dtmu0;
+                    }
+                }
+            } else {
+                zerov<T, VX>(o0); zerov<T, VX>(o1); zerov<T, VX>(o2); zerov<T, VX>(o3);
+            }
+        }
         wait(rn);
         const T *sn = sm + (size_t)(rn % S) * G::ELEMS;
         const T *so = sm + (size_t)(ro % S) * G::ELEMS;
@@ -207,7 +235,6 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
                 b6[2 * h + 1] = t[1];
             }
         }
-        const int c = k * pz + j * py + i0;
         if constexpr (EPH) {
             // rows y-2, y-1, y+1 of A (Hz) and C (Hx)
             T hzm2[VX], hzm1[VX], hzp1[VX], hxm2[VX], hxm1[VX], hxp1[VX];
@@ -218,10 +245,15 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
             ldv_rw<T, VX>(hxm1, C + (ly + 1) * TX + lx);
             ldv_rw<T, VX>(hxp1, C + (ly + 3) * TX + lx);
             T m[VX], ex[VX], ey[VX], ez[VX];
-            ldv_rw<T, VX>(m, O + 0 * G::NO + ly * TX + lx);
-            ldv_rw<T, VX>(ex, O + 1 * G::NO + ly * TX + lx);
-            ldv_rw<T, VX>(ey, O + 2 * G::NO + ly * TX + lx);
-            ldv_rw<T, VX>(ez, O + 3 * G::NO + ly * TX + lx);
+            if constexpr (OWN_SMEM) {
+                ldv_rw<T, VX>(m, O + 0 * G::NO + ly * TX + lx);
+                ldv_rw<T, VX>(ex, O + 1 * G::NO + ly * TX + lx);
+                ldv_rw<T, VX>(ey, O + 2 * G::NO + ly * TX + lx);
+                ldv_rw<T, VX>(ez, O + 3 * G::NO + ly * TX + lx);
+            } else {
+#pragma unroll
+                for (int v = 0; v < VX; v++) { m[v] = o0[v]; ex[v] = o1[v]; ey[v] = o2[v]; ez[v] = o3[v]; }
+            }
 #pragma unroll
             for (int v = 0; v < VX; v++) {
                 const T dyHz = d4(c1, c2, a6[2 + v], hzm1[v], hzp1[v], hzm2[v]);
@@ -256,14 +288,19 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
             ldv_rw<T, VX>(exp1, C + (ly + 2) * TX + lx);
             ldv_rw<T, VX>(exp2, C + (ly + 3) * TX + lx);
             T hx[VX], hy[VX], hz[VX], dm[VX];
-            ldv_rw<T, VX>(hx, O + 0 * G::NO + ly * TX + lx);
-            ldv_rw<T, VX>(hy, O + 1 * G::NO + ly * TX + lx);
-            ldv_rw<T, VX>(hz, O + 2 * G::NO + ly * TX + lx);
-            if (nown > 3) {
-                ldv_rw<T, VX>(dm, O + 3 * G::NO + ly * TX + lx);
+            if constexpr (OWN_SMEM) {
+                ldv_rw<T, VX>(hx, O + 0 * G::NO + ly * TX + lx);
+                ldv_rw<T, VX>(hy, O + 1 * G::NO + ly * TX + lx);
+                ldv_rw<T, VX>(hz, O + 2 * G::NO + ly * TX + lx);
+                if (nown > 3) {
+                    ldv_rw<T, VX>(dm, O + 3 * G::NO + ly * TX + lx);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < VX; v++) dm[v] = a.dtmu0;
+                }
             } else {
 #pragma unroll
-                for (int v = 0; v < VX; v++) dm[v] = a.dtmu0;
+                for (int v = 0; v < VX; v++) { hx[v] = o0[v]; hy[v] = o1[v]; hz[v] = o2[v]; dm[v] = o3[v]; }
             }
 #pragma unroll
             for (int v = 0; v < VX; v++) {

@@ -141,6 +141,13 @@ def write_waveform(path: str, dt: float, s: np.ndarray) -> None:
             f.write(f"{_c_exp(n * dt)} {_c_exp(v)}\n")
 
 
+def read_signal(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """A "t value" trace file (Fortran list-directed or numpy savetxt), e.g.
+    residual_wave_abso_rev.d read by corona/ver0030r_a/cpu_main.f90:41-46."""
+    a = np.loadtxt(path, dtype=np.float64, ndmin=2)
+    return a[:, 0], np.ascontiguousarray(a[:, 1])
+
+
 def spectrum_name(comp: str, shot: int, rec: int) -> str:
     """spectrum_e[xyz]_SSS_RRR.dat (read_Eobs, :913-915)."""
     return f"spectrum_{comp}_{shot:03d}_{rec:03d}.dat"
@@ -214,6 +221,19 @@ def write_f_to_d(dirname: str, name: str, freqs_hz: np.ndarray, ex_w: np.ndarray
         with open(os.path.join(dirname, f"abs{stem}{name}.d"), "w") as f:
             for fr, v in zip(freqs_hz, z):
                 f.write(f"  {float(fr):.17g}  {float(abs(v)):.17g}\n")
+
+
+def write_f_to_d_time(dirname: str, name: str, dt: float, ex_t: np.ndarray, jz_t: np.ndarray,
+                      gx_t: np.ndarray) -> None:
+    """EX_t<name>.d, JZ_t<name>.d, GXe_t<name>.d ("t re im") and the absEX_t
+    ... files ("t abs") of cpu_f_to_d_e.f90:303-320, t = n dt."""
+    for stem, z in (("EX_t", ex_t), ("JZ_t", jz_t), ("GXe_t", gx_t)):
+        with open(os.path.join(dirname, f"{stem}{name}.d"), "w") as f:
+            for n, v in enumerate(z):
+                f.write(f"  {n * dt:.17g}  {float(v.real):.17g}  {float(v.imag):.17g}\n")
+        with open(os.path.join(dirname, f"abs{stem}{name}.d"), "w") as f:
+            for n, v in enumerate(z):
+                f.write(f"  {n * dt:.17g}  {float(abs(v)):.17g}\n")
 
 
 def read_f_to_d(path: str) -> tuple[np.ndarray, np.ndarray]:

@@ -127,6 +127,21 @@ module mittet_gpu
             real(c_double), intent(out) :: grad(*)
         end function
 
+        ! satan_i model update (calc_phi, trial forward, calc_alpha, update_para2):
+        ! obs, ecal: complex(c_double_complex) (nf, nrec, nshot); grad, sigma: (nx, ny, nz);
+        ! step(1) = scaler, step(2) = alpha; sigma is updated in place.
+        integer(c_int) function mittet_fwi_update(handle, nt, obs, ecal, grad, iseabed, minval, maxval, sigma, step) &
+                bind(c, name="mittet_fwi_update")
+            import :: c_int, c_int32_t, c_ptr, c_double_complex, c_double
+            type(c_ptr), value :: handle
+            integer(c_int32_t), value :: nt, iseabed
+            complex(c_double_complex), intent(in) :: obs(*), ecal(*)
+            real(c_double), intent(in) :: grad(*)
+            real(c_double), value :: minval, maxval
+            real(c_double), intent(inout) :: sigma(*)
+            real(c_double), intent(out) :: step(2)
+        end function
+
         integer(c_int) function mittet_last_error(buf, len) bind(c, name="mittet_last_error")
             import :: c_int, c_char, c_size_t
             character(kind=c_char), intent(out) :: buf(*)

@@ -303,3 +303,15 @@ def f_to_d_h(hz_trace: np.ndarray, signal: np.ndarray, dt: float, omega0: float,
         hz_w = f_to_d(hz_trace, dt, omega0, omega, True, device)
         jz_w = f_to_d(signal, dt, omega0, omega, False, device)
         return hz_w, jz_w, hz_w / jz_w
+
+
+def to_time_domain(spec_w: np.ndarray, dt: float) -> np.ndarray:
+    """The time series f_to_d_e / f_to_d_h write after their spectra
+    (ncver0027/cpu_f_to_d_e.f90:241-320): an unnormalised inverse DFT with
+    FFTW's BACKWARD sign over the nd = len(spec_w) samples of the reference
+    frequency grid w_k = 2 pi k / (nd dt) (mittet_freq_grid_ref), scaled by
+    2 / (nd dt):  x[n] = 2 / (nd dt) sum_k X[k] exp(+2 pi i k n / nd).
+    Post-processing of a few thousand samples per trace; not on the GPU."""
+    x = np.asarray(spec_w, dtype=complex)
+    nd = x.shape[-1]
+    return np.fft.ifft(x, axis=-1) * nd * (2.0 / (nd * dt))

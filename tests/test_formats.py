@@ -77,3 +77,24 @@ def test_workload_from_satan_data_directory(tmp_path):
     courant = 1.0 / cmax / np.sqrt(3.0 / 50.0 ** 2)
     assert wl.cp.dt == courant * float(np.float32(6.0 / 7.0)) * float(np.float32(0.999)) or \
         abs(wl.cp.dt / (courant * 6.0 / 7.0 * 0.999) - 1) < 1e-6
+
+
+def test_time_domain_output_is_fftw_backward_scaled():
+    """to_time_domain = FFTW BACKWARD (e^{+2 pi i k n / nd}, unnormalised)
+    x 2/(nd dt), cpu_f_to_d_e.f90:281-305, checked against the direct sum."""
+    from mittet_main_b200.solver import to_time_domain
+
+    rng = np.random.default_rng(3)
+    nd, dt = 37, 7.4e-4
+    X = rng.normal(size=nd) + 1j * rng.normal(size=nd)
+    n = np.arange(nd)
+    direct = np.array([np.sum(X * np.exp(2j * np.pi * n * q / nd)) for q in range(nd)]) * 2.0 / (nd * dt)
+    assert np.allclose(to_time_domain(X, dt), direct, rtol=1e-12, atol=0)
+
+
+def test_time_domain_files(tmp_path):
+    z = np.array([1 + 1j, 2 - 3j, 0.5j])
+    F.write_f_to_d_time(str(tmp_path), "1010", 1e-3, z, 2 * z, 3 * z)
+    a = np.loadtxt(tmp_path / "GXe_t1010.d")
+    assert np.allclose(a[:, 0], [0.0, 1e-3, 2e-3]) and np.allclose(a[:, 1] + 1j * a[:, 2], 3 * z)
+    assert np.allclose(np.loadtxt(tmp_path / "absJZ_t1010.d")[:, 1], np.abs(2 * z))

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from mittet_main_b200 import workloads as W
-from mittet_main_b200.capi import FP32, FP64, SRC_ELECTRIC, SRC_MAGNETIC
+from mittet_main_b200.capi import FLAVOR_SATAN_I, FP32, FP64, SRC_ELECTRIC, SRC_MAGNETIC
 from mittet_main_b200.solver import Shot
 from oracle import oracle as O
 from tests.conftest import rel_l2
@@ -160,11 +160,21 @@ def test_gradient_agrees_with_satan_formula():
     cross-correlation (residualE / conv_GdelE / calc_gamma, without /sense and
     the out_True scaling), both on converged transforms (Nt long enough for the
     damped DFT to decay).  A continuous-limit formula, so the check is the
-    cosine similarity of the two gradients over the interior frame."""
+    cosine similarity of the two gradients over the interior frame, and the
+    least-squares scale between them."""
     from mittet_main_b200 import born
 
-    wl = W.small_case(n=(36, 34, 32), ncpml=8, nt=1500, precision=FP64, seed=5)
-    rec = [r for r in wl.receivers if r[3] in ("ex", "ey", "ez")]
+    # Nt: the wavelet (centred at pi/fmax ~ 1.3 s here) has ended and the damped
+    # transforms have decayed by e^-10 before the last step
+    # satan_i flavour: the ncver0027 magnetic CPML profile is negative in one
+    # layer (cpu_cpml4.f90:27), a gain that grows without bound over thousands
+    # of steps
+    wl = W.small_case(n=(36, 34, 32), ncpml=8, nt=4000, precision=FP64, seed=5, flavor=FLAVOR_SATAN_I)
+    nc = wl.cp.ncpml
+    inside = lambda r: all(nc < v <= n - nc for v, n in zip(r[:3], (wl.cp.nx, wl.cp.ny, wl.cp.nz)))
+    # E receivers off the CPML: each also becomes a dipole source of the reciprocal solves
+    rec = [r for r in wl.receivers if r[3] in ("ex", "ey", "ez") and inside(r)]
+    rec += [(x, y, z, c) for (x, y, z) in [(14, 12, 20), (24, 22, 21), (12, 24, 11)] for c in ("ex", "ey", "ez")]
     wl = replace(wl, receivers=rec, omega=2 * np.pi * np.array([1.0, 2.0]))
     true = wl.sigma.copy()
     true[12:20, 13:21, 12:20] *= 2.0
@@ -172,9 +182,21 @@ def test_gradient_agrees_with_satan_formula():
         obs, _ = s.forward(wl.nt)
     with W.make_solver(wl) as s:
         J, G = s.gradient(wl.nt, obs, checkpoint_every=200)
+    # away from the point sources and receivers: there the discrete gradient
+    # also carries the sigma-dependence of the injection gain 2 w0 dt/(sigma V)
+    # and the grid Green's functions differ most from the continuous ones
+    kk, jj, ii = np.meshgrid(np.arange(wl.cp.nz), np.arange(wl.cp.ny), np.arange(wl.cp.nx), indexing="ij")
+    far = np.ones(G.shape, dtype=bool)
+    for (x, y, z) in [p[:3] for p in wl.shots[0].points] + [r[:3] for r in wl.receivers]:
+        far &= np.maximum(np.maximum(abs(ii - (x - 1)), abs(jj - (y - 1))), abs(kk - (z - 1))) >= 3
     res = {}
     for cf in (True, False):
         gb, ecal = born.satan_formula_gradient(wl, obs, current_factor=cf)
-        res[cf] = born.compare(gb, G)
-    print("satan-formula vs discrete adjoint:", res)
-    assert max(r["cosine"] for r in res.values()) > 0.5, res
+        # satan_i's gamma is a descent direction: -dJ/dsigma
+        res[cf] = {"all": born.compare(-gb, G), "far": born.compare(-gb * far, G * far)}
+    print("satan-formula vs discrete adjoint:", res, "receivers", len(rec), "|G|", float(np.abs(G).max()))
+    # measured on a B200: cosine 0.99999994, least-squares scale 1.0065,
+    # scaled rel-L2 3.6e-4; without the current factor the cosine is 0.998
+    best = res[True]["all"]
+    assert best["cosine"] > 0.9999 and best["ls_rel_l2"] < 2e-3 and abs(best["ls_scale"] - 1) < 0.02, res
+    assert res[True]["far"]["cosine"] > 0.9999, res

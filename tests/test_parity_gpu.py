@@ -211,18 +211,21 @@ def test_single_step():
     assert np.allclose(td[0], ref, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("tma_cfg", [0, 4])
 @pytest.mark.parametrize("prec", [FP32, FP64])
 @pytest.mark.parametrize("flavor", [FLAVOR_NCVER0027, FLAVOR_SATAN_I])
-def test_tma_interior_is_bit_identical_to_plain_loads(monkeypatch, prec, flavor):
+def test_tma_interior_is_bit_identical_to_plain_loads(monkeypatch, prec, flavor, tma_cfg):
     """The TMA-staged interior kernel and the plain-load interior body use the
     same fma forms, so fields, traces and volume spectra agree bit for bit.
     The grid gives the interior partial tiles in x and y, several z chunks
-    and two shots."""
+    and two shots; both TMA layouts (own-cell tiles staged or loaded by the
+    threads) are pinned in turn."""
     wl = W.small_case(n=(150, 44, 40), ncpml=8, nt=70, precision=prec, flavor=flavor, magnetic=True)
     nx, ny, nz = wl.cp.nx, wl.cp.ny, wl.cp.nz
     second = Shot(points=[(nx // 3, ny // 2 + 3, nz // 2 - 4, "ey", SRC_ELECTRIC, 0.7)])
     wl = replace(wl, volume_dft="xyz", shots=[wl.shots[0], second])
     out = {}
+    monkeypatch.setenv("MITTET_TMA_CFG", str(tma_cfg))  # 0: own-cell tiles staged, 4: loaded by the threads
     for mode in ("ldg", "tma"):
         monkeypatch.setenv("MITTET_INTERIOR", mode)
         with W.make_solver(wl) as s:
@@ -240,3 +243,29 @@ def test_tma_interior_is_bit_identical_to_plain_loads(monkeypatch, prec, flavor)
     for fa, fb in zip(a[3], b[3]):
         for c in range(6):
             assert np.array_equal(fa[c], fb[c]), NAMES[c]
+
+
+def test_residual_reinjection_matches_oracle(tmp_path):
+    """read_source_3d_res: the magnetic sources driven by a time-reversed
+    residual (difference of two runs), read back from a "t value" file."""
+    from mittet_main_b200 import formats, rtm
+
+    wl = W.small_case(nt=120, precision=FP64, magnetic=True)
+    pert = wl.sigma.copy()
+    pert[10:16, 12:20, 12:18] *= 4.0
+    r = len(wl.receivers) // 2
+    with W.make_solver(wl) as s:
+        _, t0 = s.forward(wl.nt, want_traces=True)
+    with W.make_solver(replace(wl, sigma=pert)) as s:
+        _, t1 = s.forward(wl.nt, want_traces=True)
+    res = rtm.reversed_residual(t1[0, r], t0[0, r])
+    path = tmp_path / "residual_wave_abso_rev.d"
+    np.savetxt(path, np.c_[np.arange(1, wl.nt + 1) * wl.cp.dt, res])
+    _, sig = formats.read_signal(str(path))
+    w = rtm.reinjection_wavelet(sig)
+    wl2 = replace(wl, wavelet=w)
+    ref = oracle_run(wl2)
+    with W.make_solver(wl2) as s:
+        _, td = s.forward(wl.nt, want_traces=True)
+    assert np.abs(res).max() > 0
+    assert rel_l2(td[0], ref[0]) <= 1e-10
