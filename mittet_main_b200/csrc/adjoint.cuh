@@ -43,12 +43,6 @@ struct AdjArgs {
     DSlab slab[3];
     T c1, c2, c2t, sgn;
     double inv2w0dt;  // 1/(2 w0 dt): 1/sigma = m * inv2w0dt
-    // Interior box of this phase (no CPML profile, no psi slab, inside every
-    // update range, derivative defined; empty if none).  There the *_own step
-    // leaves lambda unchanged and mu is coefficient x lambda, so *_own stores
-    // nothing but the gradient and *_gather recomputes mu from lambda.
-    DBox ibox;
-    T ik[3];          // 1/d per axis (the interior 1/ked, 1/khd)
 };
 
 __device__ __forceinline__ bool adj_cell(int &i, int &j, int &k, int &shot, int nx, int ny, int nz) {
@@ -71,7 +65,6 @@ template <typename T>
 __global__ void adj_h_own_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
-    if (in_box(a.ibox, i, j, k)) return;  // lambda_H unchanged; mu recomputed by the gather
     const long long sb = (long long)shot * a.fshot;
     const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
     const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
@@ -157,39 +150,13 @@ __global__ void adj_h_own_kernel(AdjArgs<T> a) {
     a.lam[5][c] = in2 ? da[2] * L2 : L2;
 }
 
-// mu of the H phase at cell (i, j, k) (offset c): stored by adj_h_own outside
-// the interior box, recomputed from lambda_H inside it with the expression of
-// adj_h_own (so the value is the same bit for bit).
-//   q: 0 Dy+Ez, 1 Dz+Ey, 2 Dz+Ex, 3 Dx+Ez, 4 typo Dx Ez, 5 Dx+Ey, 6 Dy+Ex
-template <typename T>
-__device__ __forceinline__ T mu_h(const AdjArgs<T> &a, int q, long long c, long long cm, int i, int j, int k) {
-    if (!in_box(a.ibox, i, j, k)) return a.mu[q][c];
-    const T s = a.sgn;
-    const T db = a.dtmu ? a.dtmu[cm] : a.dtmu0;
-    switch (q) {
-        case 0: return -s * db * a.ik[1] * a.lam[3][c];
-        case 1: return s * db * a.ik[2] * a.lam[3][c];
-        case 2: return -s * db * a.ik[2] * a.lam[4][c];
-        case 3: return s * db * a.ik[0] * a.lam[4][c];
-        case 4: return T(0);
-        case 5: return -s * db * a.ik[0] * a.lam[5][c];
-        default: return s * db * a.ik[1] * a.lam[5][c];
-    }
-}
-
 // (D+^T mu)[u] = c1 mu[u-1] - c1 mu[u] + c2 mu[u-2] - c2 mu[u+1];  typo: c2t replaces c1 on mu[u]
-// axis 0/1/2 = x/y/z; (i, j, k) the cell, c and cm its field and model offsets.
 template <typename T>
-__device__ __forceinline__ T dplus_t(const AdjArgs<T> &a, int q, int axis, long long c, long long cm, int i, int j,
-                                     int k, T c1, T c2, T c1u) {
-    const int n = axis == 0 ? a.nx : (axis == 1 ? a.ny : a.nz);
-    const int v = axis == 0 ? i : (axis == 1 ? j : k);
-    const long long s = axis == 0 ? 1 : (axis == 1 ? (long long)a.px : a.plane);
-    const int di = axis == 0, dj = axis == 1, dk = axis == 2;
-    T r = -c1u * mu_h(a, q, c, cm, i, j, k);
-    if (v >= 1) r += c1 * mu_h(a, q, c - s, cm - s, i - di, j - dj, k - dk);
-    if (v >= 2) r += c2 * mu_h(a, q, c - 2 * s, cm - 2 * s, i - 2 * di, j - 2 * dj, k - 2 * dk);
-    if (v + 1 < n) r -= c2 * mu_h(a, q, c + s, cm + s, i + di, j + dj, k + dk);
+__device__ __forceinline__ T dplus_t(const T *__restrict__ mu, long long c, long long s, int v, int n, T c1, T c2, T c1u) {
+    T r = -c1u * mu[c];
+    if (v >= 1) r += c1 * mu[c - s];
+    if (v >= 2) r += c2 * mu[c - 2 * s];
+    if (v + 1 < n) r -= c2 * mu[c + s];
     return r;
 }
 
@@ -197,13 +164,13 @@ template <typename T>
 __global__ void adj_h_gather_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
-    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
-    const long long c = (long long)shot * a.fshot + cm;
+    const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i;
+    const long long sy = a.px, sz = a.plane;
     const T c1 = a.c1, c2 = a.c2;
-    const T gz = dplus_t(a, 0, 1, c, cm, i, j, k, c1, c2, c1) + dplus_t(a, 3, 0, c, cm, i, j, k, c1, c2, c1) +
-                 dplus_t(a, 4, 0, c, cm, i, j, k, c1, c2, a.c2t);
-    const T gy = dplus_t(a, 1, 2, c, cm, i, j, k, c1, c2, c1) + dplus_t(a, 5, 0, c, cm, i, j, k, c1, c2, c1);
-    const T gx = dplus_t(a, 2, 2, c, cm, i, j, k, c1, c2, c1) + dplus_t(a, 6, 1, c, cm, i, j, k, c1, c2, c1);
+    const T gz = dplus_t(a.mu[0], c, sy, j, a.ny, c1, c2, c1) + dplus_t(a.mu[3], c, 1, i, a.nx, c1, c2, c1) +
+                 dplus_t(a.mu[4], c, 1, i, a.nx, c1, c2, a.c2t);
+    const T gy = dplus_t(a.mu[1], c, sz, k, a.nz, c1, c2, c1) + dplus_t(a.mu[5], c, 1, i, a.nx, c1, c2, c1);
+    const T gx = dplus_t(a.mu[2], c, sz, k, a.nz, c1, c2, c1) + dplus_t(a.mu[6], c, sy, j, a.ny, c1, c2, c1);
     a.lam[0][c] += gx;
     a.lam[1][c] += gy;
     a.lam[2][c] += gz;
@@ -219,21 +186,6 @@ __global__ void adj_e_own_kernel(AdjArgs<T> a) {
     const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
     const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
     const T m = a.m[cm];
-    if (in_box(a.ibox, i, j, k)) {
-        // ca = 1, cb = m, every update in range: lambda_E is unchanged and mu is
-        // recomputed by the gather; only the gradient term (h = 0: dca = 0,
-        // dcb/cb = -1/sigma), in the arithmetic of the general path below.
-        const double isig = (double)m * a.inv2w0dt;
-        const double rcb = -isig / (1.0 + 0.0);
-        double gsum = 0.0;
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const double e0 = (double)a.E0[q][c], e1 = (double)a.E1[q][c];
-            gsum += (double)a.lam[q][c] * (0.0 * e0 + rcb * (e1 - 1.0 * e0));
-        }
-        a.grad[c] += gsum;
-        return;
-    }
     const T esh[3] = {pget(a, 0, 0, i), pget(a, 1, 0, j), pget(a, 2, 0, k)};
     const T ik[3] = {pget(a, 0, 6, i), pget(a, 1, 6, j), pget(a, 2, 6, k)};
     T ca[3], cb[3];
@@ -311,36 +263,13 @@ __global__ void adj_e_own_kernel(AdjArgs<T> a) {
     a.lam[2][c] = in2 ? ca[2] * L2 : L2;
 }
 
-// mu of the E phase at cell (i, j, k): stored by adj_e_own outside the
-// interior box, recomputed from lambda_E inside it with the expression of
-// adj_e_own.   q: 0 DyHz, 1 DzHy, 2 DzHx, 3 DxHz, 4 DxHy, 5 DyHx
-template <typename T>
-__device__ __forceinline__ T mu_e(const AdjArgs<T> &a, int q, long long c, long long cm, int i, int j, int k) {
-    if (!in_box(a.ibox, i, j, k)) return a.mu[q][c];
-    const T s = a.sgn;
-    const T cb = a.m[cm];
-    switch (q) {
-        case 0: return s * cb * a.ik[1] * a.lam[0][c];
-        case 1: return -s * cb * a.ik[2] * a.lam[0][c];
-        case 2: return s * cb * a.ik[2] * a.lam[1][c];
-        case 3: return -s * cb * a.ik[0] * a.lam[1][c];
-        case 4: return s * cb * a.ik[0] * a.lam[2][c];
-        default: return -s * cb * a.ik[1] * a.lam[2][c];
-    }
-}
-
 // (D^T mu)[u] = c1 mu[u] - c1 mu[u+1] + c2 mu[u-1] - c2 mu[u+2]
 template <typename T>
-__device__ __forceinline__ T dminus_t(const AdjArgs<T> &a, int q, int axis, long long c, long long cm, int i, int j,
-                                      int k, T c1, T c2) {
-    const int n = axis == 0 ? a.nx : (axis == 1 ? a.ny : a.nz);
-    const int v = axis == 0 ? i : (axis == 1 ? j : k);
-    const long long s = axis == 0 ? 1 : (axis == 1 ? (long long)a.px : a.plane);
-    const int di = axis == 0, dj = axis == 1, dk = axis == 2;
-    T r = c1 * mu_e(a, q, c, cm, i, j, k);
-    if (v + 1 < n) r -= c1 * mu_e(a, q, c + s, cm + s, i + di, j + dj, k + dk);
-    if (v >= 1) r += c2 * mu_e(a, q, c - s, cm - s, i - di, j - dj, k - dk);
-    if (v + 2 < n) r -= c2 * mu_e(a, q, c + 2 * s, cm + 2 * s, i + 2 * di, j + 2 * dj, k + 2 * dk);
+__device__ __forceinline__ T dminus_t(const T *__restrict__ mu, long long c, long long s, int v, int n, T c1, T c2) {
+    T r = c1 * mu[c];
+    if (v + 1 < n) r -= c1 * mu[c + s];
+    if (v >= 1) r += c2 * mu[c - s];
+    if (v + 2 < n) r -= c2 * mu[c + 2 * s];
     return r;
 }
 
@@ -348,12 +277,12 @@ template <typename T>
 __global__ void adj_e_gather_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
-    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
-    const long long c = (long long)shot * a.fshot + cm;
+    const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i;
+    const long long sy = a.px, sz = a.plane;
     const T c1 = a.c1, c2 = a.c2;
-    const T hz = dminus_t(a, 0, 1, c, cm, i, j, k, c1, c2) + dminus_t(a, 3, 0, c, cm, i, j, k, c1, c2);
-    const T hy = dminus_t(a, 1, 2, c, cm, i, j, k, c1, c2) + dminus_t(a, 4, 0, c, cm, i, j, k, c1, c2);
-    const T hx = dminus_t(a, 2, 2, c, cm, i, j, k, c1, c2) + dminus_t(a, 5, 1, c, cm, i, j, k, c1, c2);
+    const T hz = dminus_t(a.mu[0], c, sy, j, a.ny, c1, c2) + dminus_t(a.mu[3], c, 1, i, a.nx, c1, c2);
+    const T hy = dminus_t(a.mu[1], c, sz, k, a.nz, c1, c2) + dminus_t(a.mu[4], c, 1, i, a.nx, c1, c2);
+    const T hx = dminus_t(a.mu[2], c, sz, k, a.nz, c1, c2) + dminus_t(a.mu[5], c, sy, j, a.ny, c1, c2);
     a.lam[3][c] += hx;
     a.lam[4][c] += hy;
     a.lam[5][c] += hz;

@@ -9,7 +9,7 @@
 //   H phase: h_part_kernel x 5 / interior_tma_kernel
 //                   H update + CPML psi_H        cpu_eh_field_cpml42.f90:210-253, cpu_cpml4.f90:384-474
 //   sample_kernel   receiver gather + step++     cpu_output.f90:20-30
-// and every 32 steps volume_dft_kernel folds the E ring into the spectra.
+// and every 64 steps volume_dft_kernel folds the E ring into the spectra.
 // The step index lives in device memory (d_step) so a block of steps can be
 // captured once in a CUDA graph and replayed.
 //
@@ -228,19 +228,19 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 
 // ---------------------------------------------------- full-volume f_to_d
 //
-// Every ring_k (= 32) steps the E phase has left the last values of each
+// Every ring_k (= 64) steps the E phase has left the last values of each
 // selected E component in the ring; this kernel folds them into the FP64
 // accumulators:
 //   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring(vc, shot*fshot + cell, s),
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
 // Grid (cells, component, shot), one thread per cell.  A thread issues its
-// 32 ring loads (one 128-byte line per warp each) before any arithmetic, forms
-// the sum over the ring in the field precision T (at most 32 terms; for FP32
+// 64 ring loads (one 128-byte line per warp each) before any arithmetic, forms
+// the sum over the ring in the field precision T (at most 64 terms; for FP32
 // fields the partial sum carries ~1e-7 relative error) and adds it to the FP64
 // accumulators once per flush.  The weights of one group of up to four
 // frequencies are a by-value kernel parameter (zero for s >= cnt), so every
 // multiply reads its weight from the constant bank.
-constexpr int kFlushRing = 32;
+constexpr int kFlushRing = 64;
 constexpr int kFlushFreqs = 4;
 template <typename T>
 struct FlushWeights {

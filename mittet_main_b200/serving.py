@@ -62,7 +62,7 @@ def estimate_bytes(wl, mode: str = "forward", checkpoint_every: int = 200) -> in
     b = ns * (6 * fshot + 4 * slab) * esz + 2 * fshot * esz
     b += ns * len(wl.receivers) * wl.nt * esz + ns * len(wl.receivers) * len(wl.omega) * 16
     if wl.volume_dft:
-        b += 32 * 3 * ns * fshot * esz + ns * 3 * len(wl.omega) * fshot * 16
+        b += 64 * 3 * ns * fshot * esz + ns * 3 * len(wl.omega) * fshot * 16
     if mode == "gradient":
         K = checkpoint_every
         ncheck = -(-wl.nt // K)
