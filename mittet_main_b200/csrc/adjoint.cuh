@@ -43,6 +43,11 @@ struct AdjArgs {
     DSlab slab[3];
     T c1, c2, c2t, sgn;
     double inv2w0dt;  // 1/(2 w0 dt): 1/sigma = m * inv2w0dt
+    // Interior box of this phase (no CPML profile, no psi slab, inside every
+    // update range, derivative defined; empty if none): there *_own leaves
+    // lambda unchanged and only stores mu (and, for E, the gradient term).
+    DBox ibox;
+    T ik[3];          // 1/d per axis (the interior 1/ked, 1/khd)
 };
 
 __device__ __forceinline__ bool adj_cell(int &i, int &j, int &k, int &shot, int nx, int ny, int nz) {
@@ -68,8 +73,22 @@ __global__ void adj_h_own_kernel(AdjArgs<T> a) {
     const long long sb = (long long)shot * a.fshot;
     const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
     const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
-    const T m = a.m[cm];
     const T dm = a.dtmu ? a.dtmu[cm] : a.dtmu0;
+    if (in_box(a.ibox, i, j, k)) {
+        // da = 1, db = dt/mu, every update in range, no psi, no gradient term:
+        // the mu of the general path below, lambda_H unchanged
+        const T L0 = a.lam[3][c], L1 = a.lam[4][c], L2 = a.lam[5][c];
+        const T s = a.sgn;
+        a.mu[0][c] = -s * dm * a.ik[1] * L0;
+        a.mu[1][c] = s * dm * a.ik[2] * L0;
+        a.mu[2][c] = -s * dm * a.ik[2] * L1;
+        a.mu[3][c] = s * dm * a.ik[0] * L1;
+        a.mu[4][c] = T(0);
+        a.mu[5][c] = -s * dm * a.ik[0] * L2;
+        a.mu[6][c] = s * dm * a.ik[1] * L2;
+        return;
+    }
+    const T m = a.m[cm];
     const T msh[3] = {pget(a, 0, 1, i), pget(a, 1, 1, j), pget(a, 2, 1, k)};
     const T ik[3] = {pget(a, 0, 7, i), pget(a, 1, 7, j), pget(a, 2, 7, k)};
     T da[3], db[3];
@@ -186,6 +205,30 @@ __global__ void adj_e_own_kernel(AdjArgs<T> a) {
     const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
     const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
     const T m = a.m[cm];
+    if (in_box(a.ibox, i, j, k)) {
+        // ca = 1, cb = m, every update in range, no psi: the mu and gradient
+        // term of the general path below (h = 0: dca = 0, dcb/cb = -1/sigma),
+        // lambda_E unchanged
+        const T L0 = a.lam[0][c], L1 = a.lam[1][c], L2 = a.lam[2][c];
+        const T s = a.sgn;
+        a.mu[0][c] = s * m * a.ik[1] * L0;
+        a.mu[1][c] = -s * m * a.ik[2] * L0;
+        a.mu[2][c] = s * m * a.ik[2] * L1;
+        a.mu[3][c] = -s * m * a.ik[0] * L1;
+        a.mu[4][c] = s * m * a.ik[0] * L2;
+        a.mu[5][c] = -s * m * a.ik[1] * L2;
+        const double isig = (double)m * a.inv2w0dt;
+        const double rcb = -isig / (1.0 + 0.0);
+        const T L[3] = {L0, L1, L2};
+        double gsum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const double e0 = (double)a.E0[q][c], e1 = (double)a.E1[q][c];
+            gsum += (double)L[q] * (0.0 * e0 + rcb * (e1 - 1.0 * e0));
+        }
+        a.grad[c] += gsum;
+        return;
+    }
     const T esh[3] = {pget(a, 0, 0, i), pget(a, 1, 0, j), pget(a, 2, 0, k)};
     const T ik[3] = {pget(a, 0, 6, i), pget(a, 1, 6, j), pget(a, 2, 6, k)};
     T ca[3], cb[3];

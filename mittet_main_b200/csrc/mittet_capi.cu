@@ -1234,6 +1234,12 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
             ae.slab[ax] = to_dslab(h->su.se[ax]);
             ah.upd[ax] = to_dbox(h->su.upd[3 + ax]);
             ae.upd[ax] = to_dbox(h->su.upd[ax]);
+            ah.ik[ax] = ae.ik[ax] = (T)(1.0 / (ax == 0 ? h->g.dx : (ax == 1 ? h->g.dy : h->g.dz)));
+            // the forward's interior boxes (empty when the grid has none)
+            ae.ibox.lo[ax] = h->has_ibox[0] ? h->ibox[0][ax] : 0;
+            ae.ibox.hi[ax] = h->has_ibox[0] ? h->ibox[0][3 + ax] : 0;
+            ah.ibox.lo[ax] = h->has_ibox[1] ? h->ibox[1][ax] : 0;
+            ah.ibox.hi[ax] = h->has_ibox[1] ? h->ibox[1][3 + ax] : 0;
             for (int w = 0; w < 2; w++) { ah.lpsi[ax][w] = lph[ax][w].as<T>(); ae.lpsi[ax][w] = lpe[ax][w].as<T>(); }
         }
         ah.sgn = (T)h->ph.h_sign;

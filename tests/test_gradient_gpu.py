@@ -119,7 +119,8 @@ def test_autograd_function_returns_the_gradient():
         sig = torch.tensor(wl.sigma, dtype=torch.float64, requires_grad=True)
         f = fwi_misfit(sig, s, obs, wl.nt, 20)
         f.backward()
-    assert float(f) == J
+    # the misfit is an atomic reduction (equal to rounding); the gradient is deterministic
+    assert float(f.detach()) == pytest.approx(J, rel=1e-13)
     assert np.array_equal(sig.grad.numpy(), G)
 
 
