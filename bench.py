@@ -121,7 +121,7 @@ def e_phase_traffic(wl, esz):
     return float(m.group(1)) * wl.ncell * len(wl.shots) if m else None
 
 
-def run_cpu_baseline(wl, budget_s=20.0):
+def run_cpu_baseline(wl, budget_s=12.0):
     """Oracle (FP64 CPU restatement, all host threads) on a bounded sample of the
     workload: a few time steps of the same grid.  Returns (Gcell/s, sample text, threads)."""
     from oracle import oracle as O
@@ -130,10 +130,18 @@ def run_cpu_baseline(wl, budget_s=20.0):
                  cmax=cp.cmax, omega0=cp.omega0)
     mu = np.full(wl.sigma.shape, cp.mu0)
     src = wl.shots[0].points
-    sec = O.time_oracle_steps(p, wl.sigma, mu, src, wl.wavelet, 1, 4)
+    # size the sample to ~budget_s of CPU work from a 2-step probe (set-up
+    # included, so an upper bound on the step time), then time it as the
+    # difference of a 5-step and a (5+k)-step run so that set-up cancels
+    t0 = time.perf_counter()
+    O.forward(p, wl.sigma, mu, src, wl.wavelet, [], 2)
+    est = (time.perf_counter() - t0) / 2
+    k = int(min(400, max(20, budget_s / max(est, 1e-3))))
+    sec = O.time_oracle_steps(p, wl.sigma, mu, src, wl.wavelet, 5, 5 + k)
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     g = cp.nx * cp.ny * cp.nz / sec / 1e9
-    return g, f"oracle FP64, {cp.nx}x{cp.ny}x{cp.nz} grid, 3 time steps (difference of 1- and 4-step runs)", threads
+    return g, (f"oracle FP64, {cp.nx}x{cp.ny}x{cp.nz} grid, {k} time steps "
+               f"(difference of 5- and {5 + k}-step runs)"), threads
 
 
 def run_reference(args, wl):
