@@ -9,7 +9,8 @@ gradient: FWI gradient of the 128x128x96 model, 16 shots, Ex/Ey at 3
 serving: Poisson arrivals of forward (3) and gradient (1) requests over the
   grid set {64^3, 96^3, 128^3, 160x160x96, 256x256x192} (domain 6.4 km wide),
   1-32 shots, Nt scaled with the grid; p50/p99 latency and shot-solves/s of
-  the server against the serial plain path on the same GPU.
+  the server against two plain paths on the same GPU: one request at a time
+  (its shots batched), and one shot at a time.
 Times are device-synchronised wall clock of the public API calls.
 """
 from __future__ import annotations
@@ -120,6 +121,33 @@ def serving(args):
     for s in cache.values():
         s.close()
     ser = serial_latencies(reqs, service)
+    # plain one-shot-at-a-time path: every shot of a request solved alone, one
+    # after another.  Shots of a request cost the same, so one timed
+    # single-shot solve per (grid, Nt, mode) gives the request's service time.
+    from mittet_main_b200.serving import Request
+    one = {}
+    for r in reqs:
+        wl = r.workload
+        key = (wl.cp.nx, wl.cp.ny, wl.cp.nz, wl.nt, r.mode)
+        if key in one:
+            continue
+        single = Request(-1, 0.0, replace(wl, shots=[wl.shots[0]]), r.mode,
+                         None if r.obs is None else r.obs[:1], r.checkpoint_every)
+        c = {}
+        run_request(c, single)  # warm-up (autotune, graph)
+        _sync()
+        t0 = time.perf_counter()
+        run_request(c, single)
+        _sync()
+        one[key] = time.perf_counter() - t0
+        for sv in c.values():
+            sv.close()
+    service1 = {r.rid: len(r.workload.shots) * one[(r.workload.cp.nx, r.workload.cp.ny, r.workload.cp.nz,
+                                                     r.workload.nt, r.mode)] for r in reqs}
+    ser1 = serial_latencies(reqs, service1)
+    t1 = 0.0
+    for r in sorted(reqs, key=lambda r: r.arrival):
+        t1 = max(t1, r.arrival) + service1[r.rid]
     srv = MittetServer(n_slots=4, hbm_budget=150e9)
     t0 = time.perf_counter()
     res = srv.run(reqs)
@@ -134,4 +162,6 @@ def serving(args):
             "server_p50_s": percentile(lat, 50), "server_p99_s": percentile(lat, 99),
             "server_shot_solves_per_s": shots / wall, "serial_p50_s": percentile(list(ser.values()), 50),
             "serial_p99_s": percentile(list(ser.values()), 99), "serial_shot_solves_per_s": shots / t,
+            "one_shot_p50_s": percentile(list(ser1.values()), 50), "one_shot_p99_s": percentile(list(ser1.values()), 99),
+            "one_shot_shot_solves_per_s": shots / t1, "server_vs_one_shot": (shots / wall) / (shots / t1),
             "max_concurrent": srv.max_concurrent, "peak_budget_bytes": srv.peak_in_use, "errors": errors[:3]}

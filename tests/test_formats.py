@@ -98,3 +98,18 @@ def test_time_domain_files(tmp_path):
     a = np.loadtxt(tmp_path / "GXe_t1010.d")
     assert np.allclose(a[:, 0], [0.0, 1e-3, 2e-3]) and np.allclose(a[:, 1] + 1j * a[:, 2], 3 * z)
     assert np.allclose(np.loadtxt(tmp_path / "absJZ_t1010.d")[:, 1], np.abs(2 * z))
+
+
+def test_probe_positions_and_differences(tmp_path):
+    """source_posi's pattern-2 geometry and diff_probe's two differences."""
+    from mittet_main_b200 import probe
+
+    shot, rec = probe.source_posi(sp=31, y0=20, z_source=15, l_hori=6, l_sr=3)
+    assert [p[:4] for p in shot.points] == [(31, 20, 15, "hz"), (37, 20, 15, "hz")]
+    assert rec == [(31, 20, 18, "hz"), (31, 20, 12, "hz"), (37, 20, 12, "hz")]
+    tr = np.array([[1.0, 2.0, 3.0], [0.5, 1.0, 4.0], [0.25, 3.0, 1.0]])
+    d12, d23 = probe.diff_probe(tr)
+    assert np.array_equal(d12, [0.5, 1.0, -1.0]) and np.array_equal(d23, [0.25, -2.0, 3.0])
+    probe.write_diff_probe(str(tmp_path), "31", 1e-3, tr)
+    a = np.loadtxt(tmp_path / "31pattern2_23diff.d")
+    assert np.allclose(a[:, 0], [1e-3, 2e-3, 3e-3]) and np.array_equal(a[:, 1], d23)

@@ -195,6 +195,10 @@ def test_gradient_agrees_with_satan_formula():
         gb, ecal = born.satan_formula_gradient(wl, obs, current_factor=cf)
         # satan_i's gamma is a descent direction: -dJ/dsigma
         res[cf] = {"all": born.compare(-gb, G), "far": born.compare(-gb * far, G * far)}
+    # secondary figure: satan_i's gamma with its /sense normalisation (a
+    # different weighting of the cells, so only its similarity is reported)
+    gn, _ = born.satan_formula_gradient(wl, obs, normalize=True)
+    res["sense_normalised"] = born.compare(-gn, G)
     print("satan-formula vs discrete adjoint:", res, "receivers", len(rec), "|G|", float(np.abs(G).max()))
     # measured on a B200: cosine 0.99999994, least-squares scale 1.0065,
     # scaled rel-L2 3.6e-4; without the current factor the cosine is 0.998

@@ -269,3 +269,19 @@ def test_residual_reinjection_matches_oracle(tmp_path):
         _, td = s.forward(wl.nt, want_traces=True)
     assert np.abs(res).max() > 0
     assert rel_l2(td[0], ref[0]) <= 1e-10
+
+
+def test_differential_probe_matches_oracle():
+    """source_posi's two Hz coils and pattern-2 receivers; the probe
+    differences of the GPU traces equal those of the oracle's."""
+    from mittet_main_b200 import probe
+
+    wl = W.small_case(nt=150, precision=FP64, magnetic=True)
+    shot, rec = probe.source_posi(sp=14, y0=wl.cp.ny // 2, z_source=wl.cp.nz // 2, l_hori=6, l_sr=3)
+    wl2 = replace(wl, shots=[shot], receivers=rec)
+    ref = oracle_run(wl2)[0]
+    with W.make_solver(wl2) as s:
+        _, td = s.forward(wl.nt, want_traces=True)
+    assert rel_l2(td[0], ref) <= 1e-10
+    for got, want in zip(probe.diff_probe(td[0]), probe.diff_probe(ref)):
+        assert rel_l2(got, want) <= 1e-9
