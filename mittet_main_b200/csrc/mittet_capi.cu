@@ -587,8 +587,12 @@ int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a)
     }
     cudaEventRecord(h->ev_fork, h->st);
     for (int p = 1; p < kParts; p++) cudaStreamWaitEvent(h->pst[p], h->ev_fork, 0);
-    n += launch_part<T>(h, e, 0, vi[0], a, h->st);
+    // the small, latency-bound faces and edges are submitted before the
+    // interior, whose many CTAs would otherwise occupy every SM first
+    const bool faces_first = !std::getenv("MITTET_INTERIOR_FIRST");
+    if (!faces_first) n += launch_part<T>(h, e, 0, vi[0], a, h->st);
     for (int p = 1; p < kParts; p++) n += launch_part<T>(h, e, p, vi[p], a, h->pst[p]);
+    if (faces_first) n += launch_part<T>(h, e, 0, vi[0], a, h->st);
     for (int p = 1; p < kParts; p++) {
         cudaEventRecord(h->ev_join[p], h->pst[p]);
         cudaStreamWaitEvent(h->st, h->ev_join[p], 0);
