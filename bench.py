@@ -278,8 +278,13 @@ def main():
     # end to end through the public C ABI with host buffers
     e2e = None
     if not args.no_e2e:
-        import ctypes
-        sig_host = np.ascontiguousarray(wl.sigma, dtype=np.float64)
+        # inputs and outputs in pinned host memory, allocated before the timed region
+        sig_pinned = torch.from_numpy(np.ascontiguousarray(wl.sigma, dtype=np.float64)).pin_memory()
+        sig_host = sig_pinned.numpy()
+        vol_out = None
+        if wl.volume_dft:
+            vol_out = torch.empty((wl.omega.size, wl.cp.nz, wl.cp.ny, wl.cp.nx), dtype=torch.complex128,
+                                  pin_memory=True).numpy()
         h2d = sig_host.nbytes
         d2h = len(wl.shots) * nrec * nf * 16
         if wl.volume_dft:
@@ -294,7 +299,7 @@ def main():
             if wl.volume_dft:
                 for s in range(len(wl.shots)):
                     for c in wl.volume_dft:
-                        solver.volume_dft(s, "e" + c)
+                        solver.volume_dft(s, "e" + c, out=vol_out)
         torch.cuda.synchronize()
         te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=f"cuda:{dev}")
         if dist:

@@ -215,11 +215,18 @@ class MittetSolver:
         check(self._lib.mittet_forward_device(self._h, nt, ptr, st))
         return out
 
-    def volume_dft(self, shot: int, comp: str) -> np.ndarray:
-        """[nf, nz, ny, nx] complex spectra of one E component."""
-        out = np.zeros((self.nf, self.cp.nz, self.cp.ny, self.cp.nx, 2), dtype=np.float64)
-        check(self._lib.mittet_get_volume_dft(self._h, shot, "xyz".index(comp[-1]), _dptr(out)))
-        return out[..., 0] + 1j * out[..., 1]
+    def volume_dft(self, shot: int, comp: str, out: np.ndarray | None = None) -> np.ndarray:
+        """[nf, nz, ny, nx] complex spectra of one E component.  ``out``: an
+        optional C-contiguous complex128 array of that shape (for example a
+        view of pinned host memory), filled in place and returned."""
+        shape = (self.nf, self.cp.nz, self.cp.ny, self.cp.nx)
+        if out is None:
+            out = np.empty(shape, dtype=np.complex128)
+        elif out.shape != shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous complex128 array of shape {shape}")
+        check(self._lib.mittet_get_volume_dft(self._h, shot, "xyz".index(comp[-1]),
+                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
 
     def fields(self, shot: int = 0) -> np.ndarray:
         out = np.zeros((6, self.cp.nz, self.cp.ny, self.cp.nx), dtype=np.float64)
