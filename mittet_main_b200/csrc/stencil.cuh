@@ -95,14 +95,16 @@ __device__ __forceinline__ void zerov(T (&d)[VX]) {
 }
 
 // psi values o .. o+VX-1 of the lanes in mask: one vector access when every
-// lane is active, else one scalar access per active lane.
+// lane is active, else one scalar access per active lane.  A cell's psi is
+// read once, before its owner thread writes it, and by no other thread, so
+// the read-only path is valid.
 template <typename T, int VX>
 __device__ __forceinline__ void ld_psi(T (&d)[VX], const T *__restrict__ p, int o, unsigned mask) {
     if (mask == (1u << VX) - 1u) {
-        ldv_rw<T, VX>(d, p + o);
+        ldv<T, VX>(d, p + o);
     } else {
 #pragma unroll
-        for (int v = 0; v < VX; v++) d[v] = (mask >> v & 1) ? p[o + v] : T(0);
+        for (int v = 0; v < VX; v++) d[v] = (mask >> v & 1) ? __ldg(p + o + v) : T(0);
     }
 }
 template <typename T, int VX>
@@ -297,9 +299,12 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         }
         T m[VX], ex[VX], ey[VX], ez[VX];
         ldv<T, VX>(m, M + c);
-        ldv_rw<T, VX>(ex, Ex + c);
-        ldv_rw<T, VX>(ey, Ey + c);
-        ldv_rw<T, VX>(ez, Ez + c);
+        // own cells: read once, before this thread writes them, and read by no
+        // other thread in this phase, so the read-only path is valid and lets
+        // the next plane's loads move above this plane's stores
+        ldv<T, VX>(ex, Ex + c);
+        ldv<T, VX>(ey, Ey + c);
+        ldv<T, VX>(ez, Ez + c);
         T esh_z, ik_z;
         bool vz, kx, ky, kz;
         int lz;
@@ -332,8 +337,8 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         if constexpr (GX) {
 #pragma unroll
             for (int v = 0; v < VX; v++) {
-                qx0[v] = (mx >> v & 1) ? sx0[ox + lx[v]] : T(0);
-                qx1[v] = (mx >> v & 1) ? sx1[ox + lx[v]] : T(0);
+                qx0[v] = (mx >> v & 1) ? __ldg(sx0 + ox + lx[v]) : T(0);
+                qx1[v] = (mx >> v & 1) ? __ldg(sx1 + ox + lx[v]) : T(0);
             }
         }
         if constexpr (GY) {
@@ -571,9 +576,10 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
 #pragma unroll
             for (int v = 0; v < VX; v++) dm[v] = a.dtmu0;
         }
-        ldv_rw<T, VX>(hx, Hx + c);
-        ldv_rw<T, VX>(hy, Hy + c);
-        ldv_rw<T, VX>(hz, Hz + c);
+        // own cells: read once before being written, by this thread only
+        ldv<T, VX>(hx, Hx + c);
+        ldv<T, VX>(hy, Hy + c);
+        ldv<T, VX>(hz, Hz + c);
         T msh_z, ik_z;
         bool vz, kx, ky, kz;
         int lz;
@@ -606,8 +612,8 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         if constexpr (GX) {
 #pragma unroll
             for (int v = 0; v < VX; v++) {
-                qx0[v] = (mx >> v & 1) ? sx0[ox + lx[v]] : T(0);
-                qx1[v] = (mx >> v & 1) ? sx1[ox + lx[v]] : T(0);
+                qx0[v] = (mx >> v & 1) ? __ldg(sx0 + ox + lx[v]) : T(0);
+                qx1[v] = (mx >> v & 1) ? __ldg(sx1 + ox + lx[v]) : T(0);
             }
         }
         if constexpr (GY) {
