@@ -221,13 +221,22 @@ int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms);
 
 /* Stencil variant the autotuner chose for the interior launch of the E and
  * H phases at the last forward: {VX, BX, BY, ZC} = x cells per thread,
- * thread block in x and y, z planes each thread marches through. */
+ * thread block in x and y, z planes each thread marches through (ZC < 0:
+ * single-plane body, see mittet_tuned_variants). */
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
 
 /* All chosen variants: cfg[40] = [phase E, H][launch interior, x faces,
  * y faces, z faces, edges][VX, BX, BY, ZC].  VX = 0 marks the TMA-staged
- * interior kernel, whose BX x BY is then its tile in cells. */
+ * interior kernel, whose BX x BY is then its tile in cells.  ZC < 0 marks a
+ * single-plane body: a BX x BY x (-ZC) thread block, one z plane per thread. */
 int mittet_tuned_variants(mittet_handle *h, int32_t *cfg);
+
+/* The stencil variants the autotuner chooses from for FP32 (fp64 = 0) or
+ * FP64 fields: *count receives their number, cfg[4 v .. 4 v + 3] the first
+ * min(count, max) as {VX, BX, BY, ZC} (ZC < 0: single-plane body, as above).
+ * Variant v is the one the environment variable MITTET_VARIANT=v forces on
+ * every launch.  No counterpart in the reference (a tuning introspection). */
+int mittet_stencil_variants(int32_t fp64, int32_t *count, int32_t *cfg, int32_t max);
 
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);

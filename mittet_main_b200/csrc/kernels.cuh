@@ -56,16 +56,27 @@ struct PhaseArgs {
     T *ring;
     int ring_k;             // ring depth K (0 = no ring)
     int vmask;              // E components written to the ring
-    long long ring_comp;    // elements per (slot, vcomp) = nshot * fshot
+    long long ring_comp;    // elements per (slot, vcomp): ring_comp_of(nshot * fshot)
     const int *d_step;
 };
 
-// Ring layout [vcomp][tile of 32 cells][slot][32]: a warp's 32 consecutive
-// cells of one step form one 128-byte line (E-phase writes), and the ring_k
-// steps of those cells are one contiguous 4 KB block (flush reads).
-// e = shot * fshot + cell (padded layout); ring_comp = nshot * fshot.
+// Ring layout [vcomp][tile of kRingTile cells][slot][kRingTile]: one step's
+// values of a tile are kRingTile * 4 contiguous bytes (E-phase writes), and
+// the ring_k steps of a tile are one contiguous block (flush reads).  Tiles
+// shorter than about 256 cells cost the E phase DRAM write efficiency (the
+// per-step pieces land ring_k * tile apart).  e = shot * fshot + cell
+// (padded layout); ring_comp = nshot * fshot rounded up to whole tiles.
+#ifndef MITTET_RING_TILE
+#define MITTET_RING_TILE 256
+#endif
+constexpr int kRingTile = MITTET_RING_TILE;
+static_assert(kRingTile >= 32 && (kRingTile & (kRingTile - 1)) == 0, "ring tile: a power of two, >= 32 cells");
+__host__ __device__ __forceinline__ long long ring_comp_of(long long cells) {
+    return (cells + kRingTile - 1) / kRingTile * kRingTile;
+}
 __device__ __forceinline__ long long ring_index(long long ring_comp, int K, int vc, long long e, int slot) {
-    return (long long)vc * ring_comp * K + (e & ~31LL) * K + (long long)slot * 32 + (e & 31);
+    return (long long)vc * ring_comp * K + (e & ~(long long)(kRingTile - 1)) * K + (long long)slot * kRingTile +
+           (e & (kRingTile - 1));
 }
 
 __device__ __forceinline__ bool in_box(const DBox &b, int i, int j, int k) {
@@ -261,7 +272,7 @@ __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ r
     const T *__restrict__ rp = ring + ring_index(ring_comp, ring_k, vc, e, 0);
     T xs[kFlushRing];
 #pragma unroll
-    for (int s = 0; s < kFlushRing; s++) xs[s] = s < cnt ? __ldg(rp + s * 32) : T(0);
+    for (int s = 0; s < kFlushRing; s++) xs[s] = s < cnt ? __ldcs(rp + s * kRingTile) : T(0);
     T pr[kFlushFreqs], pi[kFlushFreqs];
 #pragma unroll
     for (int f = 0; f < kFlushFreqs; f++) { pr[f] = T(0); pi[f] = T(0); }

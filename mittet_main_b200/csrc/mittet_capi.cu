@@ -241,24 +241,26 @@ PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
         a.ring = h->ring.as<T>();
         a.ring_k = h->ring_k;
         a.vmask = (int)h->vmask;
-        a.ring_comp = (long long)h->nshot * h->fshot;
+        a.ring_comp = ring_comp_of((long long)h->nshot * h->fshot);
     }
     return a;
 }
 
-// Stencil variants (VX x cells per thread, BX x BY threads, ZC z planes per thread)
-// the autotuner picks from; k[phase][part] are the kernels of the five bodies.
+// Stencil variants (VX x cells per thread, BX x BY threads, ZC z planes per
+// tile, BZ threads along z: 0 = each thread marches ZC planes) the autotuner
+// picks from; k[phase][part] are the kernels of the five bodies.
 template <typename T>
 using PartKernel = void (*)(PhaseArgs<T>, const TileMap *, int, int, int);
 template <typename T>
 struct Variant {
-    int vx, bx, by, zc;
+    int vx, bx, by, zc, bz;
     PartKernel<T> k[2][kParts];
 };
 
-#define MITTET_PARTS(PH, T, vx, bx, by)                                                                      \
-    {PH##_part_kernel<T, vx, bx, by, 0>, PH##_part_kernel<T, vx, bx, by, 1>, PH##_part_kernel<T, vx, bx, by, 2>, \
-     PH##_part_kernel<T, vx, bx, by, 4>, PH##_part_kernel<T, vx, bx, by, 7>}
+#define MITTET_PARTS(PH, T, vx, bx, by, bz)                                                            \
+    {PH##_part_kernel<T, vx, bx, by, 0, bz>, PH##_part_kernel<T, vx, bx, by, 1, bz>,                   \
+     PH##_part_kernel<T, vx, bx, by, 2, bz>, PH##_part_kernel<T, vx, bx, by, 4, bz>,                   \
+     PH##_part_kernel<T, vx, bx, by, 7, bz>}
 
 template <typename T>
 const std::vector<Variant<T>> &variants();
@@ -266,8 +268,8 @@ const std::vector<Variant<T>> &variants();
 template <>
 const std::vector<Variant<float>> &variants<float>() {
     static const std::vector<Variant<float>> v = {
-#define MITTET_X(vx, bx, by, zc) \
-    {vx, bx, by, zc, {MITTET_PARTS(e, float, vx, bx, by), MITTET_PARTS(h, float, vx, bx, by)}},
+#define MITTET_X(vx, bx, by, zc, bz) \
+    {vx, bx, by, zc, bz, {MITTET_PARTS(e, float, vx, bx, by, bz), MITTET_PARTS(h, float, vx, bx, by, bz)}},
         MITTET_STENCIL_VARIANTS_F32(MITTET_X)
 #undef MITTET_X
     };
@@ -276,8 +278,8 @@ const std::vector<Variant<float>> &variants<float>() {
 template <>
 const std::vector<Variant<double>> &variants<double>() {
     static const std::vector<Variant<double>> v = {
-#define MITTET_X(vx, bx, by, zc) \
-    {vx, bx, by, zc, {MITTET_PARTS(e, double, vx, bx, by), MITTET_PARTS(h, double, vx, bx, by)}},
+#define MITTET_X(vx, bx, by, zc, bz) \
+    {vx, bx, by, zc, bz, {MITTET_PARTS(e, double, vx, bx, by, bz), MITTET_PARTS(h, double, vx, bx, by, bz)}},
         MITTET_STENCIL_VARIANTS_F64(MITTET_X)
 #undef MITTET_X
     };
@@ -556,7 +558,7 @@ int launch_part(mittet_handle *h, bool e, int part, int vi, const PhaseArgs<T> &
     const int first = h->ptile[slot][part], last = h->ptile[slot][part + 1];
     if (last <= first) return 0;
     const TileMap &th = h->tmaps_host[slot];
-    dim3 block(v.bx, v.by), grid(last - first, h->nshot);
+    dim3 block(v.bx, v.by, v.bz > 0 ? v.bz : 1), grid(last - first, h->nshot);
     v.k[e ? 0 : 1][part]<<<grid, block, 0, st>>>(a, tm, first, th.pbox[part], th.pbox[part + 1]);
     return 1;
 }
@@ -630,6 +632,19 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     const char *tcfg = std::getenv("MITTET_TMA_CFG");
     const int pin_tma = (only_tma && tcfg) ? std::atoi(tcfg) : -1;
     const bool pinned = pin_tma >= 0 && pin_tma < (int)tma_cfgs<T>().size();
+    // MITTET_VARIANT=<v> forces variant v on every part (neither cached nor
+    // looked up), e.g. to check that every body gives the same result.
+    const char *fix = std::getenv("MITTET_VARIANT");
+    const int nv = (int)variants<T>().size();
+    if (fix) {
+        const int v = std::atoi(fix);
+        if (v >= 0 && v < nv) {
+            for (int p = 0; p < kParts; p++) h->var_e[p] = h->var_h[p] = v;
+            h->ldg_int[0] = h->ldg_int[1] = v;
+            if (only_tma) h->var_e[0] = h->var_h[0] = -1;
+            return MITTET_OK;
+        }
+    }
     const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0,
                                      (try_tma ? 1 : 0) + (only_tma ? 2 : 0) + (pinned ? 4 * (pin_tma + 1) : 0));
     {
@@ -681,17 +696,6 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             fclose(f);
         }
     }
-    const char *fix = std::getenv("MITTET_VARIANT");
-    const int nv = (int)variants<T>().size();
-    if (fix) {
-        const int v = std::atoi(fix);
-        if (v >= 0 && v < nv) {
-            for (int p = 0; p < kParts; p++) h->var_e[p] = h->var_h[p] = v;
-            h->ldg_int[0] = h->ldg_int[1] = v;
-            if (only_tma) h->var_e[0] = h->var_h[0] = -1;
-            return MITTET_OK;
-        }
-    }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -721,9 +725,9 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
                         fprintf(stderr, "autotune %s %s tma %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", pname[part],
                                 TmaShape<T>::TX, TmaShape<T>::TY, tma_cfgs<T>()[-1 - v].zc, ms / reps);
                     else
-                        fprintf(stderr, "autotune %s %s vx%d %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", pname[part],
+                        fprintf(stderr, "autotune %s %s vx%d %dx%dx%d%s: %.4f ms\n", ph == 0 ? "E" : "H", pname[part],
                                 variants<T>()[v].vx, variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].zc,
-                                ms / reps);
+                                variants<T>()[v].bz > 0 ? " one-plane" : "", ms / reps);
                 }
                 const bool eligible = !(only_tma && part == 0 && v >= 0) && !(pinned && part == 0 && v != -1 - pin_tma);
                 if (eligible && ms < best) {
@@ -777,7 +781,7 @@ void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
                 w.wr[s][f] = (T)h->wt_host[q];
                 w.wi[s][f] = (T)h->wt_host[q + 1];
             }
-        volume_dft_kernel<T><<<grid, 256, 0, h->st>>>(h->ring.as<T>(), (long long)h->nshot * h->fshot, h->ring_k,
+        volume_dft_kernel<T><<<grid, 256, 0, h->st>>>(h->ring.as<T>(), ring_comp_of((long long)h->nshot * h->fshot), h->ring_k,
                                                       make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, f0, nf, w,
                                                       h->acc.as<double2>());
         h->launches++;
@@ -800,7 +804,7 @@ int run_forward(mittet_handle *h, int nt) {
     const int nf = (int)h->omega.size();
     const bool vol = h->vmask && nf > 0;
     if (vol) {
-        const size_t ring_b = (size_t)h->ring_k * 3 * ns * h->fshot * h->esz;
+        const size_t ring_b = (size_t)h->ring_k * 3 * ring_comp_of((long long)ns * h->fshot) * h->esz;
         CK(h->ring.ensure(ring_b));
         const size_t acc_b = (size_t)ns * 3 * nf * h->fshot * sizeof(double2);
         CK(h->acc.ensure(acc_b));
@@ -831,7 +835,7 @@ int run_forward(mittet_handle *h, int nt) {
         ia.ring = h->ring.as<T>();
         ia.ring_k = h->ring_k;
         ia.vmask = (int)h->vmask;
-        ia.ring_comp = (long long)ns * h->fshot;
+        ia.ring_comp = ring_comp_of((long long)ns * h->fshot);
     }
     InjectArgs<T> ia_m = ia, ia_e = ia;
     ia_m.kind = 0;
@@ -933,7 +937,7 @@ int time_kernels(mittet_handle *h, int nsteps, double *ms) {
         ia.ring = h->ring.as<T>();
         ia.ring_k = h->ring_k;
         ia.vmask = (int)h->vmask;
-        ia.ring_comp = (long long)h->nshot * h->fshot;
+        ia.ring_comp = ring_comp_of((long long)h->nshot * h->fshot);
     }
     InjectArgs<T> ia_m = ia, ia_e = ia;
     ia_m.kind = 0;
@@ -1817,12 +1821,26 @@ int mittet_tuned_variants(mittet_handle *h, int32_t *cfg) {
                     c[0] = 0; c[1] = TmaShape<T>::TX; c[2] = TmaShape<T>::TY; c[3] = tma_cfgs<T>()[-1 - vi].zc;
                 } else {
                     const auto &a = variants<T>()[vi];
-                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.zc;
+                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.bz > 0 ? -a.bz : a.zc;
                 }
             }
     };
     if (h->fp64) fill(double());
     else fill(float());
+    return MITTET_OK;
+}
+
+int mittet_stencil_variants(int32_t fp64, int32_t *count, int32_t *cfg, int32_t max) {
+    if (!count || (max > 0 && !cfg)) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    auto fill = [&](const auto &vs) {
+        *count = (int32_t)vs.size();
+        for (int v = 0; v < (int)vs.size() && v < max; v++) {
+            int32_t *c = cfg + 4 * v;
+            c[0] = vs[v].vx; c[1] = vs[v].bx; c[2] = vs[v].by; c[3] = vs[v].bz > 0 ? -vs[v].bz : vs[v].zc;
+        }
+    };
+    if (fp64) fill(variants<double>());
+    else fill(variants<float>());
     return MITTET_OK;
 }
 

@@ -88,6 +88,18 @@ __device__ __forceinline__ void stv(T *__restrict__ p, const T (&src)[VX]) {
     for (int q = 0; q < VX; q++) d[q] = src[q];
     *reinterpret_cast<V *>(p) = v;
 }
+// Streaming store (evict-first in L2) for the DFT ring: nothing reads it
+// before the flush, ring_k steps later, so its lines should not push the
+// fields' halo rows out of L2.
+template <typename T, int VX>
+__device__ __forceinline__ void stv_stream(T *__restrict__ p, const T (&src)[VX]) {
+    using V = typename VecT<T, VX>::type;
+    V v;
+    T *d = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int q = 0; q < VX; q++) d[q] = src[q];
+    __stcs(reinterpret_cast<V *>(p), v);
+}
 template <typename T, int VX>
 __device__ __forceinline__ void zerov(T (&d)[VX]) {
 #pragma unroll
@@ -140,13 +152,21 @@ __device__ __forceinline__ T leap(T ca, T sgcb, T x, T e) {  // ca e + (s cb) x
     return fma(sgcb, x, ca * e);
 }
 
-#define MITTET_MINB(T, VX, NT) ((sizeof(T) == 4 && VX == 2) ? 768 / (NT) : 512 / (NT))
-// Face and edge bodies carry psi and profile state: the wide ones get up to
-// 168 registers (3 x 128 threads per SM) instead of spilling.
-#define MITTET_MINB_GEN(T, VX, NT) ((sizeof(T) == 4 && VX == 2) ? 512 / (NT) : 384 / (NT))
+// Minimum resident blocks per SM (__launch_bounds__) of a body, NT threads:
+// marching interior bodies get up to 80 (VX = 2 FP32) or 128 registers; the
+// marching face and edge bodies carry psi and profile state and get up to
+// 128 or 168 (3 x 128 threads per SM) instead of spilling; the single-plane
+// bodies hold no window, so the interior fits 64 or 80 registers and the
+// general ones 80 or 128.
+template <typename T, int VX, int NT, int GM, int BZ>
+constexpr int part_min_blocks() {
+    const bool narrow = sizeof(T) == 4 && VX == 2;
+    if (BZ > 0) return GM == 0 ? (narrow ? 1024 : 768) / NT : (narrow ? 768 : 512) / NT;
+    return GM == 0 ? (narrow ? 768 : 512) / NT : (narrow ? 512 : 384) / NT;
+}
 
 // ------------------------------------------------------------------ E phase
-template <typename T, int VX, int GM>
+template <typename T, int VX, int GM, bool ONE>
 __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
     const long long sb = (long long)shot * a.fshot;
     T *__restrict__ Ex = a.f[0] + sb;
@@ -243,8 +263,11 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
     }
     const int slot = a.ring_k > 0 ? (*a.d_step) % a.ring_k : 0;
 
+    // ONE: this thread owns the single plane kb (a compile-time trip count
+    // of one, so the window is three loads and a fourth, not a rotation)
+    const int kend = ONE ? kb + 1 : ke;
 #pragma unroll 2
-    for (int k = kb; k < ke; k++) {
+    for (int k = kb; k < kend; k++) {
         {
             const int kk = k + 1;
             if (!GZ || kk < nz) {
@@ -404,9 +427,9 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         stv<T, VX>(Ez + c, ez);
         if (a.ring_k > 0) {
             const long long e = sb + c;
-            if (a.vmask & 1) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
-            if (a.vmask & 2) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
-            if (a.vmask & 4) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
+            if (a.vmask & 1) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
+            if (a.vmask & 2) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
+            if (a.vmask & 4) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
         }
 #pragma unroll
         for (int v = 0; v < VX; v++) {
@@ -417,7 +440,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
 }
 
 // ------------------------------------------------------------------ H phase
-template <typename T, int VX, int GM>
+template <typename T, int VX, int GM, bool ONE>
 __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
     const long long sb = (long long)shot * a.fshot;
     const T *__restrict__ Ex = a.f[0] + sb;
@@ -514,8 +537,11 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         }
     }
 
+    // ONE: this thread owns the single plane kb (a compile-time trip count
+    // of one, so the window is three loads and a fourth, not a rotation)
+    const int kend = ONE ? kb + 1 : ke;
 #pragma unroll 2
-    for (int k = kb; k < ke; k++) {
+    for (int k = kb; k < kend; k++) {
         {
             const int kk = k + 2;
             if (!GZ || kk < nz) {
@@ -709,50 +735,71 @@ __device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int q0, i
 
 // One kernel per body: GM = 0 interior, 1/2/4 the x/y/z faces, 7 edges and
 // corners.  Tiles [first_tile, first_tile + gridDim.x) of boxes [q0, q1).
+// BZ = 0: a BX x BY block, each thread marching the tile's ZC planes.
+// BZ > 0: a BX x BY x BZ block over a tile of BZ planes, one plane per
+// thread; the body then holds no rolling window and needs far fewer
+// registers, so more warps per SM keep loads in flight.
 #define MITTET_PHASE_KERNEL(PH)                                                                              \
-    template <typename T, int VX, int BX, int BY, int GM>                                                    \
-    __global__ void __launch_bounds__(BX *BY, GM == 0 ? MITTET_MINB(T, VX, BX *BY)                           \
-                                                      : MITTET_MINB_GEN(T, VX, BX *BY))                      \
+    template <typename T, int VX, int BX, int BY, int GM, int BZ = 0>                                        \
+    __global__ void __launch_bounds__(BX *BY *(BZ > 0 ? BZ : 1),                                             \
+                                      (part_min_blocks<T, VX, BX * BY * (BZ > 0 ? BZ : 1), GM, BZ>()))       \
         PH##_part_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile, int q0, int q1) { \
         int i0, j, kb, ke;                                                                                   \
         bool inside;                                                                                         \
         locate<VX, BX, BY>(tm, q0, q1, first_tile + blockIdx.x, i0, j, kb, ke, inside);                      \
-        if (inside) PH##_cells<T, VX, GM>(a, blockIdx.y, i0, j, kb, ke);                                     \
+        if constexpr (BZ > 0) {                                                                              \
+            kb += (int)threadIdx.z;                                                                          \
+            inside = inside && kb < ke;                                                                      \
+        }                                                                                                    \
+        if (inside) PH##_cells<T, VX, GM, (BZ > 0)>(a, blockIdx.y, i0, j, kb, ke);                           \
     }
 
 // e_part_kernel and h_part_kernel.
 MITTET_PHASE_KERNEL(e)
 MITTET_PHASE_KERNEL(h)
 
-// Variants the autotuner chooses from: (VX, BX, BY, ZC) = x cells per
-// thread, thread block, z planes each thread marches through.  ZC is a
-// run-time tile parameter (the same kernel serves every ZC): short chunks give
-// small boxes enough CTAs, long ones amortise the window preload.  The
-// narrow blocks (x tile of 8 or 16 cells) suit the thin x faces.
+// Variants the autotuner chooses from: (VX, BX, BY, ZC, BZ) = x cells per
+// thread, thread block in x and y, z planes per tile, threads along z.
+// BZ = 0: each thread marches the tile's ZC planes; ZC is a run-time tile
+// parameter (the same kernel serves every ZC): short chunks give small boxes
+// enough CTAs, long ones amortise the window preload.  BZ > 0 (ZC = BZ): one
+// plane per thread.  The narrow blocks (x tile of 8 or 16 cells) suit the
+// thin x faces.
 #define MITTET_STENCIL_VARIANTS_F32(X) \
-    X(2, 32, 4, 2)                     \
-    X(2, 32, 4, 4)                     \
-    X(2, 32, 4, 8)                     \
-    X(2, 32, 4, 16)                    \
-    X(2, 16, 8, 2)                     \
-    X(2, 16, 8, 4)                     \
-    X(2, 16, 8, 8)                     \
-    X(4, 16, 8, 2)                     \
-    X(4, 16, 8, 4)                     \
-    X(4, 16, 8, 8)                     \
-    X(4, 8, 16, 4)                     \
-    X(4, 16, 4, 4)                     \
-    X(2, 8, 16, 4)                     \
-    X(2, 8, 16, 8)                     \
-    X(2, 4, 32, 4)
+    X(2, 32, 4, 2, 0)                     \
+    X(2, 32, 4, 4, 0)                     \
+    X(2, 32, 4, 8, 0)                     \
+    X(2, 32, 4, 16, 0)                    \
+    X(2, 16, 8, 2, 0)                     \
+    X(2, 16, 8, 4, 0)                     \
+    X(2, 16, 8, 8, 0)                     \
+    X(4, 16, 8, 2, 0)                     \
+    X(4, 16, 8, 4, 0)                     \
+    X(4, 16, 8, 8, 0)                     \
+    X(4, 8, 16, 4, 0)                     \
+    X(4, 16, 4, 4, 0)                     \
+    X(2, 8, 16, 4, 0)                     \
+    X(2, 8, 16, 8, 0)                     \
+    X(2, 4, 32, 4, 0)                     \
+    X(4, 16, 4, 4, 4)                     \
+    X(4, 16, 8, 2, 2)                     \
+    X(4, 8, 8, 4, 4)                      \
+    X(2, 32, 4, 2, 2)                     \
+    X(2, 16, 4, 4, 4)                     \
+    X(2, 8, 8, 4, 4)                      \
+    X(2, 8, 4, 8, 8)
 #define MITTET_STENCIL_VARIANTS_F64(X) \
-    X(2, 32, 4, 2)                     \
-    X(2, 32, 4, 4)                     \
-    X(2, 32, 4, 8)                     \
-    X(2, 16, 8, 2)                     \
-    X(2, 16, 8, 4)                     \
-    X(2, 16, 8, 8)                     \
-    X(2, 16, 4, 4)                     \
-    X(2, 8, 16, 4)
+    X(2, 32, 4, 2, 0)                     \
+    X(2, 32, 4, 4, 0)                     \
+    X(2, 32, 4, 8, 0)                     \
+    X(2, 16, 8, 2, 0)                     \
+    X(2, 16, 8, 4, 0)                     \
+    X(2, 16, 8, 8, 0)                     \
+    X(2, 16, 4, 4, 0)                     \
+    X(2, 8, 16, 4, 0)                     \
+    X(2, 16, 4, 4, 4)                     \
+    X(2, 32, 4, 2, 2)                     \
+    X(2, 8, 8, 4, 4)                      \
+    X(2, 16, 8, 2, 2)
 
 }  // namespace mittet

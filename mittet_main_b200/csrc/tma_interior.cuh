@@ -273,9 +273,9 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
                 stv<T, VX>(a.f[2] + sb + c, ez);
                 if (a.ring_k > 0) {
                     const long long e = sb + c;
-                    if (a.vmask & 1) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
-                    if (a.vmask & 2) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
-                    if (a.vmask & 4) stv<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
+                    if (a.vmask & 1) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
+                    if (a.vmask & 2) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
+                    if (a.vmask & 4) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
                 }
             }
         } else {

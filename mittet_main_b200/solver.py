@@ -268,7 +268,9 @@ class MittetSolver:
         return dict(zip(["inject_magnetic", "e_phase", "inject_electric", "h_phase", "sample", "volume_dft"], ms.tolist()))
 
     def tuned_variant(self) -> dict:
-        """[VX, BX, BY, ZC] the autotuner chose per phase and launch."""
+        """[VX, BX, BY, ZC] the autotuner chose per phase and launch (VX = 0:
+        the TMA-staged interior; ZC < 0: a single-plane body with -ZC threads
+        along z)."""
         parts = ("interior", "xfaces", "yfaces", "zfaces", "edges")
         c = (ctypes.c_int32 * (2 * len(parts) * 4))()
         check(self._lib.mittet_tuned_variants(self._h, c))
@@ -278,6 +280,18 @@ class MittetSolver:
 
     def launch_count(self) -> int:
         return int(self._lib.mittet_last_launch_count(self._h))
+
+
+def stencil_variants(fp64: bool = False) -> list:
+    """The stencil variants the autotuner chooses from, as [VX, BX, BY, ZC]
+    (ZC < 0: single-plane body); index v is what MITTET_VARIANT=v forces."""
+    lib = capi.load()
+    n = ctypes.c_int32()
+    check(lib.mittet_stencil_variants(1 if fp64 else 0, ctypes.byref(n), None, 0))
+    c = (ctypes.c_int32 * (4 * n.value))()
+    check(lib.mittet_stencil_variants(1 if fp64 else 0, ctypes.byref(n), c, n.value))
+    v = list(c)
+    return [v[4 * i:4 * i + 4] for i in range(n.value)]
 
 
 def f_to_d(traces: np.ndarray, dt: float, omega0: float, omega: np.ndarray, h_factor: bool = False,

@@ -245,6 +245,42 @@ def test_tma_interior_is_bit_identical_to_plain_loads(monkeypatch, prec, flavor,
             assert np.array_equal(fa[c], fb[c]), NAMES[c]
 
 
+@pytest.mark.parametrize("prec,flavor", [(FP32, FLAVOR_NCVER0027), (FP32, FLAVOR_SATAN_I), (FP64, FLAVOR_NCVER0027)])
+def test_every_stencil_variant_is_bit_identical(monkeypatch, prec, flavor):
+    """Every variant the autotuner may choose (marching and single-plane
+    bodies, each tile shape) gives the same fields, traces and volume spectra
+    bit for bit: the bodies share their fma forms and only partition the
+    cells differently.  The grid gives partial tiles in x and y, ragged z
+    chunks, CPML slabs on every face and two shots."""
+    from mittet_main_b200.solver import stencil_variants
+
+    wl = W.small_case(n=(150, 44, 40), ncpml=8, nt=40, precision=prec, flavor=flavor, magnetic=True)
+    nx, ny, nz = wl.cp.nx, wl.cp.ny, wl.cp.nz
+    second = Shot(points=[(nx // 3, ny // 2 + 3, nz // 2 - 4, "ey", SRC_ELECTRIC, 0.7)])
+    wl = replace(wl, volume_dft="xyz", shots=[wl.shots[0], second])
+    vs = stencil_variants(prec == FP64)
+    assert any(c[3] < 0 for c in vs) and any(c[3] > 0 for c in vs), vs
+    monkeypatch.setenv("MITTET_INTERIOR", "ldg")
+    base = None
+    for v, cfg in enumerate(vs):
+        monkeypatch.setenv("MITTET_VARIANT", str(v))
+        with W.make_solver(wl) as s:
+            spec, td = s.forward(wl.nt, want_traces=True)
+            used = s.tuned_variant()
+            vols = [s.volume_dft(k, c) for k in (0, 1) for c in ("ex", "ey", "ez")]
+            fields = [s.fields(k) for k in (0, 1)]
+        assert all(u == cfg for u in used.values()), (v, cfg, used)
+        if base is None:
+            base = (spec, td, vols, fields)
+            continue
+        assert np.array_equal(spec, base[0]) and np.array_equal(td, base[1]), (v, cfg)
+        for va, vb in zip(vols, base[2]):
+            assert np.array_equal(va, vb), (v, cfg)
+        for fa, fb in zip(fields, base[3]):
+            for c in range(6):
+                assert np.array_equal(fa[c], fb[c]), (v, cfg, NAMES[c])
+
+
 def test_residual_reinjection_matches_oracle(tmp_path):
     """read_source_3d_res: the magnetic sources driven by a time-reversed
     residual (difference of two runs), read back from a "t value" file."""
