@@ -427,14 +427,21 @@ __global__ void adj_src_kernel(AdjArgs<T> a, const AdjSrc *__restrict__ pts, int
     }
 }
 
-// Copies the six field arrays of a group of shots into one history slot.
+// Copies the six field arrays of a group of shots into one history slot,
+// 16 bytes per thread and iteration (len is a multiple of 32 elements, every
+// array 16-byte aligned); blockIdx.y is the field.
 template <typename T>
-__global__ void copy_state_kernel(const T *f0, const T *f1, const T *f2, const T *f3, const T *f4, const T *f5,
-                                  T *dst, long long len) {
-    const T *src[6] = {f0, f1, f2, f3, f4, f5};
-    for (int c = 0; c < 6; c++)
-        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x)
-            dst[c * len + e] = src[c][e];
+__global__ void __launch_bounds__(256) copy_state_kernel(const T *f0, const T *f1, const T *f2, const T *f3,
+                                                         const T *f4, const T *f5, T *dst, long long len) {
+    constexpr int VX = 16 / sizeof(T);
+    using V = typename VecT<T, VX>::type;
+    const int c = blockIdx.y;
+    const T *src = c == 0 ? f0 : c == 1 ? f1 : c == 2 ? f2 : c == 3 ? f3 : c == 4 ? f4 : f5;
+    const V *__restrict__ s = reinterpret_cast<const V *>(src);
+    V *__restrict__ d = reinterpret_cast<V *>(dst + c * len);
+    const long long nv = len / VX;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nv; e += (long long)gridDim.x * blockDim.x)
+        d[e] = __ldcs(s + e);
 }
 
 // grad_out[cell] = sum over shots of grad[shot][cell], zero outside the frame

@@ -36,7 +36,8 @@ struct DSlab {
 
 template <typename T>
 struct PhaseArgs {
-    T *f[6];                // Ex Ey Ez Hx Hy Hz, shot 0
+    T *f[6];                // Ex Ey Ez Hx Hy Hz, shot 0: the phase's inputs
+    T *fo[6];               // where the phase writes its own three fields (= f: in place)
     T *psi[3][2];           // psi of this phase's slab groups (axis, which)
     const T *m;             // per-cell 2 w0 dt / sigma
     const T *dtmu;          // per-cell dt/mu or nullptr

@@ -213,7 +213,7 @@ template <typename T>
 PhaseArgs<T> phase_args(mittet_handle *h, bool e_phase) {
     PhaseArgs<T> a;
     memset(&a, 0, sizeof(a));
-    for (int c = 0; c < 6; c++) a.f[c] = h->fields[c].as<T>();
+    for (int c = 0; c < 6; c++) a.f[c] = a.fo[c] = h->fields[c].as<T>();
     for (int ax = 0; ax < 3; ax++)
         for (int w = 0; w < 2; w++) a.psi[ax][w] = (e_phase ? h->psiE : h->psiH)[ax][w].as<T>();
     a.m = h->m.as<T>();
@@ -550,7 +550,8 @@ int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a, cudaStre
 // tensor maps describe).
 template <typename T>
 bool tma_usable(const mittet_handle *h, const PhaseArgs<T> &a) {
-    return h->tma_ok && a.f[0] == h->fields[0].as<T>() && a.m == h->m.as<T>();
+    return h->tma_ok && a.f[0] == h->fields[0].as<T>() && a.fo[0] == a.f[0] && a.f[3] == h->fields[3].as<T>() &&
+           a.fo[3] == a.f[3] && a.m == h->m.as<T>();
 }
 
 // One part of a phase (0 interior, 1 faces, 2 edges and corners) with
@@ -1052,30 +1053,54 @@ int upload_sources(mittet_handle *h) {
 template <typename T>
 int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double *misfit_out, double *grad_out) {
     const int ns = h->nshot, nrec = h->nrec, nf = (int)h->omega.size();
-    const uint32_t vmask_saved = h->vmask;
-    if (h->vmask) { h->vmask = 0; drop_graph(h); }
-    int rc = run_forward<T>(h, nt);
-    h->vmask = vmask_saved;
-    if (vmask_saved) drop_graph(h);
-    if (rc) return rc;
+    // MITTET_GRAD_LOG: device time of each stage (CUDA events on the handle's
+    // stream, synchronised per stage) printed to stderr
+    const bool glog = std::getenv("MITTET_GRAD_LOG") != nullptr;
+    cudaEvent_t gev[2] = {nullptr, nullptr};
+    double gms[3] = {0, 0, 0};  // checkpoint pass, recompute, adjoint
+    if (glog) {
+        CK(cudaEventCreate(&gev[0]));
+        CK(cudaEventCreate(&gev[1]));
+    }
+    auto gmark = [&](int stage) -> int {
+        if (!glog) return MITTET_OK;
+        CK(cudaEventRecord(gev[1], h->st));
+        CK(cudaEventSynchronize(gev[1]));
+        float ms = 0.f;
+        if (stage >= 0) {
+            CK(cudaEventElapsedTime(&ms, gev[0], gev[1]));
+            gms[stage] += ms;
+        }
+        CK(cudaEventRecord(gev[0], h->st));
+        return MITTET_OK;
+    };
+    int rc = MITTET_OK;
+    if (!h->tuned) {
+        // one step of a plain forward tunes the stencil variants on this grid
+        const uint32_t vmask_saved = h->vmask;
+        if (h->vmask) { h->vmask = 0; drop_graph(h); }
+        rc = run_forward<T>(h, 1);
+        h->vmask = vmask_saved;
+        if (vmask_saved) drop_graph(h);
+        if (rc) return rc;
+    }
+    if ((rc = ensure_part_streams(h))) return rc;
+    CK(h->d_step.ensure(sizeof(int)));
+    CK(h->d_flag.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->st));
+    // The checkpoint pass of each shot group samples the receivers, so the
+    // group's residual and adjoint sources follow from it (no separate
+    // forward).
     const size_t nspec = (size_t)ns * nrec * nf;
     DevBuf d_obs, d_R, d_mis, d_asrc;
-    CK(d_obs.ensure(nspec * sizeof(double2)));
-    CK(d_R.ensure(nspec * sizeof(double2)));
+    CK(d_obs.ensure(std::max<size_t>(nspec, 1) * sizeof(double2)));
+    CK(d_R.ensure(std::max<size_t>(nspec, 1) * sizeof(double2)));
     CK(d_mis.ensure(sizeof(double)));
-    CK(d_asrc.ensure((size_t)ns * nrec * nt * sizeof(double)));
+    CK(d_asrc.ensure(std::max<size_t>((size_t)ns * nrec * nt, 1) * sizeof(double)));
+    CK(h->traces.ensure((size_t)ns * std::max(nrec, 1) * nt * h->esz));
+    CK(h->spectra.ensure(std::max<size_t>(nspec, 1) * sizeof(double2)));
     CK(cudaMemcpyAsync(d_obs.p, obs_host, nspec * sizeof(double2), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemsetAsync(d_mis.p, 0, sizeof(double), h->st));
-    residual_kernel<<<64, 256, 0, h->st>>>(h->spectra.as<double2>(), d_obs.as<double2>(), (long long)nspec,
-                                           d_R.as<double2>(), d_mis.as<double>());
-    adj_source_kernel<<<256, 256, 0, h->st>>>(d_R.as<double2>(), ns * nrec, nrec, nf, nt, h->d_omega.as<double>(),
-                                              h->ph.dt, h->ph.omega0, h->rec_is_h.as<unsigned char>(), h->hfac,
-                                              d_asrc.as<double>());
-    CK(cudaGetLastError());
-    double mis = 0.0;
-    CK(cudaMemcpyAsync(&mis, d_mis.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    *misfit_out = mis;
 
     // source points, absolute shots
     const double vol = h->g.dx * h->g.dy * h->g.dz;
@@ -1149,7 +1174,7 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         CK(d_gp.ensure(std::max<size_t>(gp.size(), 1) * sizeof(SrcPoint)));
         CK(cudaMemcpyAsync(d_gp.p, gp.data(), gp.size() * sizeof(SrcPoint), cudaMemcpyHostToDevice, h->st));
         PhaseArgs<T> ea = phase_args<T>(h, true), ha = phase_args<T>(h, false);
-        for (int c = 0; c < 6; c++) { ea.f[c] = fl[c].as<T>(); ha.f[c] = fl[c].as<T>(); }
+        for (int c = 0; c < 6; c++) ea.f[c] = ea.fo[c] = ha.f[c] = ha.fo[c] = fl[c].as<T>();
         for (int a = 0; a < 3; a++)
             for (int w = 0; w < 2; w++) { ea.psi[a][w] = pe[a][w].as<T>(); ha.psi[a][w] = pH[a][w].as<T>(); }
         ea.ring_k = 0;
@@ -1163,15 +1188,21 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         InjectArgs<T> ia_m = ia, ia_e = ia;
         ia_m.kind = 0;
         ia_e.kind = 1;
+        // receivers are sampled in the checkpoint pass only (sa_rec), into
+        // the group's rows of the trace buffer
         SampleArgs<T> sa;
         memset(&sa, 0, sizeof(sa));
         for (int c = 0; c < 6; c++) sa.f[c] = fl[c].as<T>();
         sa.nrec = 0;
         sa.nshot = Gg;
         sa.fshot = h->fshot;
-        sa.traces = h->traces.as<T>();
+        sa.traces = h->traces.as<T>() + (size_t)s0 * nrec * nt;
         sa.nt = nt;
         sa.d_step = h->d_step.as<int>();
+        SampleArgs<T> sa_rec = sa;
+        sa_rec.rec_off = h->rec_off.as<long long>();
+        sa_rec.rec_comp = h->rec_comp.as<int>();
+        sa_rec.nrec = nrec;
         bool hm = false, he = false;
         for (const auto &q : gp) { hm |= q.kind == 0; he |= q.kind == 1; }
         const bool mag0 = h->has_mag, ele0 = h->has_ele;
@@ -1188,9 +1219,14 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
                 }
             return MITTET_OK;
         };
-        auto load_state = [&](const char *src) -> int {
+        // fields to fdst[c] (the working fields when null), psi to the working psi
+        auto load_state = [&](const char *src, T *const *fdst) -> int {
             size_t o = 0;
-            for (int c = 0; c < 6; c++) { CK(cudaMemcpyAsync(fl[c].p, src + o, (size_t)Gg * F * h->esz, cudaMemcpyDeviceToDevice, h->st)); o += (size_t)G * F * h->esz; }
+            for (int c = 0; c < 6; c++) {
+                void *d = fdst ? (void *)fdst[c] : fl[c].p;
+                CK(cudaMemcpyAsync(d, src + o, (size_t)Gg * F * h->esz, cudaMemcpyDeviceToDevice, h->st));
+                o += (size_t)G * F * h->esz;
+            }
             for (int a = 0; a < 3; a++)
                 for (int w = 0; w < 2; w++) {
                     const size_t ne = (size_t)Gg * psi_elems(h, h->su.se[a], a) * h->esz, nh = (size_t)Gg * psi_elems(h, h->su.sh[a], a) * h->esz;
@@ -1204,12 +1240,13 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
             CK(cudaStreamSynchronize(h->st));  // n lives on the host stack
             return MITTET_OK;
         };
-        auto fwd_step = [&]() {
+        auto fwd_step = [&](bool sample) {
             if (h->has_mag) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_m);
             launch_phase<T>(h, true, h->var_e, ea);
             if (h->has_ele) inject_kernel<T><<<1, 128, 0, h->st>>>(ia_e);
             launch_phase<T>(h, false, h->var_h, ha);
-            sample_kernel<T><<<1, 32, 0, h->st>>>(sa);
+            if (sample) sample_kernel<T><<<1, 1024, 0, h->st>>>(sa_rec);
+            else sample_kernel<T><<<1, 32, 0, h->st>>>(sa);
         };
         // forward pass with checkpoints
         for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(fl[c].p, 0, gF * h->esz, h->st));
@@ -1219,11 +1256,33 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
                 CK(cudaMemsetAsync(pH[a][w].p, 0, (size_t)G * psi_elems(h, h->su.sh[a], a) * h->esz, h->st));
             }
         if ((rc = set_step(0))) return rc;
+        if ((rc = gmark(-1))) return rc;
         for (int n = 0; n < nt; n++) {
             if (n % K == 0 && (rc = save_state(ck.as<char>() + (size_t)(n / K) * ck_stride))) return rc;
-            fwd_step();
+            fwd_step(true);
         }
         CK(cudaGetLastError());
+        // receiver spectra, residual, misfit and adjoint sources of the group
+        if (nrec > 0 && nf > 0) {
+            const size_t g0 = (size_t)s0 * nrec;
+            finite_check_kernel<T><<<64, 256, 0, h->st>>>(sa_rec.traces, (long long)Gg * nrec * nt,
+                                                          h->d_flag.as<int>());
+            trace_dft_kernel<T><<<nf, 256, 0, h->st>>>(sa_rec.traces, Gg * nrec, nt, h->d_omega.as<double>(), nf,
+                                                       h->ph.dt, h->ph.omega0, h->rec_is_h.as<unsigned char>(), nrec,
+                                                       h->hfac, h->spectra.as<double2>() + g0 * nf);
+            residual_kernel<<<64, 256, 0, h->st>>>(h->spectra.as<double2>() + g0 * nf, d_obs.as<double2>() + g0 * nf,
+                                                   (long long)Gg * nrec * nf, d_R.as<double2>() + g0 * nf,
+                                                   d_mis.as<double>());
+            adj_source_kernel<<<256, 256, 0, h->st>>>(d_R.as<double2>() + g0 * nf, Gg * nrec, nrec, nf, nt,
+                                                      h->d_omega.as<double>(), h->ph.dt, h->ph.omega0,
+                                                      h->rec_is_h.as<unsigned char>(), h->hfac,
+                                                      d_asrc.as<double>() + g0 * nt);
+        } else if (nrec > 0) {
+            CK(cudaMemsetAsync(d_asrc.as<double>() + (size_t)s0 * nrec * nt, 0,
+                               (size_t)Gg * nrec * nt * sizeof(double), h->st));
+        }
+        CK(cudaGetLastError());
+        if ((rc = gmark(0))) return rc;
         // adjoint
         for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(lam[c].p, 0, gF * h->esz, h->st));
         for (int a = 0; a < 3; a++)
@@ -1269,17 +1328,51 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         const size_t slot = 6 * gF;
         for (int seg = ncheck - 1; seg >= 0; seg--) {
             const int n0 = seg * K, n1 = std::min(nt, n0 + K);
-            if ((rc = load_state(ck.as<char>() + (size_t)seg * ck_stride))) return rc;
-            if ((rc = set_step(n0))) return rc;
-            copy_state_kernel<T><<<512, 256, 0, h->st>>>(fl[0].as<T>(), fl[1].as<T>(), fl[2].as<T>(), fl[3].as<T>(),
-                                                         fl[4].as<T>(), fl[5].as<T>(), hist.as<T>(), (long long)gF);
-            for (int q = 0; q < n1 - n0; q++) {
-                fwd_step();
-                copy_state_kernel<T><<<512, 256, 0, h->st>>>(fl[0].as<T>(), fl[1].as<T>(), fl[2].as<T>(),
-                                                             fl[3].as<T>(), fl[4].as<T>(), fl[5].as<T>(),
-                                                             hist.as<T>() + (size_t)(q + 1) * slot, (long long)gF);
+            if (!hm && !std::getenv("MITTET_GRAD_COPY")) {
+                // Each recomputed step reads history slot q and writes slot
+                // q + 1 (the phases' outputs go straight to the next slot; the
+                // electric injection lands on the new E), so no copies.  With
+                // magnetic sources the injection changes the step's input H,
+                // which the history keeps as it was before it: copy instead.
+                // MITTET_GRAD_COPY forces the copying path (same results).
+                T *slot_f[6];
+                for (int c = 0; c < 6; c++) slot_f[c] = hist.as<T>() + c * gF;
+                if ((rc = load_state(ck.as<char>() + (size_t)seg * ck_stride, slot_f))) return rc;
+                if ((rc = set_step(n0))) return rc;
+                for (int q = 0; q < n1 - n0; q++) {
+                    T *in = hist.as<T>() + (size_t)q * slot, *out = hist.as<T>() + (size_t)(q + 1) * slot;
+                    PhaseArgs<T> eq = ea, hq = ha;
+                    for (int c = 0; c < 6; c++) {
+                        eq.f[c] = eq.fo[c] = in + c * gF;
+                        hq.f[c] = hq.fo[c] = (c < 3 ? out : in) + c * gF;
+                    }
+                    for (int c = 0; c < 3; c++) {
+                        eq.fo[c] = out + c * gF;
+                        hq.fo[3 + c] = out + (3 + c) * gF;
+                    }
+                    InjectArgs<T> iq = ia_e;
+                    for (int c = 0; c < 6; c++) iq.f[c] = out + c * gF;
+                    launch_phase<T>(h, true, h->var_e, eq);
+                    if (h->has_ele) inject_kernel<T><<<1, 128, 0, h->st>>>(iq);
+                    launch_phase<T>(h, false, h->var_h, hq);
+                    sample_kernel<T><<<1, 32, 0, h->st>>>(sa);
+                }
+            } else {
+                if ((rc = load_state(ck.as<char>() + (size_t)seg * ck_stride, nullptr))) return rc;
+                if ((rc = set_step(n0))) return rc;
+                const dim3 cgrid(148 * 2, 6);
+                copy_state_kernel<T><<<cgrid, 256, 0, h->st>>>(fl[0].as<T>(), fl[1].as<T>(), fl[2].as<T>(),
+                                                              fl[3].as<T>(), fl[4].as<T>(), fl[5].as<T>(), hist.as<T>(),
+                                                              (long long)gF);
+                for (int q = 0; q < n1 - n0; q++) {
+                    fwd_step(false);
+                    copy_state_kernel<T><<<cgrid, 256, 0, h->st>>>(fl[0].as<T>(), fl[1].as<T>(), fl[2].as<T>(),
+                                                                  fl[3].as<T>(), fl[4].as<T>(), fl[5].as<T>(),
+                                                                  hist.as<T>() + (size_t)(q + 1) * slot, (long long)gF);
+                }
             }
             CK(cudaGetLastError());
+            if ((rc = gmark(1))) return rc;
             for (int n = n1 - 1; n >= n0; n--) {
                 const int q = n - n0;
                 for (int c = 0; c < 3; c++) {
@@ -1303,6 +1396,7 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
                 adj_e_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
             }
             CK(cudaGetLastError());
+            if ((rc = gmark(2))) return rc;
         }
         h->has_mag = mag0;
         h->has_ele = ele0;
@@ -1316,6 +1410,20 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
     h->nshot = ns_saved;
     h->vmask = (uint32_t)vmask_keep;
     drop_graph(h);
+    int flag = 0;
+    double mis = 0.0;
+    CK(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(&mis, d_mis.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (glog) {
+        fprintf(stderr, "gradient stages (ms): checkpoint pass %.1f, recompute %.1f, adjoint %.1f\n", gms[0], gms[1],
+                gms[2]);
+        cudaEventDestroy(gev[0]);
+        cudaEventDestroy(gev[1]);
+    }
+    if (flag & 2) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded wait for a TMA copy gave up");
+    if (flag) return fail(MITTET_ERR_DIVERGED, "non-finite receiver samples (unstable time step or model)");
+    *misfit_out = mis;
     memcpy(grad_out, gsum.data(), ncell * sizeof(double));
     return MITTET_OK;
 }

@@ -288,7 +288,7 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
     for (int t = 0; t < 2; t++) {
         PhaseArgs<float> &a = pa[t];
         memset(&a, 0, sizeof(a));
-        for (int c = 0; c < 6; c++) a.f[c] = (float *)(base + o_f[c]);
+        for (int c = 0; c < 6; c++) a.f[c] = a.fo[c] = (float *)(base + o_f[c]);
         for (int ax = 0; ax < 3; ax++)
             for (int w = 0; w < 2; w++) a.psi[ax][w] = (float *)(base + (t == 0 ? o_pe[ax][w] : o_ph[ax][w]));
         a.m = (const float *)(base + o_m);

@@ -169,9 +169,12 @@ constexpr int part_min_blocks() {
 template <typename T, int VX, int GM, bool ONE>
 __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
     const long long sb = (long long)shot * a.fshot;
-    T *__restrict__ Ex = a.f[0] + sb;
-    T *__restrict__ Ey = a.f[1] + sb;
-    T *__restrict__ Ez = a.f[2] + sb;
+    const T *__restrict__ Ex = a.f[0] + sb;
+    const T *__restrict__ Ey = a.f[1] + sb;
+    const T *__restrict__ Ez = a.f[2] + sb;
+    T *__restrict__ Exo = a.fo[0] + sb;
+    T *__restrict__ Eyo = a.fo[1] + sb;
+    T *__restrict__ Ezo = a.fo[2] + sb;
     const T *__restrict__ Hx = a.f[3] + sb;
     const T *__restrict__ Hy = a.f[4] + sb;
     const T *__restrict__ Hz = a.f[5] + sb;
@@ -422,9 +425,9 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
             st_psi<T, VX>(sz0, oz, qz0, mz);
             st_psi<T, VX>(sz1, oz, qz1, mz);
         }
-        stv<T, VX>(Ex + c, ex);
-        stv<T, VX>(Ey + c, ey);
-        stv<T, VX>(Ez + c, ez);
+        stv<T, VX>(Exo + c, ex);
+        stv<T, VX>(Eyo + c, ey);
+        stv<T, VX>(Ezo + c, ez);
         if (a.ring_k > 0) {
             const long long e = sb + c;
             if (a.vmask & 1) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
@@ -446,9 +449,12 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
     const T *__restrict__ Ex = a.f[0] + sb;
     const T *__restrict__ Ey = a.f[1] + sb;
     const T *__restrict__ Ez = a.f[2] + sb;
-    T *__restrict__ Hx = a.f[3] + sb;
-    T *__restrict__ Hy = a.f[4] + sb;
-    T *__restrict__ Hz = a.f[5] + sb;
+    const T *__restrict__ Hx = a.f[3] + sb;
+    const T *__restrict__ Hy = a.f[4] + sb;
+    const T *__restrict__ Hz = a.f[5] + sb;
+    T *__restrict__ Hxo = a.fo[3] + sb;
+    T *__restrict__ Hyo = a.fo[4] + sb;
+    T *__restrict__ Hzo = a.fo[5] + sb;
     const T *__restrict__ M = a.m;
     const T *__restrict__ DM = a.dtmu;
     const T *__restrict__ P = a.prof;
@@ -703,9 +709,9 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
             st_psi<T, VX>(sz0, oz, qz0, mz);
             st_psi<T, VX>(sz1, oz, qz1, mz);
         }
-        stv<T, VX>(Hx + c, hx);
-        stv<T, VX>(Hy + c, hy);
-        stv<T, VX>(Hz + c, hz);
+        stv<T, VX>(Hxo + c, hx);
+        stv<T, VX>(Hyo + c, hy);
+        stv<T, VX>(Hzo + c, hz);
 #pragma unroll
         for (int v = 0; v < VX; v++) {
             wx[0][v] = wx[1][v]; wx[1][v] = wx[2][v]; wx[2][v] = wx[3][v];

@@ -268,9 +268,9 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
                 ez[v] = leap(T(1), sg * mv, curl2(dxHy, ikx, dyHx, iky), ez[v]);
             }
             if (inside) {
-                stv<T, VX>(a.f[0] + sb + c, ex);
-                stv<T, VX>(a.f[1] + sb + c, ey);
-                stv<T, VX>(a.f[2] + sb + c, ez);
+                stv<T, VX>(a.fo[0] + sb + c, ex);
+                stv<T, VX>(a.fo[1] + sb + c, ey);
+                stv<T, VX>(a.fo[2] + sb + c, ez);
                 if (a.ring_k > 0) {
                     const long long e = sb + c;
                     if (a.vmask & 1) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
@@ -317,9 +317,9 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
                 hz[v] = leap(T(1), -sg * dmv, curl2(dxEy, ikx, dyEx, iky), hz[v]);
             }
             if (inside) {
-                stv<T, VX>(a.f[3] + sb + c, hx);
-                stv<T, VX>(a.f[4] + sb + c, hy);
-                stv<T, VX>(a.f[5] + sb + c, hz);
+                stv<T, VX>(a.fo[3] + sb + c, hx);
+                stv<T, VX>(a.fo[4] + sb + c, hy);
+                stv<T, VX>(a.fo[5] + sb + c, hz);
             }
         }
 #pragma unroll
