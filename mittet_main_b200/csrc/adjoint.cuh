@@ -64,29 +64,57 @@ __device__ __forceinline__ T pget(const AdjArgs<T> &a, int axis, int which, int 
     return __ldg(a.prof + ((size_t)axis * 8 + which) * a.nmax + v);
 }
 
+// Each kernel loads what its cell needs up front and passes the values to a
+// per-cell function.  Measured alternatives that were slower on the
+// 128x128x96, 16-shot gradient (about two thirds of its cells in CPML slabs):
+// four x cells per thread with vector loads (the lanes serialise the general
+// path), and gathers that form the weights of deep-interior neighbours from
+// the adjoint fields instead of reading them (more loads: the model at every
+// E tap).
+
+// Taps of a (2,4) transposed difference along one axis; o* tell whether a
+// tap lies inside the grid.
+// (D+^T mu)[u] = c1 mu[u-1] - c1 mu[u] + c2 mu[u-2] - c2 mu[u+1];  typo: c2t replaces c1 on mu[u]
+template <typename T>
+__device__ __forceinline__ T dplus_v(T mc, T mm1, T mm2, T mp1, bool o1, bool o2, bool op, T c1, T c2, T c1u) {
+    T r = -c1u * mc;
+    if (o1) r = fma(c1, mm1, r);
+    if (o2) r = fma(c2, mm2, r);
+    if (op) r = fma(-c2, mp1, r);
+    return r;
+}
+// (D^T mu)[u] = c1 mu[u] - c1 mu[u+1] + c2 mu[u-1] - c2 mu[u+2]
+template <typename T>
+__device__ __forceinline__ T dminus_v(T mc, T mm1, T mp1, T mp2, bool om, bool op1, bool op2, T c1, T c2) {
+    T r = c1 * mc;
+    if (op1) r = fma(-c1, mp1, r);
+    if (om) r = fma(c2, mm1, r);
+    if (op2) r = fma(-c2, mp2, r);
+    return r;
+}
+
 // ---------------------------------------------------------------- H phase
 // mu[0] Dy+Ez, mu[1] Dz+Ey, mu[2] Dz+Ex, mu[3] Dx+Ez, mu[4] typo Dx Ez (psi_Hyx), mu[5] Dx+Ey, mu[6] Dy+Ex
+
+// Own half of the transposed H update at one cell: from the adjoint L of H
+// after the phase and dt/mu, the seven weights mu and the adjoint of H
+// before the phase (lam); the cell's psi adjoints and gradient (CPML cells)
+// are updated in memory.  Returns whether lam differs from L.
 template <typename T>
-__global__ void adj_h_own_kernel(AdjArgs<T> a) {
-    int i, j, k, shot;
-    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
-    const long long sb = (long long)shot * a.fshot;
-    const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
-    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
-    const T dm = a.dtmu ? a.dtmu[cm] : a.dtmu0;
+__device__ __forceinline__ bool h_own_cell(const AdjArgs<T> &a, int i, int j, int k, int shot, long long c,
+                                           long long cm, T L0, T L1, T L2, T dm, T (&mu)[7], T (&lam)[3]) {
+    const T s = a.sgn;
+    lam[0] = L0; lam[1] = L1; lam[2] = L2;
     if (in_box(a.ibox, i, j, k)) {
-        // da = 1, db = dt/mu, every update in range, no psi, no gradient term:
-        // the mu of the general path below, lambda_H unchanged
-        const T L0 = a.lam[3][c], L1 = a.lam[4][c], L2 = a.lam[5][c];
-        const T s = a.sgn;
-        a.mu[0][c] = -s * dm * a.ik[1] * L0;
-        a.mu[1][c] = s * dm * a.ik[2] * L0;
-        a.mu[2][c] = -s * dm * a.ik[2] * L1;
-        a.mu[3][c] = s * dm * a.ik[0] * L1;
-        a.mu[4][c] = T(0);
-        a.mu[5][c] = -s * dm * a.ik[0] * L2;
-        a.mu[6][c] = s * dm * a.ik[1] * L2;
-        return;
+        // da = 1, db = dt/mu, every update in range, no psi, no gradient term
+        mu[0] = -s * dm * a.ik[1] * L0;
+        mu[1] = s * dm * a.ik[2] * L0;
+        mu[2] = -s * dm * a.ik[2] * L1;
+        mu[3] = s * dm * a.ik[0] * L1;
+        mu[4] = T(0);
+        mu[5] = -s * dm * a.ik[0] * L2;
+        mu[6] = s * dm * a.ik[1] * L2;
+        return false;
     }
     const T m = a.m[cm];
     const T msh[3] = {pget(a, 0, 1, i), pget(a, 1, 1, j), pget(a, 2, 1, k)};
@@ -104,8 +132,6 @@ __global__ void adj_h_own_kernel(AdjArgs<T> a) {
         }
     }
     const bool in0 = in_box(a.upd[0], i, j, k), in1 = in_box(a.upd[1], i, j, k), in2 = in_box(a.upd[2], i, j, k);
-    const T L0 = a.lam[3][c], L1 = a.lam[4][c], L2 = a.lam[5][c];
-    const T s = a.sgn;
     T mu0 = in0 ? -s * db[0] * ik[1] * L0 : T(0);
     T mu1 = in0 ? s * db[0] * ik[2] * L0 : T(0);
     T mu2 = in1 ? -s * db[1] * ik[2] * L1 : T(0);
@@ -119,37 +145,36 @@ __global__ void adj_h_own_kernel(AdjArgs<T> a) {
         k < a.slab[0].other.hi[2]) {
         const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
         const T bh = pget(a, 0, 4, i), chd = pget(a, 0, 5, i);
-        const T lzx = a.lpsi[0][0][o] - db[2] * L2;  // psi_Hzx
-        const T lyx = a.lpsi[0][1][o] + db[1] * L1;  // psi_Hyx
+        const T lzx = fma(-db[2], L2, a.lpsi[0][0][o]);  // psi_Hzx
+        const T lyx = fma(db[1], L1, a.lpsi[0][1][o]);   // psi_Hyx
         a.lpsi[0][0][o] = bh * lzx;
         a.lpsi[0][1][o] = bh * lyx;
-        mu5 += chd * lzx;
-        mu4 += chd * lyx;
+        mu5 = fma(chd, lzx, mu5);
+        mu4 = fma(chd, lyx, mu4);
     }
     if (ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0] && k >= a.slab[1].other.lo[2] &&
         k < a.slab[1].other.hi[2]) {
         const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
         const T bh = pget(a, 1, 4, j), chd = pget(a, 1, 5, j);
-        const T lxy = a.lpsi[1][0][o] - db[0] * L0;  // psi_Hxy
-        const T lzy = a.lpsi[1][1][o] + db[2] * L2;  // psi_Hzy
+        const T lxy = fma(-db[0], L0, a.lpsi[1][0][o]);  // psi_Hxy
+        const T lzy = fma(db[2], L2, a.lpsi[1][1][o]);   // psi_Hzy
         a.lpsi[1][0][o] = bh * lxy;
         a.lpsi[1][1][o] = bh * lzy;
-        mu0 += chd * lxy;
-        mu6 += chd * lzy;
+        mu0 = fma(chd, lxy, mu0);
+        mu6 = fma(chd, lzy, mu6);
     }
     if (lz >= 0 && i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
         j < a.slab[2].other.hi[1]) {
         const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
         const T bh = pget(a, 2, 4, k), chd = pget(a, 2, 5, k);
-        const T lyz = a.lpsi[2][0][o] - db[1] * L1;  // psi_Hyz
-        const T lxz = a.lpsi[2][1][o] + db[0] * L0;  // psi_Hxz
+        const T lyz = fma(-db[1], L1, a.lpsi[2][0][o]);  // psi_Hyz
+        const T lxz = fma(db[0], L0, a.lpsi[2][1][o]);   // psi_Hxz
         a.lpsi[2][0][o] = bh * lyz;
         a.lpsi[2][1][o] = bh * lxz;
-        mu2 += chd * lyz;
-        mu1 += chd * lxz;
+        mu2 = fma(chd, lyz, mu2);
+        mu1 = fma(chd, lxz, mu1);
     }
-    a.mu[0][c] = mu0; a.mu[1][c] = mu1; a.mu[2][c] = mu2; a.mu[3][c] = mu3;
-    a.mu[4][c] = mu4; a.mu[5][c] = mu5; a.mu[6][c] = mu6;
+    mu[0] = mu0; mu[1] = mu1; mu[2] = mu2; mu[3] = mu3; mu[4] = mu4; mu[5] = mu5; mu[6] = mu6;
     // gradient (CPML cells only: interior da, db do not depend on sigma)
     double gsum = 0.0;
     const double isig = (double)m * a.inv2w0dt;
@@ -161,22 +186,37 @@ __global__ void adj_h_own_kernel(AdjArgs<T> a) {
         const double dda = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
         const double rdb = h * isig / (1.0 + h);
         const double h0 = (double)a.H0[q][c], h1 = (double)a.H1[q][c];
-        gsum += (double)L[q] * ((in[q] ? dda * h0 : 0.0) + rdb * (h1 - (in[q] ? (double)da[q] * h0 : h0)));
+        const double d = in[q] ? fma(-(double)da[q], h0, h1) : h1 - h0;
+        gsum = fma((double)L[q], fma(rdb, d, in[q] ? dda * h0 : 0.0), gsum);
     }
     if (gsum != 0.0) a.grad[c] += gsum;
-    a.lam[3][c] = in0 ? da[0] * L0 : L0;
-    a.lam[4][c] = in1 ? da[1] * L1 : L1;
-    a.lam[5][c] = in2 ? da[2] * L2 : L2;
+    lam[0] = in0 ? da[0] * L0 : L0;
+    lam[1] = in1 ? da[1] * L1 : L1;
+    lam[2] = in2 ? da[2] * L2 : L2;
+    return true;
 }
 
-// (D+^T mu)[u] = c1 mu[u-1] - c1 mu[u] + c2 mu[u-2] - c2 mu[u+1];  typo: c2t replaces c1 on mu[u]
 template <typename T>
-__device__ __forceinline__ T dplus_t(const T *__restrict__ mu, long long c, long long s, int v, int n, T c1, T c2, T c1u) {
-    T r = -c1u * mu[c];
-    if (v >= 1) r += c1 * mu[c - s];
-    if (v >= 2) r += c2 * mu[c - 2 * s];
-    if (v + 1 < n) r -= c2 * mu[c + s];
-    return r;
+__global__ void adj_h_own_kernel(AdjArgs<T> a) {
+    int i, j, k, shot;
+    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
+    const long long c = (long long)shot * a.fshot + cm;
+    const T dm = a.dtmu ? a.dtmu[cm] : a.dtmu0;
+    T mu[7], lam[3];
+    const bool ch = h_own_cell(a, i, j, k, shot, c, cm, a.lam[3][c], a.lam[4][c], a.lam[5][c], dm, mu, lam);
+#pragma unroll
+    for (int w = 0; w < 7; w++) a.mu[w][c] = mu[w];
+    if (ch) { a.lam[3][c] = lam[0]; a.lam[4][c] = lam[1]; a.lam[5][c] = lam[2]; }
+}
+
+// Taps [u, u-1, u-2, u+1] of one weight array along one axis (stride s).
+template <typename T>
+__device__ __forceinline__ void taps_p(const T *__restrict__ mu, long long c, long long s, int v, int n, T (&t)[4]) {
+    t[0] = mu[c];
+    t[1] = v >= 1 ? mu[c - s] : T(0);
+    t[2] = v >= 2 ? mu[c - 2 * s] : T(0);
+    t[3] = v + 1 < n ? mu[c + s] : T(0);
 }
 
 template <typename T>
@@ -185,11 +225,25 @@ __global__ void adj_h_gather_kernel(AdjArgs<T> a) {
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
     const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i;
     const long long sy = a.px, sz = a.plane;
+    T t0[4], t1[4], t2[4], t3[4], t4[4], t5[4], t6[4];
+    taps_p(a.mu[0], c, sy, j, a.ny, t0);
+    taps_p(a.mu[1], c, sz, k, a.nz, t1);
+    taps_p(a.mu[2], c, sz, k, a.nz, t2);
+    taps_p(a.mu[3], c, 1, i, a.nx, t3);
+    taps_p(a.mu[4], c, 1, i, a.nx, t4);
+    taps_p(a.mu[5], c, 1, i, a.nx, t5);
+    taps_p(a.mu[6], c, sy, j, a.ny, t6);
     const T c1 = a.c1, c2 = a.c2;
-    const T gz = dplus_t(a.mu[0], c, sy, j, a.ny, c1, c2, c1) + dplus_t(a.mu[3], c, 1, i, a.nx, c1, c2, c1) +
-                 dplus_t(a.mu[4], c, 1, i, a.nx, c1, c2, a.c2t);
-    const T gy = dplus_t(a.mu[1], c, sz, k, a.nz, c1, c2, c1) + dplus_t(a.mu[5], c, 1, i, a.nx, c1, c2, c1);
-    const T gx = dplus_t(a.mu[2], c, sz, k, a.nz, c1, c2, c1) + dplus_t(a.mu[6], c, sy, j, a.ny, c1, c2, c1);
+    const bool y1 = j >= 1, y2 = j >= 2, yp = j + 1 < a.ny;
+    const bool z1 = k >= 1, z2 = k >= 2, zp = k + 1 < a.nz;
+    const bool x1 = i >= 1, x2 = i >= 2, xp = i + 1 < a.nx;
+    const T gz = dplus_v(t0[0], t0[1], t0[2], t0[3], y1, y2, yp, c1, c2, c1) +
+                 dplus_v(t3[0], t3[1], t3[2], t3[3], x1, x2, xp, c1, c2, c1) +
+                 dplus_v(t4[0], t4[1], t4[2], t4[3], x1, x2, xp, c1, c2, a.c2t);
+    const T gy = dplus_v(t1[0], t1[1], t1[2], t1[3], z1, z2, zp, c1, c2, c1) +
+                 dplus_v(t5[0], t5[1], t5[2], t5[3], x1, x2, xp, c1, c2, c1);
+    const T gx = dplus_v(t2[0], t2[1], t2[2], t2[3], z1, z2, zp, c1, c2, c1) +
+                 dplus_v(t6[0], t6[1], t6[2], t6[3], y1, y2, yp, c1, c2, c1);
     a.lam[0][c] += gx;
     a.lam[1][c] += gy;
     a.lam[2][c] += gz;
@@ -197,37 +251,35 @@ __global__ void adj_h_gather_kernel(AdjArgs<T> a) {
 
 // ---------------------------------------------------------------- E phase
 // mu[0] DyHz, mu[1] DzHy, mu[2] DzHx, mu[3] DxHz, mu[4] DxHy, mu[5] DyHx
+
+// Own half of the transposed E update at one cell, from the adjoint L of E
+// after the phase, the model word m, the cell's E before (e0) and after (e1)
+// the phase and its gradient accumulator g (returned updated): the six
+// weights mu and the adjoint of E before the phase (lam); psi adjoints are
+// updated in memory.  Returns whether lam differs from L.
 template <typename T>
-__global__ void adj_e_own_kernel(AdjArgs<T> a) {
-    int i, j, k, shot;
-    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
-    const long long sb = (long long)shot * a.fshot;
-    const long long c = sb + (long long)k * a.plane + (long long)j * a.px + i;
-    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
-    const T m = a.m[cm];
+__device__ __forceinline__ bool e_own_cell(const AdjArgs<T> &a, int i, int j, int k, int shot, T m, T L0, T L1,
+                                           T L2, const T (&e0)[3], const T (&e1)[3], double &g, T (&mu)[6],
+                                           T (&lam)[3]) {
+    const T s = a.sgn;
+    lam[0] = L0; lam[1] = L1; lam[2] = L2;
+    const T L[3] = {L0, L1, L2};
+    const double isig = (double)m * a.inv2w0dt;
     if (in_box(a.ibox, i, j, k)) {
-        // ca = 1, cb = m, every update in range, no psi: the mu and gradient
-        // term of the general path below (h = 0: dca = 0, dcb/cb = -1/sigma),
-        // lambda_E unchanged
-        const T L0 = a.lam[0][c], L1 = a.lam[1][c], L2 = a.lam[2][c];
-        const T s = a.sgn;
-        a.mu[0][c] = s * m * a.ik[1] * L0;
-        a.mu[1][c] = -s * m * a.ik[2] * L0;
-        a.mu[2][c] = s * m * a.ik[2] * L1;
-        a.mu[3][c] = -s * m * a.ik[0] * L1;
-        a.mu[4][c] = s * m * a.ik[0] * L2;
-        a.mu[5][c] = -s * m * a.ik[1] * L2;
-        const double isig = (double)m * a.inv2w0dt;
-        const double rcb = -isig / (1.0 + 0.0);
-        const T L[3] = {L0, L1, L2};
+        // ca = 1, cb = m, every update in range, no psi; h = 0: dca = 0,
+        // dcb/cb = -1/sigma
+        mu[0] = s * m * a.ik[1] * L0;
+        mu[1] = -s * m * a.ik[2] * L0;
+        mu[2] = s * m * a.ik[2] * L1;
+        mu[3] = -s * m * a.ik[0] * L1;
+        mu[4] = s * m * a.ik[0] * L2;
+        mu[5] = -s * m * a.ik[1] * L2;
+        const double rcb = -isig;
         double gsum = 0.0;
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const double e0 = (double)a.E0[q][c], e1 = (double)a.E1[q][c];
-            gsum += (double)L[q] * (0.0 * e0 + rcb * (e1 - 1.0 * e0));
-        }
-        a.grad[c] += gsum;
-        return;
+        for (int q = 0; q < 3; q++) gsum = fma((double)L[q], rcb * ((double)e1[q] - (double)e0[q]), gsum);
+        g += gsum;
+        return false;
     }
     const T esh[3] = {pget(a, 0, 0, i), pget(a, 1, 0, j), pget(a, 2, 0, k)};
     const T ik[3] = {pget(a, 0, 6, i), pget(a, 1, 6, j), pget(a, 2, 6, k)};
@@ -244,8 +296,6 @@ __global__ void adj_e_own_kernel(AdjArgs<T> a) {
         }
     }
     const bool in0 = in_box(a.upd[0], i, j, k), in1 = in_box(a.upd[1], i, j, k), in2 = in_box(a.upd[2], i, j, k);
-    const T L0 = a.lam[0][c], L1 = a.lam[1][c], L2 = a.lam[2][c];
-    const T s = a.sgn;
     T mu0 = in0 ? s * cb[0] * ik[1] * L0 : T(0);   // DyHz
     T mu1 = in0 ? -s * cb[0] * ik[2] * L0 : T(0);  // DzHy
     T mu2 = in1 ? s * cb[1] * ik[2] * L1 : T(0);   // DzHx
@@ -257,63 +307,77 @@ __global__ void adj_e_own_kernel(AdjArgs<T> a) {
         k < a.slab[0].other.hi[2]) {
         const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
         const T be = pget(a, 0, 2, i), ced = pget(a, 0, 3, i);
-        const T lzx = a.lpsi[0][0][o] + cb[2] * L2;  // psi_Ezx
-        const T lyx = a.lpsi[0][1][o] - cb[1] * L1;  // psi_Eyx
+        const T lzx = fma(cb[2], L2, a.lpsi[0][0][o]);   // psi_Ezx
+        const T lyx = fma(-cb[1], L1, a.lpsi[0][1][o]);  // psi_Eyx
         a.lpsi[0][0][o] = be * lzx;
         a.lpsi[0][1][o] = be * lyx;
-        mu4 += ced * lzx;
-        mu3 += ced * lyx;
+        mu4 = fma(ced, lzx, mu4);
+        mu3 = fma(ced, lyx, mu3);
     }
     if (ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0] && k >= a.slab[1].other.lo[2] &&
         k < a.slab[1].other.hi[2]) {
         const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
         const T be = pget(a, 1, 2, j), ced = pget(a, 1, 3, j);
-        const T lxy = a.lpsi[1][0][o] + cb[0] * L0;  // psi_Exy
-        const T lzy = a.lpsi[1][1][o] - cb[2] * L2;  // psi_Ezy
+        const T lxy = fma(cb[0], L0, a.lpsi[1][0][o]);   // psi_Exy
+        const T lzy = fma(-cb[2], L2, a.lpsi[1][1][o]);  // psi_Ezy
         a.lpsi[1][0][o] = be * lxy;
         a.lpsi[1][1][o] = be * lzy;
-        mu0 += ced * lxy;
-        mu5 += ced * lzy;
+        mu0 = fma(ced, lxy, mu0);
+        mu5 = fma(ced, lzy, mu5);
     }
     if (lz >= 0 && i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
         j < a.slab[2].other.hi[1]) {
         const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
         const T be = pget(a, 2, 2, k), ced = pget(a, 2, 3, k);
-        const T lyz = a.lpsi[2][0][o] + cb[1] * L1;  // psi_Eyz
-        const T lxz = a.lpsi[2][1][o] - cb[0] * L0;  // psi_Exz
+        const T lyz = fma(cb[1], L1, a.lpsi[2][0][o]);   // psi_Eyz
+        const T lxz = fma(-cb[0], L0, a.lpsi[2][1][o]);  // psi_Exz
         a.lpsi[2][0][o] = be * lyz;
         a.lpsi[2][1][o] = be * lxz;
-        mu2 += ced * lyz;
-        mu1 += ced * lxz;
+        mu2 = fma(ced, lyz, mu2);
+        mu1 = fma(ced, lxz, mu1);
     }
-    a.mu[0][c] = mu0; a.mu[1][c] = mu1; a.mu[2][c] = mu2;
-    a.mu[3][c] = mu3; a.mu[4][c] = mu4; a.mu[5][c] = mu5;
+    mu[0] = mu0; mu[1] = mu1; mu[2] = mu2; mu[3] = mu3; mu[4] = mu4; mu[5] = mu5;
     // gradient: every cell (cb = m/(1+h) depends on sigma everywhere)
-    const double isig = (double)m * a.inv2w0dt;
     const bool in[3] = {in0, in1, in2};
-    const T L[3] = {L0, L1, L2};
     double gsum = 0.0;
     for (int q = 0; q < 3; q++) {
         const double h = (double)esh[q] * (double)m;
         const double dca = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
         const double rcb = -isig / (1.0 + h);
-        const double e0 = (double)a.E0[q][c], e1 = (double)a.E1[q][c];
-        gsum += (double)L[q] * ((in[q] ? dca * e0 : 0.0) + rcb * (e1 - (in[q] ? (double)ca[q] * e0 : e0)));
+        const double x0 = (double)e0[q], x1 = (double)e1[q];
+        const double d = in[q] ? fma(-(double)ca[q], x0, x1) : x1 - x0;
+        gsum = fma((double)L[q], fma(rcb, d, in[q] ? dca * x0 : 0.0), gsum);
     }
-    a.grad[c] += gsum;
-    a.lam[0][c] = in0 ? ca[0] * L0 : L0;
-    a.lam[1][c] = in1 ? ca[1] * L1 : L1;
-    a.lam[2][c] = in2 ? ca[2] * L2 : L2;
+    g += gsum;
+    lam[0] = in0 ? ca[0] * L0 : L0;
+    lam[1] = in1 ? ca[1] * L1 : L1;
+    lam[2] = in2 ? ca[2] * L2 : L2;
+    return true;
 }
 
-// (D^T mu)[u] = c1 mu[u] - c1 mu[u+1] + c2 mu[u-1] - c2 mu[u+2]
 template <typename T>
-__device__ __forceinline__ T dminus_t(const T *__restrict__ mu, long long c, long long s, int v, int n, T c1, T c2) {
-    T r = c1 * mu[c];
-    if (v + 1 < n) r -= c1 * mu[c + s];
-    if (v >= 1) r += c2 * mu[c - s];
-    if (v + 2 < n) r -= c2 * mu[c + 2 * s];
-    return r;
+__global__ void adj_e_own_kernel(AdjArgs<T> a) {
+    int i, j, k, shot;
+    if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
+    const long long c = (long long)shot * a.fshot + cm;
+    const T e0[3] = {a.E0[0][c], a.E0[1][c], a.E0[2][c]}, e1[3] = {a.E1[0][c], a.E1[1][c], a.E1[2][c]};
+    double g = a.grad[c];
+    T mu[6], lam[3];
+    const bool ch = e_own_cell(a, i, j, k, shot, a.m[cm], a.lam[0][c], a.lam[1][c], a.lam[2][c], e0, e1, g, mu, lam);
+    a.grad[c] = g;
+#pragma unroll
+    for (int w = 0; w < 6; w++) a.mu[w][c] = mu[w];
+    if (ch) { a.lam[0][c] = lam[0]; a.lam[1][c] = lam[1]; a.lam[2][c] = lam[2]; }
+}
+
+// Taps [u, u-1, u+1, u+2] of one weight array along one axis (stride s).
+template <typename T>
+__device__ __forceinline__ void taps_m(const T *__restrict__ mu, long long c, long long s, int v, int n, T (&t)[4]) {
+    t[0] = mu[c];
+    t[1] = v >= 1 ? mu[c - s] : T(0);
+    t[2] = v + 1 < n ? mu[c + s] : T(0);
+    t[3] = v + 2 < n ? mu[c + 2 * s] : T(0);
 }
 
 template <typename T>
@@ -322,10 +386,23 @@ __global__ void adj_e_gather_kernel(AdjArgs<T> a) {
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
     const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i;
     const long long sy = a.px, sz = a.plane;
+    T t0[4], t1[4], t2[4], t3[4], t4[4], t5[4];
+    taps_m(a.mu[0], c, sy, j, a.ny, t0);
+    taps_m(a.mu[1], c, sz, k, a.nz, t1);
+    taps_m(a.mu[2], c, sz, k, a.nz, t2);
+    taps_m(a.mu[3], c, 1, i, a.nx, t3);
+    taps_m(a.mu[4], c, 1, i, a.nx, t4);
+    taps_m(a.mu[5], c, sy, j, a.ny, t5);
     const T c1 = a.c1, c2 = a.c2;
-    const T hz = dminus_t(a.mu[0], c, sy, j, a.ny, c1, c2) + dminus_t(a.mu[3], c, 1, i, a.nx, c1, c2);
-    const T hy = dminus_t(a.mu[1], c, sz, k, a.nz, c1, c2) + dminus_t(a.mu[4], c, 1, i, a.nx, c1, c2);
-    const T hx = dminus_t(a.mu[2], c, sz, k, a.nz, c1, c2) + dminus_t(a.mu[5], c, sy, j, a.ny, c1, c2);
+    const bool ym = j >= 1, yp1 = j + 1 < a.ny, yp2 = j + 2 < a.ny;
+    const bool zm = k >= 1, zp1 = k + 1 < a.nz, zp2 = k + 2 < a.nz;
+    const bool xm = i >= 1, xp1 = i + 1 < a.nx, xp2 = i + 2 < a.nx;
+    const T hz = dminus_v(t0[0], t0[1], t0[2], t0[3], ym, yp1, yp2, c1, c2) +
+                 dminus_v(t3[0], t3[1], t3[2], t3[3], xm, xp1, xp2, c1, c2);
+    const T hy = dminus_v(t1[0], t1[1], t1[2], t1[3], zm, zp1, zp2, c1, c2) +
+                 dminus_v(t4[0], t4[1], t4[2], t4[3], xm, xp1, xp2, c1, c2);
+    const T hx = dminus_v(t2[0], t2[1], t2[2], t2[3], zm, zp1, zp2, c1, c2) +
+                 dminus_v(t5[0], t5[1], t5[2], t5[3], ym, yp1, yp2, c1, c2);
     a.lam[3][c] += hx;
     a.lam[4][c] += hy;
     a.lam[5][c] += hz;
