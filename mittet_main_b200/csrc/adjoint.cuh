@@ -219,6 +219,29 @@ __device__ __forceinline__ void taps_p(const T *__restrict__ mu, long long c, lo
     t[3] = v + 1 < n ? mu[c + s] : T(0);
 }
 
+// Gather half of the transposed H update at one cell, from the taps
+// [u, u-1, u-2, u+1] of the seven weights: adds the transposed differences
+// to the cell's lambda_E (lx, ly, lz).
+template <typename T>
+__device__ __forceinline__ void h_gather_cell(const AdjArgs<T> &a, int i, int j, int k, const T (&t0)[4],
+                                              const T (&t1)[4], const T (&t2)[4], const T (&t3)[4], const T (&t4)[4],
+                                              const T (&t5)[4], const T (&t6)[4], T &lx, T &ly, T &lz) {
+    const T c1 = a.c1, c2 = a.c2;
+    const bool y1 = j >= 1, y2 = j >= 2, yp = j + 1 < a.ny;
+    const bool z1 = k >= 1, z2 = k >= 2, zp = k + 1 < a.nz;
+    const bool x1 = i >= 1, x2 = i >= 2, xp = i + 1 < a.nx;
+    const T gz = dplus_v(t0[0], t0[1], t0[2], t0[3], y1, y2, yp, c1, c2, c1) +
+                 dplus_v(t3[0], t3[1], t3[2], t3[3], x1, x2, xp, c1, c2, c1) +
+                 dplus_v(t4[0], t4[1], t4[2], t4[3], x1, x2, xp, c1, c2, a.c2t);
+    const T gy = dplus_v(t1[0], t1[1], t1[2], t1[3], z1, z2, zp, c1, c2, c1) +
+                 dplus_v(t5[0], t5[1], t5[2], t5[3], x1, x2, xp, c1, c2, c1);
+    const T gx = dplus_v(t2[0], t2[1], t2[2], t2[3], z1, z2, zp, c1, c2, c1) +
+                 dplus_v(t6[0], t6[1], t6[2], t6[3], y1, y2, yp, c1, c2, c1);
+    lx += gx;
+    ly += gy;
+    lz += gz;
+}
+
 template <typename T>
 __global__ void adj_h_gather_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
@@ -233,20 +256,11 @@ __global__ void adj_h_gather_kernel(AdjArgs<T> a) {
     taps_p(a.mu[4], c, 1, i, a.nx, t4);
     taps_p(a.mu[5], c, 1, i, a.nx, t5);
     taps_p(a.mu[6], c, sy, j, a.ny, t6);
-    const T c1 = a.c1, c2 = a.c2;
-    const bool y1 = j >= 1, y2 = j >= 2, yp = j + 1 < a.ny;
-    const bool z1 = k >= 1, z2 = k >= 2, zp = k + 1 < a.nz;
-    const bool x1 = i >= 1, x2 = i >= 2, xp = i + 1 < a.nx;
-    const T gz = dplus_v(t0[0], t0[1], t0[2], t0[3], y1, y2, yp, c1, c2, c1) +
-                 dplus_v(t3[0], t3[1], t3[2], t3[3], x1, x2, xp, c1, c2, c1) +
-                 dplus_v(t4[0], t4[1], t4[2], t4[3], x1, x2, xp, c1, c2, a.c2t);
-    const T gy = dplus_v(t1[0], t1[1], t1[2], t1[3], z1, z2, zp, c1, c2, c1) +
-                 dplus_v(t5[0], t5[1], t5[2], t5[3], x1, x2, xp, c1, c2, c1);
-    const T gx = dplus_v(t2[0], t2[1], t2[2], t2[3], z1, z2, zp, c1, c2, c1) +
-                 dplus_v(t6[0], t6[1], t6[2], t6[3], y1, y2, yp, c1, c2, c1);
-    a.lam[0][c] += gx;
-    a.lam[1][c] += gy;
-    a.lam[2][c] += gz;
+    T lx = a.lam[0][c], ly = a.lam[1][c], lz = a.lam[2][c];
+    h_gather_cell(a, i, j, k, t0, t1, t2, t3, t4, t5, t6, lx, ly, lz);
+    a.lam[0][c] = lx;
+    a.lam[1][c] = ly;
+    a.lam[2][c] = lz;
 }
 
 // ---------------------------------------------------------------- E phase
@@ -380,6 +394,28 @@ __device__ __forceinline__ void taps_m(const T *__restrict__ mu, long long c, lo
     t[3] = v + 2 < n ? mu[c + 2 * s] : T(0);
 }
 
+// Gather half of the transposed E update at one cell, from the taps
+// [u, u-1, u+1, u+2] of the six weights: adds the transposed differences to
+// the cell's lambda_H (lx, ly, lz).
+template <typename T>
+__device__ __forceinline__ void e_gather_cell(const AdjArgs<T> &a, int i, int j, int k, const T (&t0)[4],
+                                              const T (&t1)[4], const T (&t2)[4], const T (&t3)[4], const T (&t4)[4],
+                                              const T (&t5)[4], T &lx, T &ly, T &lz) {
+    const T c1 = a.c1, c2 = a.c2;
+    const bool ym = j >= 1, yp1 = j + 1 < a.ny, yp2 = j + 2 < a.ny;
+    const bool zm = k >= 1, zp1 = k + 1 < a.nz, zp2 = k + 2 < a.nz;
+    const bool xm = i >= 1, xp1 = i + 1 < a.nx, xp2 = i + 2 < a.nx;
+    const T hz = dminus_v(t0[0], t0[1], t0[2], t0[3], ym, yp1, yp2, c1, c2) +
+                 dminus_v(t3[0], t3[1], t3[2], t3[3], xm, xp1, xp2, c1, c2);
+    const T hy = dminus_v(t1[0], t1[1], t1[2], t1[3], zm, zp1, zp2, c1, c2) +
+                 dminus_v(t4[0], t4[1], t4[2], t4[3], xm, xp1, xp2, c1, c2);
+    const T hx = dminus_v(t2[0], t2[1], t2[2], t2[3], zm, zp1, zp2, c1, c2) +
+                 dminus_v(t5[0], t5[1], t5[2], t5[3], ym, yp1, yp2, c1, c2);
+    lx += hx;
+    ly += hy;
+    lz += hz;
+}
+
 template <typename T>
 __global__ void adj_e_gather_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
@@ -393,19 +429,150 @@ __global__ void adj_e_gather_kernel(AdjArgs<T> a) {
     taps_m(a.mu[3], c, 1, i, a.nx, t3);
     taps_m(a.mu[4], c, 1, i, a.nx, t4);
     taps_m(a.mu[5], c, sy, j, a.ny, t5);
-    const T c1 = a.c1, c2 = a.c2;
-    const bool ym = j >= 1, yp1 = j + 1 < a.ny, yp2 = j + 2 < a.ny;
-    const bool zm = k >= 1, zp1 = k + 1 < a.nz, zp2 = k + 2 < a.nz;
-    const bool xm = i >= 1, xp1 = i + 1 < a.nx, xp2 = i + 2 < a.nx;
-    const T hz = dminus_v(t0[0], t0[1], t0[2], t0[3], ym, yp1, yp2, c1, c2) +
-                 dminus_v(t3[0], t3[1], t3[2], t3[3], xm, xp1, xp2, c1, c2);
-    const T hy = dminus_v(t1[0], t1[1], t1[2], t1[3], zm, zp1, zp2, c1, c2) +
-                 dminus_v(t4[0], t4[1], t4[2], t4[3], xm, xp1, xp2, c1, c2);
-    const T hx = dminus_v(t2[0], t2[1], t2[2], t2[3], zm, zp1, zp2, c1, c2) +
-                 dminus_v(t5[0], t5[1], t5[2], t5[3], ym, yp1, yp2, c1, c2);
-    a.lam[3][c] += hx;
-    a.lam[4][c] += hy;
-    a.lam[5][c] += hz;
+    T lx = a.lam[3][c], ly = a.lam[4][c], lz = a.lam[5][c];
+    e_gather_cell(a, i, j, k, t0, t1, t2, t3, t4, t5, lx, ly, lz);
+    a.lam[3][c] = lx;
+    a.lam[4][c] = ly;
+    a.lam[5][c] = lz;
+}
+
+// ------------------------------------------------ vectorised gathers
+// The gathers have no CPML branches, so VX consecutive x cells per thread
+// (VX = 4 FP32, 2 FP64; one aligned vector load per weight array and tap)
+// pay off there; the own kernels keep one thread per cell, since vector
+// lanes would serialise their general path.  Both call the same per-cell
+// functions, so the results are bit-identical.
+
+template <int VX>
+__device__ __forceinline__ bool adjv_cell(int &i0, int &j, int &k, int &shot, int nx, int ny, int nz) {
+    i0 = (blockIdx.x * blockDim.x + threadIdx.x) * VX;
+    j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int zz = blockIdx.z;
+    k = zz % nz;
+    shot = zz / nz;
+    return i0 < nx && j < ny;
+}
+// Vector at p, or zeros when !ok.
+template <typename T, int VX>
+__device__ __forceinline__ void ldv_if(T (&d)[VX], const T *p, bool ok) {
+    if (ok) ldv_rw<T, VX>(d, p);
+    else zerov<T, VX>(d);
+}
+// Stores lanes [0, nv) of a vector (the whole vector when nv == VX).
+template <typename T, int VX>
+__device__ __forceinline__ void stv_n(T *p, const T (&s)[VX], int nv) {
+    if (nv == VX) {
+        stv<T, VX>(p, s);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VX; v++)
+            if (v < nv) p[v] = s[v];
+    }
+}
+// x taps of lane v from the vectors at i0 - VX (l), i0 (m), i0 + VX (r):
+// D+ order [u, u-1, u-2, u+1] and D order [u, u-1, u+1, u+2].  Indices are
+// clamped so that no branch names an element outside its vector.
+template <typename T, int VX>
+__device__ __forceinline__ void xtaps_p(const T (&l)[VX], const T (&m)[VX], const T (&r)[VX], int v, T (&t)[4]) {
+    t[0] = m[v];
+    t[1] = v >= 1 ? m[v >= 1 ? v - 1 : 0] : l[VX - 1];
+    t[2] = v >= 2 ? m[v >= 2 ? v - 2 : 0] : l[v < 2 ? VX - 2 + v : 0];
+    t[3] = v + 1 < VX ? m[v + 1 < VX ? v + 1 : 0] : r[0];
+}
+template <typename T, int VX>
+__device__ __forceinline__ void xtaps_m(const T (&l)[VX], const T (&m)[VX], const T (&r)[VX], int v, T (&t)[4]) {
+    t[0] = m[v];
+    t[1] = v >= 1 ? m[v >= 1 ? v - 1 : 0] : l[VX - 1];
+    t[2] = v + 1 < VX ? m[v + 1 < VX ? v + 1 : 0] : r[v + 1 >= VX ? v + 1 - VX : 0];
+    t[3] = v + 2 < VX ? m[v + 2 < VX ? v + 2 : 0] : r[v + 2 >= VX ? v + 2 - VX : 0];
+}
+
+template <typename T, int VX>
+__global__ void __launch_bounds__(128) adjv_h_gather_kernel(AdjArgs<T> a) {
+    int i0, j, k, shot;
+    if (!adjv_cell<VX>(i0, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i0;
+    const long long sy = a.px, sz = a.plane;
+    const int nv = min(VX, a.nx - i0);
+    // taps [u, u-1, u-2, u+1] along y and z; x from three whole vectors
+    const long long oy[4] = {0, -sy, -2 * sy, sy}, oz[4] = {0, -sz, -2 * sz, sz}, ox[3] = {-VX, 0, VX};
+    const bool vy[4] = {true, j >= 1, j >= 2, j + 1 < a.ny}, vz[4] = {true, k >= 1, k >= 2, k + 1 < a.nz};
+    const bool vx[3] = {i0 >= VX, true, i0 + VX < a.nx};
+    T y0[4][VX], z1[4][VX], z2[4][VX], y6[4][VX], x3[3][VX], x4[3][VX], x5[3][VX];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        ldv_if<T, VX>(y0[q], a.mu[0] + c + oy[q], vy[q]);
+        ldv_if<T, VX>(z1[q], a.mu[1] + c + oz[q], vz[q]);
+        ldv_if<T, VX>(z2[q], a.mu[2] + c + oz[q], vz[q]);
+        ldv_if<T, VX>(y6[q], a.mu[6] + c + oy[q], vy[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        ldv_if<T, VX>(x3[q], a.mu[3] + c + ox[q], vx[q]);
+        ldv_if<T, VX>(x4[q], a.mu[4] + c + ox[q], vx[q]);
+        ldv_if<T, VX>(x5[q], a.mu[5] + c + ox[q], vx[q]);
+    }
+    T lx[VX], ly[VX], lz[VX];
+    ldv_rw<T, VX>(lx, a.lam[0] + c);
+    ldv_rw<T, VX>(ly, a.lam[1] + c);
+    ldv_rw<T, VX>(lz, a.lam[2] + c);
+#pragma unroll
+    for (int v = 0; v < VX; v++) {
+        if (v >= nv) continue;
+        T t0[4], t1[4], t2[4], t3[4], t4[4], t5[4], t6[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) { t0[q] = y0[q][v]; t1[q] = z1[q][v]; t2[q] = z2[q][v]; t6[q] = y6[q][v]; }
+        xtaps_p<T, VX>(x3[0], x3[1], x3[2], v, t3);
+        xtaps_p<T, VX>(x4[0], x4[1], x4[2], v, t4);
+        xtaps_p<T, VX>(x5[0], x5[1], x5[2], v, t5);
+        h_gather_cell(a, i0 + v, j, k, t0, t1, t2, t3, t4, t5, t6, lx[v], ly[v], lz[v]);
+    }
+    stv_n<T, VX>(a.lam[0] + c, lx, nv);
+    stv_n<T, VX>(a.lam[1] + c, ly, nv);
+    stv_n<T, VX>(a.lam[2] + c, lz, nv);
+}
+
+template <typename T, int VX>
+__global__ void __launch_bounds__(128) adjv_e_gather_kernel(AdjArgs<T> a) {
+    int i0, j, k, shot;
+    if (!adjv_cell<VX>(i0, j, k, shot, a.nx, a.ny, a.nz)) return;
+    const long long c = (long long)shot * a.fshot + (long long)k * a.plane + (long long)j * a.px + i0;
+    const long long sy = a.px, sz = a.plane;
+    const int nv = min(VX, a.nx - i0);
+    // taps [u, u-1, u+1, u+2]
+    const long long oy[4] = {0, -sy, sy, 2 * sy}, oz[4] = {0, -sz, sz, 2 * sz}, ox[3] = {-VX, 0, VX};
+    const bool vy[4] = {true, j >= 1, j + 1 < a.ny, j + 2 < a.ny}, vz[4] = {true, k >= 1, k + 1 < a.nz, k + 2 < a.nz};
+    const bool vx[3] = {i0 >= VX, true, i0 + VX < a.nx};
+    T y0[4][VX], z1[4][VX], z2[4][VX], y5[4][VX], x3[3][VX], x4[3][VX];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        ldv_if<T, VX>(y0[q], a.mu[0] + c + oy[q], vy[q]);
+        ldv_if<T, VX>(z1[q], a.mu[1] + c + oz[q], vz[q]);
+        ldv_if<T, VX>(z2[q], a.mu[2] + c + oz[q], vz[q]);
+        ldv_if<T, VX>(y5[q], a.mu[5] + c + oy[q], vy[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        ldv_if<T, VX>(x3[q], a.mu[3] + c + ox[q], vx[q]);
+        ldv_if<T, VX>(x4[q], a.mu[4] + c + ox[q], vx[q]);
+    }
+    T lx[VX], ly[VX], lz[VX];
+    ldv_rw<T, VX>(lx, a.lam[3] + c);
+    ldv_rw<T, VX>(ly, a.lam[4] + c);
+    ldv_rw<T, VX>(lz, a.lam[5] + c);
+#pragma unroll
+    for (int v = 0; v < VX; v++) {
+        if (v >= nv) continue;
+        T t0[4], t1[4], t2[4], t3[4], t4[4], t5[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) { t0[q] = y0[q][v]; t1[q] = z1[q][v]; t2[q] = z2[q][v]; t5[q] = y5[q][v]; }
+        xtaps_m<T, VX>(x3[0], x3[1], x3[2], v, t3);
+        xtaps_m<T, VX>(x4[0], x4[1], x4[2], v, t4);
+        e_gather_cell(a, i0 + v, j, k, t0, t1, t2, t3, t4, t5, lx[v], ly[v], lz[v]);
+    }
+    stv_n<T, VX>(a.lam[3] + c, lx, nv);
+    stv_n<T, VX>(a.lam[4] + c, ly, nv);
+    stv_n<T, VX>(a.lam[5] + c, lz, nv);
 }
 
 // ---------------------------------------------------------------- sources

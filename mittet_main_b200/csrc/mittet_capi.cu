@@ -1324,6 +1324,12 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         ae.sgn = (T)h->ph.e_sign;
         for (int c = 0; c < 7; c++) { ah.mu[c] = mu[c].as<T>(); ae.mu[c] = mu[c].as<T>(); }
         const dim3 ablk(32, 8), agrd((h->g.nx + 31) / 32, (h->g.ny + 7) / 8, h->g.nz * Gg);
+        // gathers: AVX x cells per thread (MITTET_ADJ_GATHER=cell: one per
+        // thread, bit-identical)
+        constexpr int AVX = sizeof(T) == 4 ? 4 : 2;
+        const char *gmode = std::getenv("MITTET_ADJ_GATHER");
+        const bool gather_cell = gmode && std::string(gmode) == "cell";
+        const dim3 vblk(32, 4), vgrd((h->g.nx + 32 * AVX - 1) / (32 * AVX), (h->g.ny + 3) / 4, h->g.nz * Gg);
         const T *H = hist.as<T>();
         const size_t slot = 6 * gF;
         for (int seg = ncheck - 1; seg >= 0; seg--) {
@@ -1387,13 +1393,15 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
                                                           nrec, Gg, h->fshot, asrc, nt, n, 1);
                 if (hm) adj_src_kernel<T><<<(int)(asp.size() + 63) / 64, 64, 0, h->st>>>(ah, d_asp.as<AdjSrc>(), (int)asp.size(), h->wave.as<double>(), n, 0, s0, s1);
                 adj_h_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
-                adj_h_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
+                if (gather_cell) adj_h_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
+                else adjv_h_gather_kernel<T, AVX><<<vgrd, vblk, 0, h->st>>>(ah);
                 adj_inject_kernel<T><<<4, 256, 0, h->st>>>(aa.lam[0], aa.lam[1], aa.lam[2], aa.lam[3], aa.lam[4],
                                                           aa.lam[5], h->rec_off.as<long long>(), h->rec_comp.as<int>(),
                                                           nrec, Gg, h->fshot, asrc, nt, n, 0);
                 if (he) adj_src_kernel<T><<<(int)(asp.size() + 63) / 64, 64, 0, h->st>>>(ae, d_asp.as<AdjSrc>(), (int)asp.size(), h->wave.as<double>(), n, 1, s0, s1);
                 adj_e_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
-                adj_e_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
+                if (gather_cell) adj_e_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
+                else adjv_e_gather_kernel<T, AVX><<<vgrd, vblk, 0, h->st>>>(ae);
             }
             CK(cudaGetLastError());
             if ((rc = gmark(2))) return rc;

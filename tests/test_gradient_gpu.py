@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from mittet_main_b200 import workloads as W
-from mittet_main_b200.capi import FLAVOR_SATAN_I, FP32, FP64, SRC_ELECTRIC, SRC_MAGNETIC
+from mittet_main_b200.capi import FLAVOR_NCVER0027, FLAVOR_SATAN_I, FP32, FP64, SRC_ELECTRIC, SRC_MAGNETIC
 from mittet_main_b200.solver import Shot
 from oracle import oracle as O
 from tests.conftest import rel_l2
@@ -231,3 +231,31 @@ def test_recompute_into_history_is_bit_identical(monkeypatch, prec):
     assert res["copy"][0] == pytest.approx(res["direct"][0], rel=1e-13)
     assert np.abs(res["copy"][1]).max() > 0
     assert np.array_equal(res["copy"][1], res["direct"][1])
+
+
+@pytest.mark.parametrize("prec,flavor,with_mu", [(FP32, FLAVOR_NCVER0027, False), (FP64, FLAVOR_SATAN_I, False),
+                                                 (FP32, FLAVOR_SATAN_I, True)])
+def test_vector_gathers_are_bit_identical(monkeypatch, prec, flavor, with_mu):
+    """The adjoint gathers with several x cells per thread (vector loads of
+    the weights) and with one cell per thread call the same per-cell
+    arithmetic, so the gradients agree bit for bit.  nx = 45 leaves a partial
+    vector at the end of every row; the two shots carry a magnetic and an
+    electric source."""
+    wl = W.small_case(n=(45, 34, 30), ncpml=6, nt=60, precision=prec, flavor=flavor, magnetic=True, seed=5)
+    wl = replace(wl, shots=[wl.shots[0], Shot(points=[(30, 12, 15, "ey", SRC_ELECTRIC, 0.8)])])
+    rng = np.random.default_rng(9)
+    if with_mu:
+        wl = replace(wl, mu=wl.cp.mu0 * (1.0 + 0.2 * rng.random(wl.sigma.shape)))
+    obs = (rng.normal(size=(2, len(wl.receivers), len(wl.omega)))
+           + 1j * rng.normal(size=(2, len(wl.receivers), len(wl.omega)))) * 1e-12
+    res = {}
+    for mode in ("cell", "vector"):
+        if mode == "cell":
+            monkeypatch.setenv("MITTET_ADJ_GATHER", "cell")
+        else:
+            monkeypatch.delenv("MITTET_ADJ_GATHER", raising=False)
+        with W.make_solver(wl) as s:
+            res[mode] = s.gradient(wl.nt, obs, checkpoint_every=25)
+    assert res["cell"][0] == pytest.approx(res["vector"][0], rel=1e-13)
+    assert np.abs(res["cell"][1]).max() > 0
+    assert np.array_equal(res["cell"][1], res["vector"][1])
