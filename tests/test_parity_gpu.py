@@ -106,6 +106,23 @@ def test_gpu_fp64_final_fields_match_oracle():
         assert rel_l2(G[c], F[c]) <= 1e-10, NAMES[c]
 
 
+@pytest.mark.parametrize("n,ncpml", [((16, 17, 16), 6), ((33, 17, 16), 6), ((37, 21, 19), 5)])
+@pytest.mark.parametrize("flavor", [FLAVOR_NCVER0027, FLAVOR_SATAN_I])
+def test_box_layout_edge_cases_match_oracle(n, ncpml, flavor):
+    """The smallest grids the CPML allows (2 ncpml + 4 cells per axis): no
+    interior box in x (every cell in the general body), an interior box of
+    three or four rows and planes, and odd sizes: final fields and traces
+    against the oracle (FP64, 1e-10)."""
+    wl = W.small_case(n=n, ncpml=ncpml, nt=60, precision=FP64, flavor=flavor, magnetic=True, seed=3)
+    tr, F = oracle_run(wl, want_fields=True)[0]
+    with W.make_solver(wl) as s:
+        _, td = s.forward(wl.nt, want_traces=True)
+        G = s.fields(0)
+    assert rel_l2(td[0], tr) <= 1e-10
+    for c in range(6):
+        assert rel_l2(G[c], F[c]) <= 1e-10, NAMES[c]
+
+
 def test_sign_flipped_bp_updates_match_oracle():
     wl = W.small_case(nt=120, precision=FP64)
     cp = replace(wl.cp, e_sign=-1, h_sign=-1, check_cfl=True)
