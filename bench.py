@@ -190,6 +190,8 @@ def main():
     ap.add_argument("--ref-seg-steps", type=int, default=4)
     ap.add_argument("--grid", default="", help="NXxNYxNZ override of the workload grid (profiling cases)")
     ap.add_argument("--no-volume", action="store_true", help="disable the full-volume f_to_d")
+    ap.add_argument("--shots", type=int, default=0, help="gradient: shots (0 = 16)")
+    ap.add_argument("--checkpoint", type=int, default=0, help="gradient: checkpoint interval (0 = 200)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

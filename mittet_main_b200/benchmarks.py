@@ -68,15 +68,17 @@ def gradient(args):
     from mittet_main_b200.capi import FP64, FP32
     prec = FP64 if args.precision == "fp64" else FP32
     nt = args.nt or 4000
-    true = W.gradient_case(nt=nt, precision=prec, true_model=True)
-    start = W.gradient_case(nt=nt, precision=prec, true_model=False)
+    nshot = getattr(args, "shots", 0) or 16
+    ck = getattr(args, "checkpoint", 0) or 200
+    true = W.gradient_case(nt=nt, precision=prec, true_model=True, nshot=nshot)
+    start = W.gradient_case(nt=nt, precision=prec, true_model=False, nshot=nshot)
     with W.make_solver(true) as s:
         obs, _ = s.forward(true.nt)
     with W.make_solver(start) as s:
-        s.gradient(start.nt, obs, 200)  # warm-up
+        s.gradient(start.nt, obs, ck)  # warm-up
         _sync()
         t0 = time.perf_counter()
-        J, G = s.gradient(start.nt, obs, 200)
+        J, G = s.gradient(start.nt, obs, ck)
         _sync()
         tg = time.perf_counter() - t0
         t0 = time.perf_counter()
@@ -86,7 +88,7 @@ def gradient(args):
     cells = start.ncell * start.nt * len(start.shots)
     nc = start.cp.ncpml
     body = G[nc:-nc, nc:-nc, nc:-nc]
-    return {"report": "gradient", "workload": start.name, "nt": start.nt, "shots": len(start.shots),
+    return {"report": "gradient", "workload": start.name, "nt": start.nt, "shots": len(start.shots), "checkpoint_every": ck,
             "seconds_per_gradient": tg, "seconds_per_forward": tf, "gradient_over_forward": tg / tf,
             "forward_equivalent_gcell_s": cells / tg / 1e9, "misfit": J,
             "grad_max_abs": float(np.abs(body).max())}

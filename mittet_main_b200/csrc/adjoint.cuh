@@ -183,8 +183,9 @@ __device__ __forceinline__ bool h_own_cell(const AdjArgs<T> &a, int i, int j, in
     for (int q = 0; q < 3; q++) {
         if (msh[q] == T(0)) continue;
         const double h = (double)msh[q] * (double)m;
-        const double dda = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
-        const double rdb = h * isig / (1.0 + h);
+        const double r = 1.0 / (1.0 + h);
+        const double dda = 2.0 * h * isig * r * r;
+        const double rdb = h * isig * r;
         const double h0 = (double)a.H0[q][c], h1 = (double)a.H1[q][c];
         const double d = in[q] ? fma(-(double)da[q], h0, h1) : h1 - h0;
         gsum = fma((double)L[q], fma(rdb, d, in[q] ? dda * h0 : 0.0), gsum);
@@ -355,9 +356,13 @@ __device__ __forceinline__ bool e_own_cell(const AdjArgs<T> &a, int i, int j, in
     const bool in[3] = {in0, in1, in2};
     double gsum = 0.0;
     for (int q = 0; q < 3; q++) {
+        // an axis without CPML profile (h = 0) gives dca = 0, rcb = -1/sigma
+        // exactly: skip its FP64 division
+        const bool prof = esh[q] != T(0);
         const double h = (double)esh[q] * (double)m;
-        const double dca = 2.0 * h * isig / ((1.0 + h) * (1.0 + h));
-        const double rcb = -isig / (1.0 + h);
+        const double r = prof ? 1.0 / (1.0 + h) : 1.0;
+        const double dca = prof ? 2.0 * h * isig * r * r : 0.0;
+        const double rcb = -isig * r;
         const double x0 = (double)e0[q], x1 = (double)e1[q];
         const double d = in[q] ? fma(-(double)ca[q], x0, x1) : x1 - x0;
         gsum = fma((double)L[q], fma(rcb, d, in[q] ? dca * x0 : 0.0), gsum);
