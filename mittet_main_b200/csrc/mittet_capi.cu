@@ -1131,6 +1131,7 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
     CK(cudaMemGetInfo(&freeb, &totb));
     const size_t budget = (size_t)(0.75 * (double)freeb);
     int G = (int)std::min<size_t>((size_t)ns, std::max<size_t>(1, budget / std::max<size_t>(per_shot, 1)));
+    if (const char *gcap = std::getenv("MITTET_GRAD_GROUP")) G = std::max(1, std::min(G, std::atoi(gcap)));
     if ((size_t)G * per_shot > budget) return fail(MITTET_ERR_OOM, "one shot of the gradient needs %zu bytes, %zu free", per_shot, freeb);
 
     DevBuf fl[6], pe[3][2], pH[3][2], hist, ck, lam[6], lpe[3][2], lph[3][2], mu[7], gacc, gred, d_gsrc;
