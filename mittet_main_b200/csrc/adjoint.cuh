@@ -96,6 +96,14 @@ __device__ __forceinline__ T dminus_v(T mc, T mm1, T mp1, T mp2, bool om, bool o
 // ---------------------------------------------------------------- H phase
 // mu[0] Dy+Ez, mu[1] Dz+Ey, mu[2] Dz+Ex, mu[3] Dx+Ez, mu[4] typo Dx Ez (psi_Hyx), mu[5] Dx+Ey, mu[6] Dy+Ex
 
+// Resident 256-thread blocks per SM asked of the own kernels: 6 in FP32
+// (40 registers, a few bytes of spill; latency-bound, they gain from the
+// extra warps: adjoint 6.5 -> 6.2 s), 4 in FP64 (more would spill heavily).
+template <typename T>
+constexpr int kOwnMinBlocks() {
+    return sizeof(T) == 4 ? 6 : 4;
+}
+
 // Own half of the transposed H update at one cell: from the adjoint L of H
 // after the phase and dt/mu, the seven weights mu and the adjoint of H
 // before the phase (lam); the cell's psi adjoints and gradient (CPML cells)
@@ -198,7 +206,7 @@ __device__ __forceinline__ bool h_own_cell(const AdjArgs<T> &a, int i, int j, in
 }
 
 template <typename T>
-__global__ void adj_h_own_kernel(AdjArgs<T> a) {
+__global__ void __launch_bounds__(256, kOwnMinBlocks<T>()) adj_h_own_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
     const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
@@ -375,7 +383,7 @@ __device__ __forceinline__ bool e_own_cell(const AdjArgs<T> &a, int i, int j, in
 }
 
 template <typename T>
-__global__ void adj_e_own_kernel(AdjArgs<T> a) {
+__global__ void __launch_bounds__(256, kOwnMinBlocks<T>()) adj_e_own_kernel(AdjArgs<T> a) {
     int i, j, k, shot;
     if (!adj_cell(i, j, k, shot, a.nx, a.ny, a.nz)) return;
     const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
