@@ -8,8 +8,10 @@
 //          adjoint weight mu of every derivative the phase used at that cell,
 //          the cell's gradient terms, and the adjoint of the phase input of
 //          its own field (lambda <- ca lambda, psi-adjoint <- b psi-adjoint);
-//   *_gather (one cell): adds the transposed (2,4) differences of those mu
-//          to the other field's adjoint, reading mu at the neighbours.
+//   *_gather: adds the transposed (2,4) differences of those mu to the
+//          other field's adjoint, reading mu at the neighbours (the gradient
+//          launches adjv_*_gather, several x cells per thread; adj_*_gather,
+//          one cell per thread, gives the same bits).
 // Adjoint step n (reverse of forward step n):
 //   inject a_H[n] -> lambda_H ; H_own ; H_gather (-> lambda_E) ;
 //   inject a_E[n] -> lambda_E ; source terms ; E_own ; E_gather (-> lambda_H).

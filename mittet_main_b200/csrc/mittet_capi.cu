@@ -874,7 +874,8 @@ int run_forward(mittet_handle *h, int nt) {
         h->tuned = true;
     }
     h->launches = 0;
-    // One graph holds G = ring_k steps (+ the volume flush when enabled).
+    // One graph holds G = ring_k steps; the volume flush of those steps (when
+    // enabled) is launched after each replay.
     const int G = h->ring_k;
     const long long key = ((long long)nt << 20) ^ ((long long)ns << 4) ^ (vol ? 1 : 0) ^ ((long long)h->nrec << 40);
     if (!h->gexec || h->graph_key != key) {
