@@ -184,6 +184,14 @@ int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double 
 int mittet_gradient(mittet_handle *h, int32_t nt, const double *obs, int32_t checkpoint_every,
                     double *misfit, double *grad);
 
+/* mittet_gradient keeps its work buffers (checkpoints, the segment history,
+ * adjoint state: about (K + 1) * 6 + 25 field volumes per shot of a group)
+ * in the handle for the next call, since an FWI loop calls it once per
+ * iteration and allocating them anew costs up to a second.  This frees them,
+ * e.g. before the handle serves other work.  No counterpart in the reference
+ * (whose arrays are static). */
+int mittet_release_gradient_buffers(mittet_handle *h);
+
 /* One satan_i model update after a gradient (fwi3d_cpu_inv_fwi_v1.4.c:85-107):
  *   calc_phi (fwi3d_cpu_function_v1.4.c:2565-2603): scaler = 0.01f * max sigma /
  *     max grad over the cells with 0-based k <= iseabed (both maxima start at

@@ -151,6 +151,30 @@ struct mittet_handle_s {
     bool tuned = false;
     DevBuf ring, acc;
     std::vector<double> wt_host;  // volume-DFT weights [n][f] (re, im)
+    // Work buffers of mittet_gradient, kept for the next call on this handle
+    // (an FWI loop calls it once per iteration; allocating and freeing ~100
+    // GB each time costs up to a second).  mittet_release_gradient_buffers
+    // frees them.
+    struct GradBufs {
+        DevBuf obs, R, mis, asrc, asp, fl[6], pe[3][2], pH[3][2], hist, ck, lam[6], lpe[3][2], lph[3][2], mu[7],
+            gacc, gred;
+        template <typename F>
+        void each(F f) {
+            for (DevBuf *b : {&obs, &R, &mis, &asrc, &asp, &hist, &ck, &gacc, &gred}) f(*b);
+            for (int c = 0; c < 6; c++) { f(fl[c]); f(lam[c]); }
+            for (int c = 0; c < 7; c++) f(mu[c]);
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 2; w++) { f(pe[a][w]); f(pH[a][w]); f(lpe[a][w]); f(lph[a][w]); }
+        }
+        size_t held() {
+            size_t n = 0;
+            each([&](DevBuf &b) { n += b.bytes; });
+            return n;
+        }
+        void release() {
+            each([](DevBuf &b) { b.release(); });
+        }
+    } gb;
 
     DevBuf fields[6], psiE[3][2], psiH[3][2];
     int alloc_shots = -1;
@@ -1057,7 +1081,14 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
     // MITTET_GRAD_LOG: device time of each stage (CUDA events on the handle's
     // stream, synchronised per stage) printed to stderr
     const bool glog = std::getenv("MITTET_GRAD_LOG") != nullptr;
-    cudaEvent_t gev[2] = {nullptr, nullptr};
+    struct EventPair {  // destroyed on every return
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~EventPair() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } gevs;
+    cudaEvent_t *gev = gevs.e;
     double gms[3] = {0, 0, 0};  // checkpoint pass, recompute, adjoint
     if (glog) {
         CK(cudaEventCreate(&gev[0]));
@@ -1093,7 +1124,8 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
     // group's residual and adjoint sources follow from it (no separate
     // forward).
     const size_t nspec = (size_t)ns * nrec * nf;
-    DevBuf d_obs, d_R, d_mis, d_asrc;
+    auto &B = h->gb;
+    DevBuf &d_obs = B.obs, &d_R = B.R, &d_mis = B.mis, &d_asrc = B.asrc;
     CK(d_obs.ensure(std::max<size_t>(nspec, 1) * sizeof(double2)));
     CK(d_R.ensure(std::max<size_t>(nspec, 1) * sizeof(double2)));
     CK(d_mis.ensure(sizeof(double)));
@@ -1117,7 +1149,7 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         a.g = p.kind == MITTET_SRC_MAGNETIC ? p.amp * h->ph.dt / (h->mu_h.empty() ? h->ph.mu0 : h->mu_h[c0]) / vol
                                             : p.amp * h->ph.dt * 2.0 * h->ph.omega0 / h->sigma_h[c0] / vol;
     }
-    DevBuf d_asp;
+    DevBuf &d_asp = B.asp;
     CK(d_asp.ensure(std::max<size_t>(asp.size(), 1) * sizeof(AdjSrc)));
     CK(cudaMemcpyAsync(d_asp.p, asp.data(), asp.size() * sizeof(AdjSrc), cudaMemcpyHostToDevice, h->st));
 
@@ -1130,12 +1162,15 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
                                       psiE + psiH + 6 * F + psiE + psiH + 7 * F) + 8 * F;
     size_t freeb = 0, totb = 0;
     CK(cudaMemGetInfo(&freeb, &totb));
-    const size_t budget = (size_t)(0.75 * (double)freeb);
+    const size_t budget = (size_t)(0.75 * (double)(freeb + B.held() - d_obs.bytes - d_R.bytes - d_mis.bytes -
+                                                   d_asrc.bytes - d_asp.bytes));
     int G = (int)std::min<size_t>((size_t)ns, std::max<size_t>(1, budget / std::max<size_t>(per_shot, 1)));
     if (const char *gcap = std::getenv("MITTET_GRAD_GROUP")) G = std::max(1, std::min(G, std::atoi(gcap)));
     if ((size_t)G * per_shot > budget) return fail(MITTET_ERR_OOM, "one shot of the gradient needs %zu bytes, %zu free", per_shot, freeb);
 
-    DevBuf fl[6], pe[3][2], pH[3][2], hist, ck, lam[6], lpe[3][2], lph[3][2], mu[7], gacc, gred, d_gsrc;
+    DevBuf(&fl)[6] = B.fl, (&lam)[6] = B.lam, (&mu)[7] = B.mu;
+    DevBuf(&pe)[3][2] = B.pe, (&pH)[3][2] = B.pH, (&lpe)[3][2] = B.lpe, (&lph)[3][2] = B.lph;
+    DevBuf &hist = B.hist, &ck = B.ck, &gacc = B.gacc, &gred = B.gred;
     const size_t gF = (size_t)G * F;
     for (int c = 0; c < 6; c++) { CK(fl[c].ensure(gF * h->esz)); CK(lam[c].ensure(gF * h->esz)); }
     for (int c = 0; c < 7; c++) CK(mu[c].ensure(gF * h->esz));
@@ -1425,12 +1460,9 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
     CK(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaMemcpyAsync(&mis, d_mis.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    if (glog) {
+    if (glog)
         fprintf(stderr, "gradient stages (ms): checkpoint pass %.1f, recompute %.1f, adjoint %.1f\n", gms[0], gms[1],
                 gms[2]);
-        cudaEventDestroy(gev[0]);
-        cudaEventDestroy(gev[1]);
-    }
     if (flag & 2) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded wait for a TMA copy gave up");
     if (flag) return fail(MITTET_ERR_DIVERGED, "non-finite receiver samples (unstable time step or model)");
     *misfit_out = mis;
@@ -1982,6 +2014,15 @@ int mittet_time_kernels(mittet_handle *h, int32_t nsteps, double *ms) {
     rc = h->fp64 ? time_kernels<double>(h, nsteps, ms) : time_kernels<float>(h, nsteps, ms);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->st));
+    return MITTET_OK;
+}
+
+int mittet_release_gradient_buffers(mittet_handle *h) {
+    if (!h) return fail(MITTET_ERR_INVALID_ARG, "null handle");
+    int rc = set_device(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    h->gb.release();
     return MITTET_OK;
 }
 

@@ -92,7 +92,12 @@ def run_request(solver_cache: dict, req: Request):
     s.set_freqs(wl.omega)
     s.set_volume_dft(wl.volume_dft) if wl.volume_dft else s.set_volume_dft("")
     if req.mode == "gradient":
-        return s.gradient(wl.nt, req.obs, req.checkpoint_every)
+        try:
+            return s.gradient(wl.nt, req.obs, req.checkpoint_every)
+        finally:
+            # the admission estimate counts the gradient buffers for this
+            # request only: hand them back before the slot takes other work
+            s.release_gradient_buffers()
     spec, _ = s.forward(wl.nt)
     return spec
 

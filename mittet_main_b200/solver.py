@@ -242,6 +242,10 @@ class MittetSolver:
         check(self._lib.mittet_gradient(self._h, nt, _dptr(o), checkpoint_every, _dptr(misfit), _dptr(grad)))
         return float(misfit[0]), grad
 
+    def release_gradient_buffers(self):
+        """Free the work buffers ``gradient`` keeps on the device for its next call."""
+        check(self._lib.mittet_release_gradient_buffers(self._h))
+
     def fwi_update(self, nt: int, obs: np.ndarray, ecal: np.ndarray, grad: np.ndarray, sigma: np.ndarray,
                    iseabed: int, minval: float, maxval: float):
         """satan_i's model update (calc_phi, trial forward, calc_alpha,

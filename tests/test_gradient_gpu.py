@@ -279,3 +279,17 @@ def test_shot_groups_give_the_same_gradient(monkeypatch):
     assert res["one"][0] == pytest.approx(res["both"][0], rel=1e-13)
     assert np.abs(res["both"][1]).max() > 0
     assert rel_l2(res["one"][1], res["both"][1]) <= 1e-14
+
+
+def test_gradient_buffers_are_kept_and_released():
+    """The handle keeps the gradient's work buffers for the next call; a call
+    after mittet_release_gradient_buffers allocates them again.  All three
+    calls give the same gradient."""
+    wl, obs = case(FP64, nt=70)
+    with W.make_solver(wl) as s:
+        J1, G1 = s.gradient(wl.nt, obs, checkpoint_every=20)
+        J2, G2 = s.gradient(wl.nt, obs, checkpoint_every=20)
+        s.release_gradient_buffers()
+        J3, G3 = s.gradient(wl.nt, obs, checkpoint_every=20)
+    assert J1 == pytest.approx(J2, rel=1e-13) and J1 == pytest.approx(J3, rel=1e-13)
+    assert np.array_equal(G1, G2) and np.array_equal(G1, G3)
