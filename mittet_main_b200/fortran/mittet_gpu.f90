@@ -127,6 +127,13 @@ module mittet_gpu
             real(c_double), intent(out) :: grad(*)
         end function
 
+        ! frees the work buffers mittet_gradient keeps in the handle for its next call
+        integer(c_int) function mittet_release_gradient_buffers(handle) &
+                bind(c, name="mittet_release_gradient_buffers")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: handle
+        end function
+
         ! satan_i model update (calc_phi, trial forward, calc_alpha, update_para2):
         ! obs, ecal: complex(c_double_complex) (nf, nrec, nshot); grad, sigma: (nx, ny, nz);
         ! step(1) = scaler, step(2) = alpha; sigma is updated in place.
