@@ -107,18 +107,27 @@ def stencil_bytes(wl, esz):
     return b * len(wl.shots)
 
 
-def e_phase_traffic(wl, esz):
-    """DRAM bytes of one E-phase launch set, from the committed ncu capture of
-    the same kernels (bytes per cell of the 256x256x96 twin, scaled by the
-    cells of this launch).  Only FP32 fields with the 3-component volume DFT
-    were captured; other configurations return None."""
+def stencil_read_bytes(wl, esz):
+    """Algorithmic read bytes of one E-phase launch: 6 fields and the model
+    word per cell, 2 psi per cell of each E slab group."""
+    cp = wl.cp
+    n = cp.nx * cp.ny * cp.nz
+    nc = cp.ncpml
+    slab_cells = 2 * (nc - 1) * (cp.ny * cp.nz + cp.nx * cp.nz + cp.nx * cp.ny)
+    return (7 * esz * n + 2 * esz * slab_cells) * len(wl.shots)
+
+
+def e_phase_profile(esz, volume):
+    """DRAM read bytes per cell of the E-phase kernels from the committed ncu
+    summary (a one-pass capture of every E-phase launch of a step of the
+    256x256x96 twin, FP32 fields with the 3-component volume DFT); None for
+    other configurations."""
     import re
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                        "plain_gpu_256x256x192_launches_and_dram.md")
-    if esz != 4 or wl.volume_dft != "xyz" or not os.path.exists(path):
+    path = os.path.join(ROOT, "profiles", "e_phase_dram_256x256x96.md")
+    if esz != 4 or volume != "xyz" or not os.path.exists(path):
         return None
-    m = re.search(r"e_phase_dram_bytes_per_cell:\s*([0-9.]+)", open(path).read())
-    return float(m.group(1)) * wl.ncell * len(wl.shots) if m else None
+    m = re.search(r"e_phase_dram_read_bytes_per_cell:\s*([0-9.]+)", open(path).read())
+    return {"read": float(m.group(1)), "source": "profiles/e_phase_dram_256x256x96.md"} if m else None
 
 
 def run_cpu_baseline(wl, budget_s=12.0):
@@ -158,7 +167,8 @@ def run_reference(args, wl):
     t = float(np.sum(timed))
     ncell = cp.nx * cp.ny * cp.nz
     value = ncell * seg * args.steps / t / 1e9
-    sample = (f"satan_i e/h_field_cpml42 + e/hpml_abcs4 (gcc -O2 -fopenmp, {threads} threads), "
+    sample = (f"satan_i e/h_field_cpml42 + e/hpml_abcs4 (gcc -fopenmp -O3 as satan_i/Makefile:12, "
+              f"{threads} threads), "
               f"{cp.nx}x{cp.ny}x{cp.nz} grid, {seg} time steps per bench step")
     return {
         "metric": "Gcell/s", "value": value, "unit": "Gcell/s", "impl": "reference",
@@ -187,6 +197,8 @@ def main():
     ap.add_argument("--nt", type=int, default=0, help="override Nt (0 = workload default)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 sub-record")
+    ap.add_argument("--no-batching", action="store_true", help="skip the batched-vs-one-at-a-time sub-record")
     ap.add_argument("--ref-seg-steps", type=int, default=4)
     ap.add_argument("--grid", default="", help="NXxNYxNZ override of the workload grid (profiling cases)")
     ap.add_argument("--no-volume", action="store_true", help="disable the full-volume f_to_d")
@@ -238,32 +250,7 @@ def main():
     nrec = len(wl.receivers)
     out = torch.zeros((len(wl.shots), nrec, nf, 2), dtype=torch.float64, device=f"cuda:{dev}")
     stream = torch.cuda.current_stream()
-
-    for _ in range(args.warmup):
-        solver.forward_device(wl.nt, out, stream)
-    torch.cuda.synchronize()
-    launches0 = solver.launch_count()
-
-    sampler = ClockSampler(dev)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        solver.forward_device(wl.nt, out, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    if dist:
-        dist.barrier()
-    t_ms = e0.elapsed_time(e1)
-    t = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{dev}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_ms = float(t.item())
+    t_ms, launches0, clocks = timed_solves(solver, wl, args.steps, args.warmup, dist, dev, out, stream)
     cells = wl.cell_updates()
     total_cells = cells * args.steps * world
     value = total_cells / (t_ms / 1e3) / 1e9
@@ -272,10 +259,8 @@ def main():
     # per-kernel device times (CUDA events on the launching stream) for the roofline
     kt = solver.time_kernels(min(64, wl.nt))
     esz = 8 if prec == FP64 else 4
-    ebytes = stencil_bytes(wl, esz)
-    e_ms = kt["e_phase"]
-    achieved = ebytes / (e_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
+    roof = roofline(wl, esz, kt, peak, peak_kind)
 
     # end to end through the public C ABI with host buffers
     e2e = None
@@ -309,6 +294,34 @@ def main():
         te = float(te.item())
         e2e = {"value": total_cells / te / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h}
+    stencil_variant = solver.tuned_variant()
+    solver.close()
+
+    extras = {}
+    if rank == 0 and world == 1:
+        # the same workload with FP64 fields (the reference's precision)
+        if not args.no_fp64 and prec == FP32:
+            wl64 = replace(wl, cp=replace(wl.cp, precision=FP64))
+            s64 = W.make_solver(wl64)
+            out64 = torch.zeros_like(out)
+            st64, sw64 = max(1, min(args.steps, 2)), 1
+            t64, l64, c64 = timed_solves(s64, wl64, st64, sw64, None, dev, out64, stream)
+            kt64 = s64.time_kernels(min(64, wl.nt))
+            s64.close()
+            extras["fp64"] = {"value": cells * st64 / (t64 / 1e3) / 1e9, "unit": "Gcell/s", "steps": st64,
+                              "warmup": sw64, "ms_per_step": t64 / st64, "kernel_ms": kt64,
+                              "roofline": roofline(wl64, 8, kt64, peak, peak_kind), "clocks": c64}
+        # batched against one at a time on the small serving grids (32 shots,
+        # Nt scaled with the grid as in the serving mix)
+        if not args.no_batching:
+            from mittet_main_b200.benchmarks import batching_ratio
+            rows = {}
+            for g in (64, 96):
+                bw = W.serving_case(g, g, g, 32, int(6000 * g / 256))
+                rows[f"{g}^3x32"] = batching_ratio(bw, repeats=2)
+            extras["batched_vs_one_at_a_time"] = {
+                "value": rows["64^3x32"]["batched_vs_one_at_a_time"], "workload": "64^3, 32 shots, Nt 1500",
+                "metric": "shot-solves/s batched / one shot at a time", "runs": rows}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -331,18 +344,68 @@ def main():
             "shot_solves_per_s": len(wl.shots) * args.steps * world / (t_ms / 1e3),
             "gpu_launches": gpu_launches,
             "kernel_ms": kt,
-            "stencil_variant": solver.tuned_variant(),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": e_phase_traffic(wl, esz), "kernel": "E phase (e_part_kernel x5 / interior_tma_kernel)",
-                         "alg_bytes_per_launch": ebytes, "peak_source": peak_kind},
+            "stencil_variant": stencil_variant,
+            "roofline": roof,
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            **extras,
         }
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist:
         dist.destroy_process_group()
+
+
+def timed_solves(solver, wl, steps, warmup, dist, dev, out, stream):
+    """W untimed solves, then K solves bracketed by a barrier and a device
+    synchronisation, timed with CUDA events on the launching stream (max over
+    ranks).  Returns (ms for the K solves, kernel launches per solve, clocks)."""
+    import torch
+    for _ in range(warmup):
+        solver.forward_device(wl.nt, out, stream)
+    torch.cuda.synchronize()
+    launches = solver.launch_count()
+    sampler = ClockSampler(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        solver.forward_device(wl.nt, out, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{dev}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), launches, clocks
+
+
+def roofline(wl, esz, kt, peak, peak_kind):
+    """HBM roofline of the E phase (the largest kernel group): algorithmic
+    bytes per launch over its CUDA-event time, against the measured copy
+    bandwidth, with the DRAM reads per cell of the profiled E-phase kernels."""
+    ebytes = stencil_bytes(wl, esz)
+    achieved = ebytes / (kt["e_phase"] / 1e3) / 1e9
+    cells = wl.ncell * len(wl.shots)
+    alg_reads = stencil_read_bytes(wl, esz) / cells
+    prof = e_phase_profile(esz, wl.volume_dft)
+    r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+         "kernel": "E phase (e_part_kernel parts / interior_tma_kernel)", "alg_bytes_per_launch": ebytes,
+         "alg_read_bytes_per_cell": alg_reads, "peak_source": peak_kind, "traffic": None}
+    if prof:
+        r["read_bytes_per_cell"] = prof["read"]
+        r["read_amplification"] = prof["read"] / alg_reads
+        # DRAM writes of a kernel are partly flushed from L2 during later
+        # kernels, so the algorithmic writes stand in for them
+        r["traffic"] = prof["read"] * cells + (ebytes - stencil_read_bytes(wl, esz))
+        r["traffic_source"] = prof["source"] + " (reads, per cell x cells) + algorithmic writes"
+    return r
 
 
 if __name__ == "__main__":

@@ -212,6 +212,29 @@ int mittet_release_gradient_buffers(mittet_handle *h);
 int mittet_fwi_update(mittet_handle *h, int32_t nt, const double *obs, const double *ecal, const double *grad,
                       int32_t iseabed, double minval, double maxval, double *sigma, double *step);
 
+/* satan_i's frequency-domain gradient formula, evaluated on GPU `device`
+ * in one pass over the cells (replaces residualE, sensitivity, conv_GdelE
+ * and calc_gamma, satan_i/fwi3d_cpu_function_v1.4.c:2202-2384).  All
+ * complex arrays are interleaved (re, im) doubles, cells x fastest
+ * (n = nx*ny*nz), frequency index w = 0 .. nf-1 (satan_i's upperF = nf):
+ *   rec_pos: [nrec][3] 1-based receiver cells (model_env.dat positions)
+ *   obs:     [3 comp][nrec][nf]        Exobs, Eyobs, Ezobs
+ *   e_ff:    [3 comp][nf][n]           EcalX_ff, EcalY_ff, EcalZ_ff
+ *   e_bb:    [3 comp][nrec][3 dir][nf][n]  EcalX_bb, EcalY_bb, EcalZ_bb
+ * Outputs (each may be NULL except grad):
+ *   err_sum: sum |dE| over receivers, frequencies and x, y, z (residualE)
+ *   de:      [3 dir][nrec][nf]  delEx_f, delEy_f, delEz_f = obs - e_ff at the
+ *            receiver; with obs = NULL it is an input instead: the residual
+ *            itself (residualE skipped)
+ *   sense:   [n]  sum over rec, dir, w, comp of |e_ff e_bb|
+ *   e_back:  [3 comp][nf][n]  sum over rec, dir of e_bb conj(de)
+ *   grad:    [n]  in/out: += Re sum_w sum_c e_ff e_back (divided by sense
+ *            when normalize = 1, as calc_gamma does) on [ncpml, n - ncpml)
+ *            per axis; untouched elsewhere. */
+int mittet_satan_gamma(int32_t device, const mittet_grid *grid, int32_t nrec, const int32_t *rec_pos, int32_t nf,
+                       const double *obs, const double *e_ff, const double *e_bb, int32_t normalize,
+                       double *err_sum, double *de, double *sense, double *e_back, double *grad);
+
 /* Device-resident variants for callers that keep data on the GPU (the
  * PyTorch front end).  Pointers are device pointers of the handle's device;
  * stream is the caller's cudaStream_t (NULL = the legacy default stream): the
@@ -252,16 +275,20 @@ int64_t mittet_last_launch_count(mittet_handle *h);
 /* Forward solve that allocates no device memory.  No counterpart in the
  * reference (whose Fortran/C drivers own static arrays); it exists for hosts
  * that cannot call cudaMalloc/cudaFree: cudaFree synchronises the whole
- * device and stalls other streams of a serving process, code running during
- * stream capture may not allocate, and some hosts' device memory belongs to
- * another allocator.  Every intermediate buffer lives in one file-scope
- * __device__ array of 32 MiB that each GPU loading the library keeps until
- * exit; a solve whose padded layout does not fit (about 96^3 cells with a few
- * hundred receivers for a few thousand steps), or with more than 256 cells
- * on an axis, 64 points, 2048 receivers or 256 frequencies, is rejected with
- * MITTET_ERR_INVALID_ARG.  FP32 fields with an FP64 f_to_d, one shot (every
- * point has shot 0), uniform permeability phys->mu0.
- *   sigma_dev:   device, nx*ny*nz doubles, x fastest
+ * device and stalls the other streams of a serving process, and some hosts'
+ * device memory belongs to another allocator.  Every intermediate buffer
+ * lives in one file-scope __device__ array of 32 MiB that each GPU loading
+ * the library keeps until exit; a solve whose padded layout does not fit
+ * (about 96^3 cells with a few hundred receivers for a few thousand steps),
+ * or with more than 256 cells on an axis, 64 points, 2048 receivers or 256
+ * frequencies, is rejected with MITTET_ERR_INVALID_ARG.  FP32 fields with an
+ * FP64 f_to_d, one shot (every point has shot 0), uniform permeability
+ * phys->mu0.
+ *   sigma_dev:   device, nx*ny*nz doubles, x fastest; every value must be
+ *                positive and finite: unlike mittet_set_model this call does
+ *                not read the model back to check it, and it runs no
+ *                finite check on the result (a bad model or an unstable dt
+ *                gives Inf/NaN spectra, not MITTET_ERR_DIVERGED)
  *   wavelet_dev: device, nt+1 doubles, w[n] = s(n dt)
  *   pts, rec, omega: host arrays (copied into the device array)
  *   rec_fd_dev:  device output, [nrec][nf] complex (interleaved doubles)

@@ -26,6 +26,43 @@ def _sync():
     torch.cuda.synchronize()
 
 
+def batching_ratio(wl, repeats: int = 1) -> dict:
+    """All shots of ``wl`` in one batched solve against the same shots solved
+    one at a time (mittet_set_sources + mittet_forward per shot) on the same
+    GPU; best of ``repeats`` timed runs of each after a warm-up."""
+    ns = len(wl.shots)
+    from mittet_main_b200 import workloads as W
+    tb = float("inf")
+    with W.make_solver(wl) as s:
+        s.forward(wl.nt)  # warm-up (autotune, graph)
+        for _ in range(repeats):
+            _sync()
+            t0 = time.perf_counter()
+            spec_b, _ = s.forward(wl.nt)
+            _sync()
+            tb = min(tb, time.perf_counter() - t0)
+    one = replace(wl, shots=[wl.shots[0]])
+    tp = float("inf")
+    with W.make_solver(one) as s:
+        s.forward(wl.nt)
+        for _ in range(repeats):
+            _sync()
+            t0 = time.perf_counter()
+            specs = []
+            for k in range(ns):
+                s.set_shots([wl.shots[k]])
+                sp, _ = s.forward(wl.nt)
+                specs.append(sp[0])
+            _sync()
+            tp = min(tp, time.perf_counter() - t0)
+    same = all(np.array_equal(spec_b[k], specs[k]) for k in range(ns))
+    cells = wl.ncell * wl.nt
+    return {"workload": wl.name, "nt": wl.nt, "shots": ns,
+            "batched_shot_solves_per_s": ns / tb, "one_at_a_time_shot_solves_per_s": ns / tp,
+            "batched_vs_one_at_a_time": tp / tb, "batched_gcell_s": ns * cells / tb / 1e9,
+            "one_at_a_time_gcell_s": ns * cells / tp / 1e9, "identical_results": bool(same)}
+
+
 def batching(args):
     from mittet_main_b200 import workloads as W
     from mittet_main_b200.capi import FP64, FP32
@@ -34,33 +71,10 @@ def batching(args):
     kw = {}
     if args.grid:
         kw["nx"], kw["ny"], kw["nz"] = (int(v) for v in args.grid.split("x"))
+    if getattr(args, "shots", 0):
+        kw["nshot"] = args.shots
     wl = W.batched(nt=nt, precision=prec, **kw)
-    ns = len(wl.shots)
-    with W.make_solver(wl) as s:
-        s.forward(wl.nt)  # warm-up (autotune, graph)
-        _sync()
-        t0 = time.perf_counter()
-        spec_b, _ = s.forward(wl.nt)
-        _sync()
-        tb = time.perf_counter() - t0
-    one = replace(wl, shots=[wl.shots[0]])
-    with W.make_solver(one) as s:
-        s.forward(wl.nt)
-        _sync()
-        t0 = time.perf_counter()
-        specs = []
-        for k in range(ns):
-            s.set_shots([wl.shots[k]])
-            sp, _ = s.forward(wl.nt)
-            specs.append(sp[0])
-        _sync()
-        tp = time.perf_counter() - t0
-    same = all(np.array_equal(spec_b[k], specs[k]) for k in range(ns))
-    cells = wl.ncell * wl.nt
-    return {"report": "batching", "workload": wl.name, "nt": wl.nt, "shots": ns,
-            "batched_shot_solves_per_s": ns / tb, "plain_shot_solves_per_s": ns / tp,
-            "speedup": tp / tb, "batched_gcell_s": ns * cells / tb / 1e9, "plain_gcell_s": ns * cells / tp / 1e9,
-            "identical_results": bool(same)}
+    return {"report": "batching", **batching_ratio(wl)}
 
 
 def gradient(args):

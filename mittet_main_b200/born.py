@@ -44,12 +44,65 @@ from .solver import Shot, f_to_d
 _DIRS = ("ex", "ey", "ez")
 
 
+def satan_gamma(nx: int, ny: int, nz: int, ncpml: int, rec_pos, obs, e_ff, e_bb, normalize: bool = True,
+                grad=None, residual=None, device: int = 0) -> dict:
+    """satan_i's residualE + sensitivity + conv_GdelE + calc_gamma
+    (fwi3d_cpu_function_v1.4.c:2202-2384) in one GPU pass
+    (``mittet_satan_gamma``).  Arrays in satan_i's layouts, cells [nz, ny, nx]:
+
+      rec_pos [nrec, 3] 1-based;  obs [3, nrec, nf];  e_ff [3, nf, nz, ny, nx];
+      e_bb [3 comp, nrec, 3 dir, nf, nz, ny, nx]
+
+    Returns dict(err_sum, de [3, nrec, nf], sense [nz, ny, nx],
+    e_back [3, nf, nz, ny, nx], grad [nz, ny, nx]); grad is ``grad`` (or
+    zeros) plus this call's gamma, inside [ncpml, n - ncpml) only.  With
+    ``obs=None`` the residual [3, nrec, nf] is given as ``residual`` instead
+    of being formed from obs (residualE skipped)."""
+    import ctypes
+
+    from . import capi
+
+    def cbuf(a, shape):
+        a = np.asarray(a, dtype=np.complex128).reshape(shape)
+        return np.ascontiguousarray(a).view(np.float64)
+
+    nrec = int(np.asarray(rec_pos).reshape(-1, 3).shape[0]) if len(rec_pos) else 0
+    e_ff = np.asarray(e_ff)
+    nf = e_ff.shape[1]
+    n = nx * ny * nz
+    pos = np.ascontiguousarray(np.asarray(rec_pos, dtype=np.int32).reshape(-1, 3))
+    o = cbuf(obs, (3, nrec, nf)) if (nrec and obs is not None) else None
+    ff = cbuf(e_ff, (3, nf, n))
+    bb = cbuf(e_bb, (3, nrec, 3, nf, n)) if nrec else np.zeros(2)
+    g = np.zeros(n) if grad is None else np.array(grad, dtype=np.float64).reshape(n)
+    err = np.zeros(1)
+    de = np.zeros(3 * max(nrec, 1) * nf * 2)
+    if o is None and nrec:  # the residual itself is given
+        de[: 3 * nrec * nf * 2] = cbuf(residual, (3, nrec, nf))
+    sense = np.zeros(n)
+    back = np.zeros(3 * nf * n * 2)
+    D = ctypes.POINTER(ctypes.c_double)
+    dp = lambda a: a.ctypes.data_as(D)  # noqa: E731
+    grid = capi.Grid(nx, ny, nz, 1.0, 1.0, 1.0, ncpml)
+    capi.check(capi.load().mittet_satan_gamma(device, ctypes.byref(grid), nrec,
+                                              pos.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), nf, dp(o) if o is not None else None, dp(ff),
+                                              dp(bb), 1 if normalize else 0, dp(err), dp(de), dp(sense), dp(back),
+                                              dp(g)))
+    cplx = lambda a: a[0::2] + 1j * a[1::2]  # noqa: E731
+    return {"err_sum": float(err[0]), "de": cplx(de)[: 3 * nrec * nf].reshape(3, nrec, nf),
+            "sense": sense.reshape(nz, ny, nx), "e_back": cplx(back).reshape(3, nf, nz, ny, nx),
+            "grad": g.reshape(nz, ny, nx)}
+
+
 def satan_formula_gradient(wl, obs: np.ndarray, normalize: bool = False, shot: int = 0, current_factor: bool = True):
     """Born gradient of one shot of workload ``wl`` (satan_i calc_gamma form).
 
     obs: [nshot, nrec, nf] observed spectra at wl.receivers / wl.omega.
     Returns (grad [nz, ny, nx], ecal [nrec, nf]).  Only electric receivers
-    contribute, as in satan_i."""
+    contribute, as in satan_i.  The reduction over receivers, directions and
+    frequencies is ``satan_gamma`` (the GPU kernel pinned to satan_i's own
+    functions) with E_ff = E / J_w, E_bb = the dipole spectra and
+    dE = the residual of each receiver's component."""
     from . import workloads as W
 
     cp = wl.cp
@@ -65,37 +118,31 @@ def satan_formula_gradient(wl, obs: np.ndarray, normalize: bool = False, shot: i
         if comp in _DIRS and (x, y, z) not in positions:
             positions.append((x, y, z))
     index = {(r[0], r[1], r[2], r[3]): q for q, r in enumerate(wl.receivers)}
-    shots, weights = [], []
-    for (x, y, z) in positions:
-        for d in _DIRS:
-            q = index.get((x, y, z, d))
-            if q is None:
-                continue
-            shots.append(Shot(points=[(x, y, z, d, SRC_ELECTRIC, 1.0)]))
-            weights.append(np.conj(dE[q]))  # [nf]
     nf = len(wl.omega)
-    eback = np.zeros_like(eff)
-    sense = np.zeros(eff.shape[2:]) if normalize else None
+    shots, slots = [], []
+    for p, (x, y, z) in enumerate(positions):
+        for d, name in enumerate(_DIRS):
+            if index.get((x, y, z, name)) is not None:
+                shots.append(Shot(points=[(x, y, z, name, SRC_ELECTRIC, 1.0)]))
+                slots.append((p, d))
+    jw = f_to_d(np.asarray(wl.wavelet[:wl.nt], dtype=np.float64)[None], cp.dt, cp.omega0, wl.omega,
+                h_factor=current_factor)[0]
+    nx, ny, nz = cp.nx, cp.ny, cp.nz
+    e_bb = np.zeros((3, len(positions), 3, nf, nz, ny, nx), dtype=np.complex128)
+    # the residual of each (position, direction); zero where no receiver
+    res = np.zeros((3, len(positions), nf), dtype=np.complex128)
     if shots:
         back = replace(wl, shots=shots, volume_dft="xyz")
         with W.make_solver(back) as s:
             s.forward(wl.nt)
-            for k, wgt in enumerate(weights):
+            for k, (p, d) in enumerate(slots):
                 for c, name in enumerate(_DIRS):
-                    g = s.volume_dft(k, name)  # [nf, nz, ny, nx]
-                    eback[c] += g * wgt[:, None, None, None]
-                    if normalize:
-                        sense += np.abs(eff[c] * g).sum(axis=0)
-    jw = f_to_d(np.asarray(wl.wavelet[:wl.nt], dtype=np.float64)[None], cp.dt, cp.omega0, wl.omega,
-                h_factor=current_factor)[0]
-    prod = (eff * eback).sum(axis=0)  # [nf, nz, ny, nx]
-    grad = np.real(prod / jw[:, None, None, None]).sum(axis=0) * (cp.dx * cp.dy * cp.dz)
-    if normalize:
-        grad = grad / np.where(sense > 0, sense, 1.0)
-    nc = cp.ncpml
-    out = np.zeros_like(grad)
-    out[nc:-nc, nc:-nc, nc:-nc] = grad[nc:-nc, nc:-nc, nc:-nc]
-    return out, ecal
+                    e_bb[c, p, d] = s.volume_dft(k, name)
+                res[d, p] = dE[index[(*positions[p], _DIRS[d])]]
+    e_ff = eff / jw[None, :, None, None, None]
+    pos = np.array(positions, dtype=np.int32).reshape(-1, 3)
+    r = satan_gamma(nx, ny, nz, cp.ncpml, pos, None, e_ff, e_bb, normalize=normalize, residual=res)
+    return r["grad"] * (1.0 if normalize else cp.dx * cp.dy * cp.dz), ecal
 
 
 def compare(g_ref: np.ndarray, g: np.ndarray) -> dict:

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmittet_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "mittet_capi.cu"), os.path.join(HERE, "csrc", "mittet_noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("mittet_capi.cu", "gamma.cu", "mittet_noalloc.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(ROOT, "include", "mittet.h")]
 

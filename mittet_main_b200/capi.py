@@ -102,6 +102,8 @@ SIGNATURES = {
     "mittet_gradient": (ctypes.c_int, [_VP, _I, _P(_D), _I, _P(_D), _P(_D)]),
     "mittet_release_gradient_buffers": (ctypes.c_int, [_VP]),
     "mittet_fwi_update": (ctypes.c_int, [_VP, _I, _P(_D), _P(_D), _P(_D), _I, _D, _D, _P(_D), _P(_D)]),
+    "mittet_satan_gamma": (ctypes.c_int, [_I, _P(Grid), _I, _P(_I), _I, _P(_D), _P(_D), _P(_D), _I, _P(_D),
+                                          _P(_D), _P(_D), _P(_D), _P(_D)]),
     "mittet_set_model_device": (ctypes.c_int, [_VP, _VP, _VP, _I]),
     "mittet_forward_device": (ctypes.c_int, [_VP, _I, _VP, _VP]),
     "mittet_time_kernels": (ctypes.c_int, [_VP, _I, _P(_D)]),

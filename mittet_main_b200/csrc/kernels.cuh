@@ -246,24 +246,24 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 //   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring(vc, shot*fshot + cell, s),
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
 // Grid (cells, component, shot), one thread per cell.  A thread issues its
-// 64 ring loads (one 128-byte line per warp each) before any arithmetic, forms
-// the sum over the ring in the field precision T (at most 64 terms; for FP32
-// fields the partial sum carries ~1e-7 relative error) and adds it to the FP64
-// accumulators once per flush.  The weights of one group of up to four
-// frequencies are a by-value kernel parameter (zero for s >= cnt), so every
-// multiply reads its weight from the constant bank.
+// 64 ring loads (one 128-byte line per warp each) before any arithmetic and
+// forms every product and partial sum in FP64 (the ring samples are exact in
+// FP64, the weights are FP64), so the whole transform is accumulated in FP64
+// whatever the field precision: the FP32 path's only DFT error is the
+// rounding of the field samples themselves.  The weights of one group of up
+// to four frequencies are a by-value kernel parameter (zero for s >= cnt), so
+// every multiply reads its weight from the constant bank.
 constexpr int kFlushRing = 64;
 constexpr int kFlushFreqs = 4;
-template <typename T>
 struct FlushWeights {
-    T wr[kFlushRing][kFlushFreqs];
-    T wi[kFlushRing][kFlushFreqs];
+    double wr[kFlushRing][kFlushFreqs];
+    double wi[kFlushRing][kFlushFreqs];
 };
 
 template <typename T>
 __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ ring, long long ring_comp, int ring_k,
                                                          int3 vcs, long long fshot, int cnt, int f0, int nf,
-                                                         const __grid_constant__ FlushWeights<T> w,
+                                                         const __grid_constant__ FlushWeights w,
                                                          double2 *__restrict__ acc) {
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= fshot) return;
@@ -274,23 +274,25 @@ __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ r
     T xs[kFlushRing];
 #pragma unroll
     for (int s = 0; s < kFlushRing; s++) xs[s] = s < cnt ? __ldcs(rp + s * kRingTile) : T(0);
-    T pr[kFlushFreqs], pi[kFlushFreqs];
+    double pr[kFlushFreqs], pi[kFlushFreqs];
 #pragma unroll
-    for (int f = 0; f < kFlushFreqs; f++) { pr[f] = T(0); pi[f] = T(0); }
+    for (int f = 0; f < kFlushFreqs; f++) { pr[f] = 0.0; pi[f] = 0.0; }
 #pragma unroll
-    for (int s = 0; s < kFlushRing; s++)
+    for (int s = 0; s < kFlushRing; s++) {
+        const double x = (double)xs[s];
 #pragma unroll
         for (int f = 0; f < kFlushFreqs; f++) {
-            pr[f] = fma(w.wr[s][f], xs[s], pr[f]);
-            pi[f] = fma(w.wi[s][f], xs[s], pi[f]);
+            pr[f] = fma(w.wr[s][f], x, pr[f]);
+            pi[f] = fma(w.wi[s][f], x, pi[f]);
         }
+    }
     double2 *__restrict__ ap = acc + (((long long)shot * 3 + vc) * nf + f0) * fshot + cell;
 #pragma unroll
     for (int f = 0; f < kFlushFreqs; f++)
         if (f0 + f < nf) {
             double2 v = ap[(long long)f * fshot];
-            v.x += (double)pr[f];
-            v.y += (double)pi[f];
+            v.x += pr[f];
+            v.y += pi[f];
             ap[(long long)f * fshot] = v;
         }
 }

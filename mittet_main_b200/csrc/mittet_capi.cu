@@ -140,6 +140,7 @@ struct mittet_handle_s {
     int var_h[kParts] = {0};   // x/y/z face and edge launches of each phase;
                                // var[0] = -1 - c selects TMA interior config c
     TmaMaps tma_maps[2];       // tensor maps of the E and H interior (current buffers)
+    int tma_spin = kMbarSpinLimit;  // polls before a TMA wait gives up (MITTET_TMA_SPIN_LIMIT)
     int tma_nown[2] = {0, 0};
     bool tma_ok = false;
     int ibox[2][6] = {{0}};    // interior box of each phase: lo xyz, hi xyz
@@ -563,6 +564,7 @@ int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a, cudaStre
     tl.ntx = (tl.x1 - tl.x0 + S::TX - 1) / S::TX;
     tl.nty = (tl.y1 - tl.y0 + S::TY - 1) / S::TY;
     tl.zc = c.zc;
+    tl.spin_limit = h->tma_spin;
     const int nzc = (tl.z1 - tl.z0 + c.zc - 1) / c.zc;
     const dim3 grid(tl.ntx * tl.nty * nzc, h->nshot), block(S::TX / 2, S::TY);
     const size_t smem = c.smem(e);
@@ -809,13 +811,13 @@ void launch_volume_flush(mittet_handle *h, int cnt, int n0) {
         if (h->vmask >> c & 1) vc[nvc++] = c;
     const dim3 grid((unsigned)((h->fshot + 255) / 256), nvc, h->nshot);
     for (int f0 = 0; f0 < nf; f0 += kFlushFreqs) {
-        FlushWeights<T> w;
+        FlushWeights w;
         memset(&w, 0, sizeof(w));
         for (int s = 0; s < cnt; s++)
             for (int f = 0; f < kFlushFreqs && f0 + f < nf; f++) {
                 const size_t q = ((size_t)(n0 + s) * nf + f0 + f) * 2;
-                w.wr[s][f] = (T)h->wt_host[q];
-                w.wi[s][f] = (T)h->wt_host[q + 1];
+                w.wr[s][f] = h->wt_host[q];
+                w.wi[s][f] = h->wt_host[q + 1];
             }
         volume_dft_kernel<T><<<grid, 256, 0, h->st>>>(h->ring.as<T>(), ring_comp_of((long long)h->nshot * h->fshot), h->ring_k,
                                                       make_int3(vc[0], vc[1], vc[2]), h->fshot, cnt, f0, nf, w,
@@ -1046,10 +1048,16 @@ int validate_ready(mittet_handle *h, int nt) {
 }
 
 // Upload the point sources with their per-point gain (depends on the model).
+// The captured step graph reads the points from d_pts at run time, so it
+// stays valid unless the buffer moves or the number or kinds of points
+// change (those are baked into the graph's launches).
 int upload_sources(mittet_handle *h) {
     if (!h->has_model || h->pts.empty()) return MITTET_OK;
     std::vector<SrcPoint> dp(h->pts.size());
     const double vol = h->g.dx * h->g.dy * h->g.dz;
+    const bool mag0 = h->has_mag, ele0 = h->has_ele;
+    const int npts0 = h->npts;
+    const void *buf0 = h->d_pts.p;
     h->has_mag = h->has_ele = false;
     for (size_t q = 0; q < h->pts.size(); q++) {
         const mittet_point_source &p = h->pts[q];
@@ -1071,7 +1079,7 @@ int upload_sources(mittet_handle *h) {
     CK(cudaMemcpyAsync(h->d_pts.p, dp.data(), dp.size() * sizeof(SrcPoint), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->npts = (int)dp.size();
-    drop_graph(h);
+    if (h->d_pts.p != buf0 || h->npts != npts0 || h->has_mag != mag0 || h->has_ele != ele0) drop_graph(h);
     return MITTET_OK;
 }
 
@@ -1589,6 +1597,9 @@ int mittet_create(const mittet_grid *g, const mittet_phys *ph, mittet_handle **o
     h->ph = *ph;
     h->fp64 = ph->precision == MITTET_FP64;
     h->esz = h->fp64 ? 8 : 4;
+    // MITTET_TMA_SPIN_LIMIT=<polls> shortens the bounded waits of the TMA
+    // interior, so that a test can make them give up (MITTET_ERR_DEVICE_TIMEOUT)
+    if (const char *sl = std::getenv("MITTET_TMA_SPIN_LIMIT")) h->tma_spin = std::max(0, std::atoi(sl));
     h->px = (g->nx + 31) / 32 * 32;
     h->plane = (long long)h->px * g->ny;
     h->fshot = h->plane * g->nz;
@@ -1674,12 +1685,16 @@ int mittet_set_model(mittet_handle *h, const double *sigma, const double *mu) {
         CK(cudaMemcpyAsync(dm.p, mu, n * 8, cudaMemcpyHostToDevice, h->st));
     }
     const size_t cb = (size_t)h->fshot * h->esz;
+    const void *m0 = h->m.p, *dm0 = h->dtmu.p;
     CK(h->m.ensure(cb));
     CK(cudaMemsetAsync(h->m.p, 0, cb, h->st));
     if (mu) {
         CK(h->dtmu.ensure(cb));
         CK(cudaMemsetAsync(h->dtmu.p, 0, cb, h->st));
     }
+    // the step graph reads the model words at run time: it stays valid while
+    // the buffers stay where they are and the permeability mode is unchanged
+    if (h->m.p != m0 || h->dtmu.p != dm0 || h->has_mu != (mu != nullptr) || !h->has_model) drop_graph(h);
     const double k = 2.0 * h->ph.omega0 * h->ph.dt;
     if (h->fp64)
         model_kernel<double><<<1024, 256, 0, h->st>>>(ds.as<double>(), mu ? dm.as<double>() : nullptr, h->g.nx, h->g.ny,
@@ -1693,7 +1708,6 @@ int mittet_set_model(mittet_handle *h, const double *sigma, const double *mu) {
     CK(cudaStreamSynchronize(h->st));
     h->has_model = true;
     h->has_mu = mu != nullptr;
-    drop_graph(h);
     return upload_sources(h);
 }
 
@@ -1727,12 +1741,14 @@ int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu,
         h->mu_h.clear();
     }
     const size_t cb = (size_t)h->fshot * h->esz;
+    const void *m0 = h->m.p, *dm0 = h->dtmu.p;
     CK(h->m.ensure(cb));
     CK(cudaMemsetAsync(h->m.p, 0, cb, h->st));
     if (mu) {
         CK(h->dtmu.ensure(cb));
         CK(cudaMemsetAsync(h->dtmu.p, 0, cb, h->st));
     }
+    if (h->m.p != m0 || h->dtmu.p != dm0 || h->has_mu != (mu != nullptr) || !h->has_model) drop_graph(h);
     const double k = 2.0 * h->ph.omega0 * h->ph.dt;
     if (h->fp64 && is_fp64)
         model_kernel_dev<double><<<1024, 256, 0, h->st>>>((const double *)sigma, (const double *)mu, h->g.nx, h->g.ny,
@@ -1748,7 +1764,6 @@ int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu,
     CK(cudaStreamSynchronize(h->st));
     h->has_model = true;
     h->has_mu = mu != nullptr;
-    drop_graph(h);
     return upload_sources(h);
 }
 
@@ -1766,9 +1781,9 @@ int mittet_set_sources(mittet_handle *h, int32_t nshot, int32_t npoint, const mi
     }
     int rc = set_device(h);
     if (rc) return rc;
+    if (h->nshot != nshot) drop_graph(h);  // the batch shape is baked into the graph and the tuning
     h->nshot = nshot;
     h->pts.assign(pts, pts + npoint);
-    drop_graph(h);
     return upload_sources(h);
 }
 

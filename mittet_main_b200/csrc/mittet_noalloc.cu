@@ -3,11 +3,9 @@
 //
 // Who needs it: host code that must not call cudaMalloc/cudaFree.  cudaFree
 // (and often cudaMalloc) synchronises the whole device, which stalls every
-// other stream of a latency-bound serving process; code running while a
-// stream is being captured into a CUDA graph may not allocate at all; and
-// hosts whose device memory is owned by another allocator (a framework's
-// caching allocator, a fixed per-process budget) cannot take memory behind
-// its back.  For them this entry point keeps every intermediate buffer of the
+// other stream of a latency-bound serving process; and hosts whose device
+// memory is owned by another allocator (a framework's caching allocator, a
+// fixed per-process budget) cannot take memory behind its back.  For them this entry point keeps every intermediate buffer of the
 // solve (fields, CPML psi slabs, model words, profiles, receiver traces) in
 // one file-scope __device__ array of fixed size, and takes its inputs and
 // outputs from the caller.  It launches the same stencil kernels as

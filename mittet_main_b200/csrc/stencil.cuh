@@ -10,8 +10,9 @@
 // CPML terms, and only edges and corners (GM = 7) pay for all of them.
 // Five launches per phase (interior, x faces, y faces, z faces, edges), each
 // with its own thread-tile shape; blockIdx.x enumerates tiles through a TileMap in global
-// memory, blockIdx.y is the shot.  The interior box is the exact interior
-// (x edges on multiples of 4 cells), so its last tile in x and y may be
+// memory, blockIdx.y is the shot.  The interior box's x edges lie on 32-cell
+// (128-byte) line boundaries inside the exact interior (multiples of 4 cells
+// on grids too narrow for that), so its last tile in x and y may be
 // partial.  Every body uses the same explicit fma forms, so a cell gets
 // bit-identical results whichever body computes it.
 //

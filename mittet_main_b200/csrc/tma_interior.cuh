@@ -22,7 +22,8 @@
 // the interior body in stencil.cuh, so results are bit-identical to it, and
 // stores its cells (and, in the E phase, the DFT ring) straight to HBM.
 //
-// Every mbarrier wait is bounded.  A wait that gives up sets bit 1 of the
+// Every mbarrier wait is bounded (TmaTiling::spin_limit polls; the handle's
+// default is kMbarSpinLimit).  A wait that gives up sets bit 1 of the
 // error word (the host reports MITTET_ERR_DEVICE_TIMEOUT) and the CTA's abort
 // flag; after the next __syncthreads() every thread leaves the plane loop
 // together, thread 0 issues no further copy and waits (again bounded) for
@@ -49,6 +50,7 @@ struct TmaMaps {
 struct TmaTiling {
     int x0, y0, z0, x1, y1, z1;  // interior box [x0, x1) x [y0, y1) x [z0, z1)
     int ntx, nty, zc;            // tiles in x and y, z planes per chunk
+    int spin_limit;              // polls before an mbarrier wait gives up
 };
 
 // Stage geometry shared by the host (shared-memory size) and the kernel;
@@ -83,6 +85,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// Non-blocking test of the same phase: one poll costs a few cycles, so a
+// wait limited to a few polls gives up before any copy can land.
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
@@ -91,7 +106,8 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
-constexpr int kMbarSpinLimit = 1 << 20;   // try_wait polls before a wait gives up
+constexpr int kMbarSpinLimit = 1 << 20;   // default try_wait polls before a wait gives up
+constexpr int kMbarQuickLimit = 4096;     // limits below this poll with test_wait
 constexpr int kMbarDrainLimit = 1 << 16;  // polls per in-flight copy when draining
 
 template <typename T, int TX, int TY, int S, bool EPH, bool OWN_SMEM>
@@ -148,16 +164,20 @@ __global__ void __launch_bounds__((TX / 2) * TY) interior_tma_kernel(const Phase
             tma_load_3d(smem_addr(st + G::OO + q * G::NO), &maps.map[3 + q], X0, Y0, model ? p : zs + p, bar);
         }
     };
+    // tl.spin_limit below kMbarQuickLimit (a caller's short limit) polls with
+    // the non-blocking test_wait, so the limit counts a few cycles each.
+    const int spin = tl.spin_limit;
+    const bool quick = spin < kMbarQuickLimit;
     auto wait = [&](int r) {
         const uint32_t bar = smem_addr(&bars[r % S]);
         const uint32_t par = (uint32_t)(r / S) & 1u;
-        for (int it = 0; !mbar_try_wait(bar, par); it++) {
+        for (int it = 0; !(quick ? mbar_test_wait(bar, par) : mbar_try_wait(bar, par)); it++) {
             if (*(volatile int *)&s_abort || ((it & 1023) == 1023 && (*(volatile int *)err & 2))) {
                 gave_up = 1;
                 s_abort = 1;
                 return;
             }
-            if (it >= kMbarSpinLimit) {
+            if (it >= spin) {
                 atomicOr(err, 2);
                 gave_up = 1;
                 s_abort = 1;

@@ -11,7 +11,10 @@
 ! C ABI takes, and 1-based (ix,iy,iz) positions are passed unchanged.
 !
 ! No Fortran compiler was available where this build was made, so this
-! module is provided as source; see INTEGRATION.md for the call sequence.
+! module is provided as source.  Call sequence: mittet_phys_defaults,
+! mittet_create, then mittet_set_model / mittet_set_sources /
+! mittet_set_wavelet / mittet_set_receivers / mittet_set_freqs, then
+! mittet_forward once per shot set, and mittet_destroy.
 !-----------------------------------------------------------------------------
 module mittet_gpu
     use iso_c_binding

@@ -82,11 +82,11 @@ def _time_base(sig, d, flavor=FLAVOR_NCVER0027, precision=FP32, nx=None, ny=None
 FREQS4 = np.array([0.25, 0.5, 1.0, 2.0])
 
 
-def plain_cpu(nt: int = 3000, n: int = 64, precision=FP32) -> Workload:
+def plain_cpu(nt: int = 3000, n: int = 64, precision=FP32, flavor=FLAVOR_NCVER0027) -> Workload:
     d = 50.0
     sig = np.full((n, n, n), 1.0)
     sig[: n // 2] = 0.01  # sigma = 0.01 for k < 32 (0-based), 1.0 below
-    cp, fmax = _time_base(sig, d, precision=precision, nx=n, ny=n, nz=n, ncpml=10)
+    cp, fmax = _time_base(sig, d, flavor=flavor, precision=precision, nx=n, ny=n, nz=n, ncpml=10)
     c = n // 2
     shots = [Shot(points=[(c, c, c - 2, "ex", SRC_ELECTRIC, 1.0)])]
     rec = [(x, c, c - 1, comp) for x in range(n // 4, n // 4 + 32) for comp in ("ex", "ey", "ez", "hx", "hy", "hz")]
@@ -107,10 +107,11 @@ def surface_grid(nx, ny, ncpml, m):
     return [(int(x), int(y)) for y in ys for x in xs]
 
 
-def plain_gpu(nt: int = 6000, nx=256, ny=256, nz=192, precision=FP32, volume=True, seed=2026) -> Workload:
+def plain_gpu(nt: int = 6000, nx=256, ny=256, nz=192, precision=FP32, volume=True, seed=2026,
+              flavor=FLAVOR_NCVER0027) -> Workload:
     d = 25.0 * 256 / nx if nx != 256 else 25.0
     sig = c2_model(nx, ny, nz, seed)
-    cp, fmax = _time_base(sig, d, precision=precision, nx=nx, ny=ny, nz=nz, ncpml=16)
+    cp, fmax = _time_base(sig, d, flavor=flavor, precision=precision, nx=nx, ny=ny, nz=nz, ncpml=16)
     kz = cp.ncpml + 3  # receivers at 0-based k = ncpml + 2
     shots = [Shot(points=[(nx // 2, ny // 2, kz, "ex", SRC_ELECTRIC, 1.0)])]
     rec = [(x, y, kz, "ex") for (x, y) in surface_grid(nx, ny, cp.ncpml, 16)]

@@ -25,6 +25,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "satan_ref")
+# the same sources built with the reference's own flags (gcc -fopenmp -O3):
+# the timed CPU reference arm; REF_PATH is the bit-parity build
+REF_O3_PATH = os.path.join(HERE, "_ref", "satan_ref_o3")
 
 FLAVOR_NCVER0027 = 0
 FLAVOR_SATAN_I = 1
@@ -198,11 +201,16 @@ def satan_params(ix, iy, iz, dx, dy, dz, ncpml, omega0, minval):
                   omega0=omega0, flavor=FLAVOR_SATAN_I, psi_hyx_typo=0, c2=C2_C)
 
 
-def run_satan_reference(ix, iy, iz, dx, dy, dz, ncpml, omega0, sigma, wavelet, nt, src, src_comp, receivers):
+def run_satan_reference(ix, iy, iz, dx, dy, dz, ncpml, omega0, sigma, wavelet, nt, src, src_comp, receivers,
+                        nvol=0):
     """Run the reference's own satan_i kernels (oracle/_ref/satan_ref).
 
     src: 1-based (px, py, pz); src_comp in 0..2; receivers: list of (px, py, pz, comp 0..5).
-    Returns (dt, cmax, traces[nrec, nt], fields[6, iz, iy, ix]).
+    Returns (dt, cmax, traces[nrec, nt], fields[6, iz, iy, ix]).  With nvol > 0
+    a fifth item: the reference's full-volume transform laplaceToFreq_2 of the
+    E history, [3, nvol - 1, iz, iy, ix] complex at w = 1 .. nvol-1 of the grid
+    w 2 pi / ((nt + 1) dt), divided by sqrt(-2 w0 / (i w)) (its G = E / J with
+    a unit current impulse and out_True = 1).
     """
     if not os.path.exists(REF_PATH):
         raise FileNotFoundError(REF_PATH)
@@ -214,30 +222,39 @@ def run_satan_reference(ix, iy, iz, dx, dy, dz, ncpml, omega0, sigma, wavelet, n
         buf = struct.pack("<10i", *hdr)
         for r in receivers:
             buf += struct.pack("<4i", *r)
+        if nvol:
+            buf += struct.pack("<i", nvol)
         buf += struct.pack("<6d", dx, dy, dz, omega0, float(sigma.min()), float(sigma.max()))
         buf += sigma.tobytes() + np.ascontiguousarray(wavelet[: nt + 1], dtype=np.float64).tobytes()
         with open(os.path.join(d, "in.bin"), "wb") as f:
             f.write(buf)
         env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "4"))
-        subprocess.check_call([REF_PATH, "in.bin", "out.bin"], cwd=d, env=env,
-                              stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        args = [REF_PATH, "fwd", "in.bin", "out.bin"] if nvol else [REF_PATH, "in.bin", "out.bin"]
+        subprocess.check_call(args, cwd=d, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         raw = np.fromfile(os.path.join(d, "out.bin"), dtype=np.float64)
     dt, cmax = raw[0], raw[1]
     nrec = len(receivers)
     traces = raw[2: 2 + nrec * nt].reshape(nrec, nt)
-    fields = raw[2 + nrec * nt:].reshape(6, iz, iy, ix)
-    assert fields.size == 6 * n
-    return float(dt), float(cmax), traces, fields
+    o = 2 + nrec * nt
+    fields = raw[o:o + 6 * n].reshape(6, iz, iy, ix)
+    if not nvol:
+        assert raw.size == o + 6 * n
+        return float(dt), float(cmax), traces, fields
+    v = raw[o + 6 * n:]
+    vol = (v[0::2] + 1j * v[1::2]).reshape(3, nvol - 1, iz, iy, ix)
+    return float(dt), float(cmax), traces, fields, vol
 
 
 def time_satan_reference(ix, iy, iz, dx, dy, dz, ncpml, omega0, sigma, steps_per_seg, nseg, src, src_comp=0,
-                         threads=None):
+                         threads=None, binary=None):
     """Wall time of nseg segments of steps_per_seg steps of the reference's own
-    satan_i kernels (timing mode of oracle/_ref/satan_ref).  The reference's
-    coefficient dumps (./data/coef*.dat, ./data/pml_conductivity_*) go to
-    /dev/null so set-up does not write gigabytes of text."""
-    if not os.path.exists(REF_PATH):
-        raise FileNotFoundError(REF_PATH)
+    satan_i kernels (timing mode of oracle/_ref/satan_ref_o3, the build with
+    the reference's own -O3 flags, unless ``binary`` names another).  The
+    reference's coefficient dumps (./data/coef*.dat, ./data/pml_conductivity_*)
+    go to /dev/null so set-up does not write gigabytes of text."""
+    exe = binary or REF_O3_PATH
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
     sigma = np.ascontiguousarray(sigma, dtype=np.float64).reshape(-1)
     nt_total = steps_per_seg * nseg
     with tempfile.TemporaryDirectory() as d:
@@ -254,7 +271,7 @@ def time_satan_reference(ix, iy, iz, dx, dy, dz, ncpml, omega0, sigma, steps_per
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
-        subprocess.check_call([REF_PATH, "in.bin", "out.bin", str(nseg)], cwd=d, env=env,
+        subprocess.check_call([exe, "in.bin", "out.bin", str(nseg)], cwd=d, env=env,
                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         return np.fromfile(os.path.join(d, "out.bin"), dtype=np.float64)
 
@@ -361,3 +378,107 @@ def update_para2(sigma, grad, obs, ecal, e2, scaler, iseabed, minval, maxval, nc
     inner += np.where(ks <= iseabed, (alpha * scaler) * g, 0.0)
     np.clip(inner, minval, maxval, out=inner)
     return out, alpha
+
+
+# ------------------------------------ satan_i post-processing, reference runs
+
+def _run_ref_mode(mode: str, payload: bytes, files=()):
+    """Run oracle/_ref/satan_ref in one of its array modes; returns (raw output
+    bytes, {name: text of each requested ./data file the reference wrote})."""
+    if not os.path.exists(REF_PATH):
+        raise FileNotFoundError(REF_PATH)
+    with tempfile.TemporaryDirectory() as d:
+        os.mkdir(os.path.join(d, "data"))
+        with open(os.path.join(d, "in.bin"), "wb") as f:
+            f.write(payload)
+        env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "4"))
+        subprocess.check_call([REF_PATH, mode, "in.bin", "out.bin"], cwd=d, env=env,
+                              stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        with open(os.path.join(d, "out.bin"), "rb") as f:
+            raw = f.read()
+        texts = {}
+        for name in files:
+            with open(os.path.join(d, "data", name)) as f:
+                texts[name] = f.read()
+    return raw, texts
+
+
+def _c(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128)).tobytes()
+
+
+def run_satan_ftod(traces, jx, dt, omega0, upper_f, files=()):
+    """satan_i laplaceToFreq (fwi3d_cpu_function_v1.4.c:1976-2089) on given
+    traces [nrec, 3, it] (Ex, Ey, Ez) and source trace jx [it].  Returns
+    ([nrec, 4, it] complex: EX_w, EY_w, EZ_w, JX_w on w_n = n 2 pi/(it dt),
+    texts of the requested spectrum files)."""
+    tr = np.ascontiguousarray(traces, dtype=np.float64)
+    nrec, _, it = tr.shape
+    buf = struct.pack("<3i", it, nrec, upper_f) + struct.pack("<2d", dt, omega0)
+    buf += tr.tobytes() + np.ascontiguousarray(jx, dtype=np.float64).tobytes()
+    raw, texts = _run_ref_mode("ftod", buf, files)
+    out = np.frombuffer(raw, dtype=np.complex128).reshape(nrec, 4, it)
+    return out, texts
+
+
+def run_satan_gamma(shape, ncpml, rec_pos, d, obs, e_ff, e_bb, files=()):
+    """satan_i residualE, sensitivity, conv_GdelE and calc_gamma
+    (fwi3d_cpu_function_v1.4.c:2202-2384).  shape (ix, iy, iz); rec_pos
+    [nrec, 3] 1-based; obs [3, nrec, nf]; e_ff [3, nf, n]; e_bb
+    [3, nrec, 3, nf, n].  Returns dict(err_sum, de [3, nrec, nf], sense [n],
+    e_back [3, nf, n], grad [n]) and the requested file texts."""
+    ix, iy, iz = shape
+    n = ix * iy * iz
+    nrec, nf = len(rec_pos), np.asarray(e_ff).shape[1]
+    buf = struct.pack("<6i", ix, iy, iz, ncpml, nrec, nf)
+    buf += np.ascontiguousarray(rec_pos, dtype=np.int32).tobytes() + struct.pack("<3d", *d)
+    buf += b"".join(_c(np.asarray(a)[c]) for a in (obs, e_ff, e_bb) for c in range(3))
+    raw, texts = _run_ref_mode("gamma", buf, files)
+    v = np.frombuffer(raw, dtype=np.float64)
+    o = 1
+    err = float(v[0])
+    cv = lambda a: a[0::2] + 1j * a[1::2]  # noqa: E731
+    de = cv(v[o:o + 2 * 3 * nrec * nf]).reshape(3, nrec, nf)
+    o += 2 * 3 * nrec * nf
+    sense = v[o:o + n].copy()
+    o += n
+    back = cv(v[o:o + 2 * 3 * nf * n]).reshape(3, nf, n)
+    o += 2 * 3 * nf * n
+    grad = v[o:o + n].copy()
+    return {"err_sum": err, "de": de, "sense": sense, "e_back": back, "grad": grad}, texts
+
+
+def run_satan_update(shape, ncpml, iseabed, rec_pos, d, minval, maxval, sig, grad, de, e_ffl, e_ff2, files=()):
+    """satan_i calc_phi, calc_alpha(0), update_para2(0)
+    (fwi3d_cpu_function_v1.4.c:2565-2603, 2757-2832).  de [3, nrec, nf];
+    e_ffl, e_ff2 [3, nf, n].  Returns dict(scaler, k1, k2, alpha, sig2 [n],
+    sig [n]) and the requested file texts (sig_tmp.dat, gradient_000.dat,
+    sig_000.dat)."""
+    ix, iy, iz = shape
+    n = ix * iy * iz
+    nrec, nf = len(rec_pos), np.asarray(e_ffl).shape[1]
+    buf = struct.pack("<7i", ix, iy, iz, ncpml, iseabed, nrec, nf)
+    buf += np.ascontiguousarray(rec_pos, dtype=np.int32).tobytes() + struct.pack("<5d", *d, minval, maxval)
+    buf += np.ascontiguousarray(sig, dtype=np.float64).tobytes() + np.ascontiguousarray(grad, dtype=np.float64).tobytes()
+    buf += b"".join(_c(np.asarray(a)[c]) for a in (de, e_ffl, e_ff2) for c in range(3))
+    raw, texts = _run_ref_mode("update", buf, files)
+    v = np.frombuffer(raw, dtype=np.float64)
+    return {"scaler": float(v[0]), "k1": complex(v[1], v[2]), "k2": complex(v[3], v[4]), "alpha": float(v[5]),
+            "sig2": v[6:6 + n].copy(), "sig": v[6 + n:6 + 2 * n].copy()}, texts
+
+
+def satan_gamma(shape, ncpml, rec_pos, obs, e_ff, e_bb):
+    """numpy restatement of satan_i residualE, sensitivity, conv_GdelE and
+    calc_gamma (fwi3d_cpu_function_v1.4.c:2202-2384), same layouts as
+    run_satan_gamma (one shot, grad starting at zero)."""
+    ix, iy, iz = shape
+    obs, e_ff, e_bb = (np.asarray(a, dtype=np.complex128) for a in (obs, e_ff, e_bb))
+    cells = np.array([((z - 1) * iy + (y - 1)) * ix + (x - 1) for (x, y, z) in rec_pos], dtype=np.int64)
+    de = obs - e_ff[:, :, cells].transpose(0, 2, 1)                         # residualE :2222-2228
+    err = float(np.sum(np.abs(de).transpose(1, 2, 0)))                       # :2236-2238
+    sense = np.abs(e_ff[:, None, None] * e_bb).sum(axis=(0, 1, 2, 3))        # sensitivity :2276-2278
+    back = np.einsum("crdwn,drw->cwn", e_bb, np.conj(de))                    # conv_GdelE :2329-2342
+    g = np.real((e_ff * back).sum(axis=0)).sum(axis=0) / sense               # calc_gamma :2372-2374
+    m = np.zeros((iz, iy, ix), dtype=bool)
+    m[ncpml:iz - ncpml, ncpml:iy - ncpml, ncpml:ix - ncpml] = True
+    return {"err_sum": err, "de": de, "sense": sense, "e_back": back, "grad": np.where(m.ravel(), g, 0.0)}

@@ -1,6 +1,7 @@
 """CPU tests of the benchmark script's contract pieces that need no GPU: the
-DRAM traffic it reports for the roofline is read from the committed ncu
-summary, and its options parse."""
+roofline record it builds (algorithmic bytes, the DRAM reads per cell read
+from the committed ncu summary, a traffic figure that cannot fall below the
+algorithmic bytes), and its options parse."""
 import importlib.util
 import os
 
@@ -14,11 +15,22 @@ def load_bench():
     return mod
 
 
-def test_roofline_traffic_comes_from_the_committed_profile():
+def test_roofline_record():
     from mittet_main_b200 import workloads as W
     bench = load_bench()
     wl = W.plain_gpu(nt=64)
-    t = bench.e_phase_traffic(wl, 4)
-    # 40.1 B per cell in the summary, for the 256 x 256 x 192 launch
-    assert t is not None and 30 * wl.ncell < t < 60 * wl.ncell
-    assert bench.e_phase_traffic(wl, 8) is None  # only FP32 was captured
+    r = bench.roofline(wl, 4, {"e_phase": 0.2}, 6537.3, "measured")
+    alg = bench.stencil_bytes(wl, 4)
+    assert r["alg_bytes_per_launch"] == alg
+    assert abs(r["achieved"] - alg / 0.2e-3 / 1e9) < 1e-6 and abs(r["frac"] - r["achieved"] / 6537.3) < 1e-12
+    # 6 fields + model word read per cell, plus the psi of the slab cells
+    assert 28.0 < r["alg_read_bytes_per_cell"] < 32.0
+    prof = bench.e_phase_profile(4, "xyz")
+    if prof is None:
+        assert r["traffic"] is None
+    else:
+        assert r["read_bytes_per_cell"] == prof["read"]
+        assert r["traffic"] >= alg and r["read_amplification"] >= 1.0
+    assert bench.e_phase_profile(8, "xyz") is None  # only FP32 was captured
+    r64 = bench.roofline(wl, 8, {"e_phase": 0.3}, 6537.3, "measured")
+    assert r64["traffic"] is None and r64["alg_bytes_per_launch"] == 2 * alg

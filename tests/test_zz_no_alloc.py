@@ -1,13 +1,16 @@
 """GPU test of mittet_forward_noalloc, the entry point for callers that cannot
-call cudaMalloc (serving code that must not stall other streams on the
-device-wide synchronisation of cudaFree, code running during stream capture,
-hosts whose device memory belongs to another allocator).
+call cudaMalloc: serving code that must not stall its other streams on the
+device-wide synchronisation cudaFree brings, and hosts whose device memory
+belongs to another allocator.
 
-It must give the spectra of the regular entry point, mittet_forward, within
-the FP32 tolerance of the parity tests, on two calls in a row (the second
-call finds the scratch array full of the first call's state), and allocate no
-device memory on a call after the first.  The file is named so pytest
-collects it last.
+Both entry points run the same stencil bodies with the same explicit fma
+forms (the no-alloc one uses the general body on every cell, the regular one
+the interior, face and edge bodies the autotuner picks, all of which give a
+cell bit-identical results), the same source gains and the same f_to_d
+kernel, so the spectra must be equal bit for bit, with an electric and with a
+magnetic source, on two calls in a row (the second call finds the scratch
+array full of the first call's state), and a call after the first must
+allocate no device memory.  The file is named so pytest collects it last.
 """
 import ctypes
 
@@ -17,7 +20,6 @@ import pytest
 from mittet_main_b200 import capi
 from mittet_main_b200 import workloads as W
 from mittet_main_b200.capi import FP32
-from tests.conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -37,13 +39,15 @@ def _noalloc_call(lib, wl, sigma_d, wave_d, out_d):
     capi.check(rc)
 
 
-def test_noalloc_forward_matches_regular_entry_point_twice():
+@pytest.mark.parametrize("magnetic", [False, True])
+def test_noalloc_forward_matches_regular_entry_point_twice(magnetic):
     import torch
 
-    wl = W.small_case(n=(40, 36, 32), ncpml=8, nt=200, precision=FP32, magnetic=False)
+    wl = W.small_case(n=(40, 36, 32), ncpml=8, nt=200, precision=FP32, magnetic=magnetic)
     with W.make_solver(wl) as s:
         ref, _ = s.forward(wl.nt)
     ref = ref[0]  # [nrec, nf]
+    assert np.abs(ref).max() > 0
 
     lib = capi.load()
     dev = torch.device("cuda:0")
@@ -61,9 +65,7 @@ def test_noalloc_forward_matches_regular_entry_point_twice():
         o = out_d.cpu().numpy()
         outs.append(o[..., 0] + 1j * o[..., 1])
     for got in outs:
-        ise = np.array([r[3].startswith("e") for r in wl.receivers])
-        assert rel_l2(got[ise], ref[ise]) <= 1e-4
-        assert rel_l2(got[~ise], ref[~ise]) <= 1e-4
+        assert np.array_equal(got, ref), f"max |diff| {np.abs(got - ref).max():.3e}"
     # the second call allocates nothing on the device
     assert free_after[1][1] == free_after[1][0]
 
