@@ -191,7 +191,7 @@ def main():
     ap.add_argument("--workload", default="plain_gpu", choices=["plain_gpu", "batched", "plain_cpu"])
     ap.add_argument("--mode", default="solve", choices=["solve", "batching", "gradient", "serving"],
                     help="solve: the headline line; batching/gradient/serving: the other workloads' reports")
-    ap.add_argument("--requests", type=int, default=24, help="serving: number of requests")
+    ap.add_argument("--requests", type=int, default=16, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate per second")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--nt", type=int, default=0, help="override Nt (0 = workload default)")
@@ -295,6 +295,7 @@ def main():
         e2e = {"value": total_cells / te / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h}
     stencil_variant = solver.tuned_variant()
+    launch_path = solver.launch_path()
     solver.close()
 
     extras = {}
@@ -345,6 +346,7 @@ def main():
             "gpu_launches": gpu_launches,
             "kernel_ms": kt,
             "stencil_variant": stencil_variant,
+            "launch_path": launch_path,
             "roofline": roof,
             "clocks": clocks,
             "e2e": e2e,

@@ -269,6 +269,14 @@ int mittet_tuned_variants(mittet_handle *h, int32_t *cfg);
  * every launch.  No counterpart in the reference (a tuning introspection). */
 int mittet_stencil_variants(int32_t fp64, int32_t *count, int32_t *cfg, int32_t max);
 
+/* Which launch the last forward's time loop used: *variant = -1 for the
+ * stepped graph of part kernels, else the stencil variant (index as in
+ * mittet_stencil_variants) whose tiles and thread shape the persistent
+ * multi-shot launch ran, with *grid its CTAs.  The autotuner picks it by
+ * timing a block of steps of each (MITTET_PERSIST=0/1 forces one).  No
+ * counterpart in the reference (a tuning introspection). */
+int mittet_persistent_variant(mittet_handle *h, int32_t *variant, int32_t *grid);
+
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);
 

@@ -8,9 +8,9 @@ gradient: FWI gradient of the 128x128x96 model, 16 shots, Ex/Ey at 3
   of forward-equivalent work.
 serving: Poisson arrivals of forward (3) and gradient (1) requests over the
   grid set {64^3, 96^3, 128^3, 160x160x96, 256x256x192} (domain 6.4 km wide),
-  1-32 shots, Nt scaled with the grid; p50/p99 latency and shot-solves/s of
-  the server against two plain paths on the same GPU: one request at a time
-  (its shots batched), and one shot at a time.
+  1-32 shots, Nt = 6000 nx / 256; p50/p99 latency and shot-solves/s of the
+  server against two plain paths served in real time on the same GPU: one
+  request at a time (its shots batched), and one shot at a time.
 Times are device-synchronised wall clock of the public API calls.
 """
 from __future__ import annotations
@@ -41,6 +41,7 @@ def batching_ratio(wl, repeats: int = 1) -> dict:
             spec_b, _ = s.forward(wl.nt)
             _sync()
             tb = min(tb, time.perf_counter() - t0)
+        path_b = s.launch_path()
     one = replace(wl, shots=[wl.shots[0]])
     tp = float("inf")
     with W.make_solver(one) as s:
@@ -55,12 +56,14 @@ def batching_ratio(wl, repeats: int = 1) -> dict:
                 specs.append(sp[0])
             _sync()
             tp = min(tp, time.perf_counter() - t0)
+        path_p = s.launch_path()
     same = all(np.array_equal(spec_b[k], specs[k]) for k in range(ns))
     cells = wl.ncell * wl.nt
     return {"workload": wl.name, "nt": wl.nt, "shots": ns,
             "batched_shot_solves_per_s": ns / tb, "one_at_a_time_shot_solves_per_s": ns / tp,
             "batched_vs_one_at_a_time": tp / tb, "batched_gcell_s": ns * cells / tb / 1e9,
-            "one_at_a_time_gcell_s": ns * cells / tp / 1e9, "identical_results": bool(same)}
+            "one_at_a_time_gcell_s": ns * cells / tp / 1e9, "identical_results": bool(same),
+            "batched_launch": path_b, "one_at_a_time_launch": path_p}
 
 
 def batching(args):
@@ -108,13 +111,32 @@ def gradient(args):
             "grad_max_abs": float(np.abs(body).max())}
 
 
+def one_shot_at_a_time(solver_cache: dict, req):
+    """Executor of the plain one-shot-at-a-time path: every shot of the
+    request solved alone on the grid's handle, one after another."""
+    from mittet_main_b200.serving import Request, run_request
+    wl = req.workload
+    outs = []
+    for k, shot in enumerate(wl.shots):
+        single = Request(req.rid, req.arrival, replace(wl, shots=[shot]), req.mode,
+                         None if req.obs is None else req.obs[k:k + 1], req.checkpoint_every)
+        outs.append(run_request(solver_cache, single))
+    return outs
+
+
 def serving(args):
+    """The serving mix: Poisson arrivals (rate args.rate, args.requests
+    requests, seeded), grids {64^3, 96^3, 128^3, 160x160x96, 256x256x192}
+    with dx = 6400 m / nx, 1-32 shots, Nt = 6000 nx / 256 (args.nt scales it:
+    Nt x args.nt / 6000), forward:gradient = 3:1, 150 GB budget.  Three
+    arms, each served in real time from the same arrival process on the same
+    GPU: the server (4 slots, continuous batching), one request at a time
+    (one slot, its shots batched) and one shot at a time (one slot, each shot
+    solved alone)."""
     from mittet_main_b200 import workloads as W
-    from mittet_main_b200.capi import FP32
-    from mittet_main_b200.serving import (MittetServer, percentile, poisson_requests, run_request,
-                                          serial_latencies)
+    from mittet_main_b200.serving import MittetServer, percentile, poisson_requests, run_request
     grids = [(64, 64, 64), (96, 96, 96), (128, 128, 128), (160, 160, 96), (256, 256, 192)]
-    scale = args.nt / 6000.0 if args.nt else 0.1  # Nt = 6000 * nx/256 * scale
+    scale = args.nt / 6000.0 if args.nt else 1.0
 
     def make(i, rng):
         nx, ny, nz = grids[int(rng.integers(len(grids)))]
@@ -122,62 +144,43 @@ def serving(args):
         nt = max(50, int(6000 * nx / 256 * scale))
         return W.serving_case(nx, ny, nz, nshot, nt, seed=int(rng.integers(1 << 30)))
 
-    reqs = poisson_requests(args.requests, args.rate, make)
-    # serial plain path: one request at a time on one handle
-    service = {}
-    cache = {}
-    for r in reqs[:1]:
-        run_request(cache, r)  # warm-up
-    for r in reqs:
-        _sync()
-        t0 = time.perf_counter()
-        run_request(cache, r)
-        _sync()
-        service[r.rid] = time.perf_counter() - t0
-    for s in cache.values():
-        s.close()
-    ser = serial_latencies(reqs, service)
-    # plain one-shot-at-a-time path: every shot of a request solved alone, one
-    # after another.  Shots of a request cost the same, so one timed
-    # single-shot solve per (grid, Nt, mode) gives the request's service time.
+    n = args.requests
+    reqs = poisson_requests(n, args.rate, make)
+    shots = sum(len(r.workload.shots) for r in reqs)
+    # warm-up: the autotuner's choices are cached per (grid, shots, ...) for
+    # the process; fill them for every batch shape the arms meet with short
+    # solves, so that no arm pays for tuning the others then reuse
     from mittet_main_b200.serving import Request
-    one = {}
+    seen = set()
     for r in reqs:
         wl = r.workload
-        key = (wl.cp.nx, wl.cp.ny, wl.cp.nz, wl.nt, r.mode)
-        if key in one:
-            continue
-        single = Request(-1, 0.0, replace(wl, shots=[wl.shots[0]]), r.mode,
-                         None if r.obs is None else r.obs[:1], r.checkpoint_every)
-        c = {}
-        run_request(c, single)  # warm-up (autotune, graph)
+        for ns in (len(wl.shots), 1):
+            key = (wl.cp.nx, wl.cp.ny, wl.cp.nz, ns)
+            if key in seen:
+                continue
+            seen.add(key)
+            short = replace(wl, shots=wl.shots[:ns], nt=64, wavelet=wl.wavelet[:65])
+            run_request({}, Request(-1, 0.0, short))
+    _sync()
+    out = {"report": "serving", "requests": n, "rate_per_s": args.rate, "nt_scale": scale, "shots": shots,
+           "grids": sorted({f"{r.workload.cp.nx}x{r.workload.cp.ny}x{r.workload.cp.nz}" for r in reqs}),
+           "modes": {m: sum(r.mode == m for r in reqs) for m in ("forward", "gradient")}}
+    arms = [("server", 4, run_request), ("one_request_at_a_time", 1, run_request),
+            ("one_shot_at_a_time", 1, one_shot_at_a_time)]
+    for name, slots, ex in arms:
+        srv = MittetServer(n_slots=slots, hbm_budget=150e9, executor=ex)
         _sync()
         t0 = time.perf_counter()
-        run_request(c, single)
+        res = srv.run(reqs)
         _sync()
-        one[key] = time.perf_counter() - t0
-        for sv in c.values():
-            sv.close()
-    service1 = {r.rid: len(r.workload.shots) * one[(r.workload.cp.nx, r.workload.cp.ny, r.workload.cp.nz,
-                                                     r.workload.nt, r.mode)] for r in reqs}
-    ser1 = serial_latencies(reqs, service1)
-    t1 = 0.0
-    for r in sorted(reqs, key=lambda r: r.arrival):
-        t1 = max(t1, r.arrival) + service1[r.rid]
-    srv = MittetServer(n_slots=4, hbm_budget=150e9)
-    t0 = time.perf_counter()
-    res = srv.run(reqs)
-    wall = time.perf_counter() - t0
-    shots = sum(len(r.workload.shots) for r in reqs)
-    lat = [r.latency for r in res]
-    errors = [r.error for r in res if r.error]
-    t = 0.0
-    for r in sorted(reqs, key=lambda r: r.arrival):
-        t = max(t, r.arrival) + service[r.rid]
-    return {"report": "serving", "requests": len(reqs), "rate_per_s": args.rate, "nt_scale": scale,
-            "server_p50_s": percentile(lat, 50), "server_p99_s": percentile(lat, 99),
-            "server_shot_solves_per_s": shots / wall, "serial_p50_s": percentile(list(ser.values()), 50),
-            "serial_p99_s": percentile(list(ser.values()), 99), "serial_shot_solves_per_s": shots / t,
-            "one_shot_p50_s": percentile(list(ser1.values()), 50), "one_shot_p99_s": percentile(list(ser1.values()), 99),
-            "one_shot_shot_solves_per_s": shots / t1, "server_vs_one_shot": (shots / wall) / (shots / t1),
-            "max_concurrent": srv.max_concurrent, "peak_budget_bytes": srv.peak_in_use, "errors": errors[:3]}
+        wall = time.perf_counter() - t0
+        lat = [r.latency for r in res]
+        errors = [r.error for r in res if r.error]
+        out[name] = {"p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
+                     "shot_solves_per_s": shots / wall, "max_concurrent": srv.max_concurrent,
+                     "peak_budget_bytes": srv.peak_in_use, "handle_reuses": srv.reuses,
+                     "evictions": srv.evictions, "errors": errors[:3]}
+    out["server_vs_one_shot"] = out["server"]["shot_solves_per_s"] / out["one_shot_at_a_time"]["shot_solves_per_s"]
+    out["server_vs_one_request"] = (out["server"]["shot_solves_per_s"] /
+                                    out["one_request_at_a_time"]["shot_solves_per_s"])
+    return out

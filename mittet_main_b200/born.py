@@ -78,7 +78,7 @@ def satan_gamma(nx: int, ny: int, nz: int, ncpml: int, rec_pos, obs, e_ff, e_bb,
     err = np.zeros(1)
     de = np.zeros(3 * max(nrec, 1) * nf * 2)
     if o is None and nrec:  # the residual itself is given
-        de[: 3 * nrec * nf * 2] = cbuf(residual, (3, nrec, nf))
+        de[: 3 * nrec * nf * 2] = cbuf(residual, (3, nrec, nf)).ravel()
     sense = np.zeros(n)
     back = np.zeros(3 * nf * n * 2)
     D = ctypes.POINTER(ctypes.c_double)

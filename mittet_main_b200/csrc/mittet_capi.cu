@@ -27,6 +27,7 @@
 
 #include "../../include/mittet.h"
 #include "kernels.cuh"
+#include "persistent.cuh"
 #include "tma_interior.cuh"
 #include "adjoint.cuh"
 #include "setup_host.h"
@@ -183,6 +184,15 @@ struct mittet_handle_s {
     int last_nt = 0;
     int64_t launches = 0;
 
+    // persistent launch (persistent.cuh): the stencil variant whose tile
+    // maps and thread shape it uses (-1: the stepped graph of part kernels),
+    // whether the choice was made for the current tuning, its grid size and
+    // barrier words
+    int persist_vi = -1;
+    bool persist_decided = false;
+    int persist_grid = 0;
+    DevBuf bar;
+
     // cached CUDA graph of G steps
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
@@ -210,6 +220,7 @@ void drop_graph(mittet_handle *h) {
     h->gexec = nullptr;
     h->graph_steps = 0;
     h->tuned = false;  // the shot count or ring may have changed
+    h->persist_decided = false;
 }
 
 int ensure_state(mittet_handle *h) {
@@ -651,6 +662,211 @@ void launch_step(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &h
     h->launches++;
 }
 
+// ------------------------------------------------------- persistent launch
+// The kernel instances of persistent.cuh, by thread shape: each serves the
+// stencil variants of that shape (their tile maps give the z chunk ZC).
+template <typename T>
+using PersistKernel = void (*)(PersistArgs<T>);
+
+template <typename T>
+PersistKernel<T> persist_kernel_for(int vx, int bx, int by) {
+    if (vx == 2 && bx == 32 && by == 4) return persistent_steps_kernel<T, 2, 32, 4>;
+    if (vx == 2 && bx == 16 && by == 8) return persistent_steps_kernel<T, 2, 16, 8>;
+    if constexpr (sizeof(T) == 4)
+        if (vx == 4 && bx == 16 && by == 8) return persistent_steps_kernel<T, 4, 16, 8>;
+    return nullptr;
+}
+
+// Co-resident grid of the persistent kernel of variant vi: CTAs per SM from
+// its occupancy times the SMs, at most one CTA per tile of the larger phase.
+template <typename T>
+int persist_grid_for(mittet_handle *h, int vi) {
+    const Variant<T> &v = variants<T>()[vi];
+    PersistKernel<T> k = persist_kernel_for<T>(v.vx, v.bx, v.by);
+    if (!k || v.bz > 0) return 0;
+    int nb = 0, nsm = 0, coop = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, v.bx * v.by, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->ph.device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->ph.device) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (!coop || nb <= 0) return 0;
+    const long long tiles = (long long)std::max(h->ptile[2 * vi][kParts], h->ptile[2 * vi + 1][kParts]) * h->nshot;
+    return (int)std::min<long long>((long long)nb * nsm, tiles);
+}
+
+template <typename T>
+PersistArgs<T> persist_args(mittet_handle *h, int vi, int grid, int nsteps, const PhaseArgs<T> &ea,
+                            const PhaseArgs<T> &ha, const InjectArgs<T> &ia_m, const InjectArgs<T> &ia_e,
+                            const SampleArgs<T> &sa) {
+    PersistArgs<T> p;
+    memset(&p, 0, sizeof(p));
+    p.e = ea;
+    p.h = ha;
+    p.tme = h->tmaps.as<TileMap>() + 2 * vi;
+    p.tmh = h->tmaps.as<TileMap>() + 2 * vi + 1;
+    p.ntile_e = h->ptile[2 * vi][kParts];
+    p.ntile_h = h->ptile[2 * vi + 1][kParts];
+    p.nshot = h->nshot;
+    p.im = ia_m;
+    p.ie = ia_e;
+    p.has_mag = h->has_mag ? 1 : 0;
+    p.has_ele = h->has_ele ? 1 : 0;
+    p.smp = sa;
+    p.nsteps = nsteps;
+    p.ctl.bar = h->bar.as<GridBarrier>();
+    p.ctl.err = h->d_flag.as<int>();
+    // MITTET_PERSIST_STALL=1 makes every barrier wait for one CTA more than
+    // the grid has, so that a test can watch the waits give up
+    const char *stall = std::getenv("MITTET_PERSIST_STALL");
+    p.ctl.expect = (unsigned)grid + ((stall && std::atoi(stall) == 1) ? 1u : 0u);
+    const char *wms = std::getenv("MITTET_PERSIST_WAIT_MS");
+    const double ms = wms ? std::max(1.0, std::atof(wms)) : 2000.0;
+    p.ctl.wait_ns = (unsigned long long)(ms * 1e6);
+    return p;
+}
+
+// One cooperative launch of nsteps steps (and the reset of its barrier words).
+template <typename T>
+int launch_persistent(mittet_handle *h, int vi, int grid, const PersistArgs<T> &p, cudaStream_t st) {
+    const Variant<T> &v = variants<T>()[vi];
+    PersistKernel<T> k = persist_kernel_for<T>(v.vx, v.bx, v.by);
+    CK(cudaMemsetAsync(h->bar.p, 0, sizeof(GridBarrier), st));
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)v.bx, (unsigned)v.by);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k, p));
+    return MITTET_OK;
+}
+
+// Device time of one replay of a graph (after one untimed replay).
+int time_graph(mittet_handle *h, cudaGraphExec_t g, float *ms) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaGraphLaunch(g, h->st));
+    CK(cudaEventRecord(e0, h->st));
+    CK(cudaGraphLaunch(g, h->st));
+    CK(cudaEventRecord(e1, h->st));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return MITTET_OK;
+}
+
+// Chooses between the stepped graph of part kernels and the persistent
+// launch for this grid and batch by timing one captured block of G steps of
+// each (MITTET_PERSIST=0 / 1 forces one).  Leaves zero fields behind.
+std::mutex g_persist_mu;
+std::map<std::array<long long, 8>, int> g_persist_cache;  // choice per (grid, shots, precision, points, ring)
+
+template <typename T>
+int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha, const InjectArgs<T> &ia_m,
+                      const InjectArgs<T> &ia_e, const SampleArgs<T> &sa, int G) {
+    h->persist_decided = true;
+    h->persist_vi = -1;
+    const char *mode = std::getenv("MITTET_PERSIST");
+    const int force = mode ? std::atoi(mode) : -1;
+    if (force == 0) return MITTET_OK;
+    CK(h->bar.ensure(sizeof(GridBarrier)));
+    const std::array<long long, 8> key = {h->g.nx, h->g.ny, h->g.nz, h->nshot, (long long)h->fp64 + 2 * (force == 1),
+                                          (long long)h->has_mag + 2 * h->has_ele, ea.ring_k, h->nrec};
+    if (!std::getenv("MITTET_PERSIST_STALL")) {
+        std::lock_guard<std::mutex> lk(g_persist_mu);
+        auto it = g_persist_cache.find(key);
+        if (it != g_persist_cache.end()) {
+            h->persist_vi = it->second;
+            if (h->persist_vi >= 0) h->persist_grid = persist_grid_for<T>(h, h->persist_vi);
+            return MITTET_OK;
+        }
+    }
+    const bool log = std::getenv("MITTET_TUNE_LOG") != nullptr;
+    auto capture = [&](int vi, cudaGraphExec_t *out) -> int {
+        cudaGraph_t graph;
+        *out = nullptr;
+        if (cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return 1;
+        }
+        int bad = 0;
+        if (vi < 0) {
+            for (int s = 0; s < G; s++) launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+        } else {
+            const int grid = persist_grid_for<T>(h, vi);
+            bad = grid <= 0 || launch_persistent<T>(h, vi, grid, persist_args<T>(h, vi, grid, G, ea, ha, ia_m, ia_e, sa),
+                                                     h->st) != MITTET_OK;
+        }
+        cudaError_t ec = cudaStreamEndCapture(h->st, &graph);
+        if (ec != cudaSuccess || bad) {
+            cudaGetLastError();
+            if (ec == cudaSuccess) cudaGraphDestroy(graph);
+            return 1;
+        }
+        ec = cudaGraphInstantiate(out, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ec != cudaSuccess) {
+            cudaGetLastError();
+            *out = nullptr;
+            return 1;
+        }
+        return 0;
+    };
+    float best = 1e30f;
+    int best_vi = -1;
+    if (force != 1) {
+        cudaGraphExec_t g;
+        if (capture(-1, &g) == 0) {
+            float ms = 0;
+            int rc = time_graph(h, g, &ms);
+            cudaGraphExecDestroy(g);
+            if (rc) return rc;
+            best = ms;
+            if (log) fprintf(stderr, "persist? stepped graph: %.4f ms per %d steps\n", ms, G);
+        }
+    }
+    const auto &vs = variants<T>();
+    for (int vi = 0; vi < (int)vs.size(); vi++) {
+        if (vs[vi].bz > 0 || !persist_kernel_for<T>(vs[vi].vx, vs[vi].bx, vs[vi].by) || vs[vi].zc > 8) continue;
+        cudaGraphExec_t g;
+        if (capture(vi, &g)) continue;
+        CK(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->st));
+        float ms = 0;
+        int rc = time_graph(h, g, &ms);
+        cudaGraphExecDestroy(g);
+        if (rc) return rc;
+        int flag = 0;
+        CK(cudaMemcpy(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->st));
+        if (log)
+            fprintf(stderr, "persist? vx%d %dx%dx%d grid %d: %.4f ms per %d steps%s\n", vs[vi].vx, vs[vi].bx, vs[vi].by,
+                    vs[vi].zc, persist_grid_for<T>(h, vi), ms, G, (flag & 4) ? " (barrier gave up)" : "");
+        if ((flag & 4) && force != 1) continue;
+        if (ms < best || (force == 1 && best_vi < 0)) {
+            best = ms;
+            best_vi = vi;
+        }
+    }
+    h->persist_vi = best_vi;
+    if (best_vi >= 0) h->persist_grid = persist_grid_for<T>(h, best_vi);
+    if (!std::getenv("MITTET_PERSIST_STALL")) {
+        std::lock_guard<std::mutex> lk(g_persist_mu);
+        g_persist_cache[key] = best_vi;
+    }
+    int rc = ensure_state(h);  // back to zero fields and psi
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->d_step.p, 0, sizeof(int), h->st));
+    return MITTET_OK;
+}
+
 // ------------------------------------------------------------- autotuner
 // Picks, per phase, the fastest stencil variant for this grid, shot count and
 // precision by timing each candidate on the handle's own buffers (zero
@@ -899,17 +1115,36 @@ int run_forward(mittet_handle *h, int nt) {
         if (rc) return rc;
         h->tuned = true;
     }
-    h->launches = 0;
     // One graph holds G = ring_k steps; the volume flush of those steps (when
     // enabled) is launched after each replay.
     const int G = h->ring_k;
-    const long long key = ((long long)nt << 20) ^ ((long long)ns << 4) ^ (vol ? 1 : 0) ^ ((long long)h->nrec << 40);
+    if (!h->persist_decided) {
+        rc = decide_persistent<T>(h, ea, ha, ia_m, ia_e, sa, G);
+        if (rc) return rc;
+    }
+    h->launches = 0;
+    const long long key = ((long long)nt << 20) ^ ((long long)ns << 4) ^ (vol ? 1 : 0) ^ ((long long)h->nrec << 40) ^
+                          ((long long)(h->persist_vi + 1) << 52);
     if (!h->gexec || h->graph_key != key) {
-        drop_graph(h);
+        if (h->gexec) cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
         h->launches = 0;
-        for (int s = 0; s < G; s++) launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+        if (h->persist_vi >= 0) {
+            rc = launch_persistent<T>(h, h->persist_vi, h->persist_grid,
+                                      persist_args<T>(h, h->persist_vi, h->persist_grid, G, ea, ha, ia_m, ia_e, sa),
+                                      h->st);
+            if (rc) {
+                cudaGraph_t dead;
+                cudaStreamEndCapture(h->st, &dead);
+                if (dead) cudaGraphDestroy(dead);
+                return rc;
+            }
+            h->launches = 1;
+        } else {
+            for (int s = 0; s < G; s++) launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+        }
         h->graph_launches = h->launches;
         cudaError_t ec = cudaStreamEndCapture(h->st, &graph);
         if (ec != cudaSuccess) return fail(MITTET_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
@@ -928,8 +1163,13 @@ int run_forward(mittet_handle *h, int nt) {
         done += G;
     }
     const int rem = nt - done;
-    for (int s = 0; s < rem; s++) {
-        launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
+    if (rem > 0 && h->persist_vi >= 0) {
+        rc = launch_persistent<T>(h, h->persist_vi, h->persist_grid,
+                                  persist_args<T>(h, h->persist_vi, h->persist_grid, rem, ea, ha, ia_m, ia_e, sa), h->st);
+        if (rc) return rc;
+        h->launches++;
+    } else {
+        for (int s = 0; s < rem; s++) launch_step<T>(h, ea, ha, ia_m, ia_e, sa);
     }
     if (rem > 0 && vol) launch_volume_flush<T>(h, rem, done);
     CK(cudaGetLastError());
@@ -1472,6 +1712,7 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         fprintf(stderr, "gradient stages (ms): checkpoint pass %.1f, recompute %.1f, adjoint %.1f\n", gms[0], gms[1],
                 gms[2]);
     if (flag & 2) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded wait for a TMA copy gave up");
+    if (flag & 4) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded grid-barrier wait of the persistent launch gave up");
     if (flag) return fail(MITTET_ERR_DIVERGED, "non-finite receiver samples (unstable time step or model)");
     *misfit_out = mis;
     memcpy(grad_out, gsum.data(), ncell * sizeof(double));
@@ -1878,6 +2119,7 @@ int mittet_forward(mittet_handle *h, int32_t nt, double *rec_fd, double *rec_td)
     CK(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     if (flag & 2) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded wait for a TMA copy gave up");
+    if (flag & 4) return fail(MITTET_ERR_DEVICE_TIMEOUT, "a bounded grid-barrier wait of the persistent launch gave up");
     if (flag) return fail(MITTET_ERR_DIVERGED, "non-finite receiver samples (unstable time step or model)");
     return MITTET_OK;
 }
@@ -1972,6 +2214,13 @@ int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double 
 }
 
 int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1; }
+
+int mittet_persistent_variant(mittet_handle *h, int32_t *variant, int32_t *grid) {
+    if (!h || !variant || !grid) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    *variant = h->persist_decided ? h->persist_vi : -1;
+    *grid = *variant >= 0 ? h->persist_grid : 0;
+    return MITTET_OK;
+}
 
 int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg) {
     if (!h || !e_cfg || !h_cfg) return fail(MITTET_ERR_INVALID_ARG, "null argument");

@@ -72,6 +72,23 @@ __device__ __forceinline__ void ldv(T (&dst)[VX], const T *__restrict__ p) {
 #pragma unroll
     for (int q = 0; q < VX; q++) dst[q] = s[q];
 }
+// Loads of values this launch may also write (fields, psi).  CG = false:
+// the read-only path (every launch of the stepped graph only reads the other
+// phase's fields).  CG = true: L2-coherent loads (ld.global.cg), for a
+// persistent kernel in which the same array is written by another CTA in an
+// earlier phase of the same launch.
+template <typename T, int VX, bool CG>
+__device__ __forceinline__ void ldf(T (&dst)[VX], const T *__restrict__ p) {
+    using V = typename VecT<T, VX>::type;
+    const V v = CG ? __ldcg(reinterpret_cast<const V *>(p)) : __ldg(reinterpret_cast<const V *>(p));
+    const T *s = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int q = 0; q < VX; q++) dst[q] = s[q];
+}
+template <typename T, bool CG>
+__device__ __forceinline__ T ldx(const T *__restrict__ p) {
+    return CG ? __ldcg(p) : __ldg(p);
+}
 template <typename T, int VX>
 __device__ __forceinline__ void ldv_rw(T (&dst)[VX], const T *__restrict__ p) {
     using V = typename VecT<T, VX>::type;
@@ -111,13 +128,13 @@ __device__ __forceinline__ void zerov(T (&d)[VX]) {
 // lane is active, else one scalar access per active lane.  A cell's psi is
 // read once, before its owner thread writes it, and by no other thread, so
 // the read-only path is valid.
-template <typename T, int VX>
+template <typename T, int VX, bool CG>
 __device__ __forceinline__ void ld_psi(T (&d)[VX], const T *__restrict__ p, int o, unsigned mask) {
     if (mask == (1u << VX) - 1u) {
-        ldv<T, VX>(d, p + o);
+        ldf<T, VX, CG>(d, p + o);
     } else {
 #pragma unroll
-        for (int v = 0; v < VX; v++) d[v] = (mask >> v & 1) ? __ldg(p + o + v) : T(0);
+        for (int v = 0; v < VX; v++) d[v] = (mask >> v & 1) ? ldx<T, CG>(p + o + v) : T(0);
     }
 }
 template <typename T, int VX>
@@ -167,8 +184,9 @@ constexpr int part_min_blocks() {
 }
 
 // ------------------------------------------------------------------ E phase
-template <typename T, int VX, int GM, bool ONE>
-__device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
+template <typename T, int VX, int GM, bool ONE, bool CG = false>
+__device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke,
+                                        int step = -1) {
     const long long sb = (long long)shot * a.fshot;
     const T *__restrict__ Ex = a.f[0] + sb;
     const T *__restrict__ Ey = a.f[1] + sb;
@@ -258,14 +276,14 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
     for (int q = 0; q < 3; q++) {
         const int kk = kb - 2 + q;
         if (!GZ || (kk >= 0 && kk < nz)) {
-            ldv<T, VX>(wx[q], Hx + kk * pz + col);
-            ldv<T, VX>(wy[q], Hy + kk * pz + col);
+            ldf<T, VX, CG>(wx[q], Hx + kk * pz + col);
+            ldf<T, VX, CG>(wy[q], Hy + kk * pz + col);
         } else {
             zerov<T, VX>(wx[q]);
             zerov<T, VX>(wy[q]);
         }
     }
-    const int slot = a.ring_k > 0 ? (*a.d_step) % a.ring_k : 0;
+    const int slot = a.ring_k > 0 ? (step >= 0 ? step : *a.d_step) % a.ring_k : 0;
 
     // ONE: this thread owns the single plane kb (a compile-time trip count
     // of one, so the window is three loads and a fourth, not a rotation)
@@ -275,8 +293,8 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         {
             const int kk = k + 1;
             if (!GZ || kk < nz) {
-                ldv<T, VX>(wx[3], Hx + kk * pz + col);
-                ldv<T, VX>(wy[3], Hy + kk * pz + col);
+                ldf<T, VX, CG>(wx[3], Hx + kk * pz + col);
+                ldf<T, VX, CG>(wy[3], Hy + kk * pz + col);
             } else {
                 zerov<T, VX>(wx[3]);
                 zerov<T, VX>(wy[3]);
@@ -286,14 +304,14 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         T hzx[3 * VX], hyx[3 * VX];
         {
             T t[VX];
-            ldv<T, VX>(t, Hz + c);
+            ldf<T, VX, CG>(t, Hz + c);
 #pragma unroll
             for (int v = 0; v < VX; v++) { hzx[VX + v] = t[v]; hyx[VX + v] = wy[2][v]; }
             if (has_l) {
-                ldv<T, VX>(t, Hz + c - VX);
+                ldf<T, VX, CG>(t, Hz + c - VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) hzx[v] = t[v];
-                ldv<T, VX>(t, Hy + c - VX);
+                ldf<T, VX, CG>(t, Hy + c - VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) hyx[v] = t[v];
             } else {
@@ -301,10 +319,10 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
                 for (int v = 0; v < VX; v++) { hzx[v] = T(0); hyx[v] = T(0); }
             }
             if (has_r) {
-                ldv<T, VX>(t, Hz + c + VX);
+                ldf<T, VX, CG>(t, Hz + c + VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) hzx[2 * VX + v] = t[v];
-                ldv<T, VX>(t, Hy + c + VX);
+                ldf<T, VX, CG>(t, Hy + c + VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) hyx[2 * VX + v] = t[v];
             } else {
@@ -314,12 +332,12 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         }
         T hzm2[VX], hzm1[VX], hzp1[VX], hxm2[VX], hxm1[VX], hxp1[VX];
         if (vy) {
-            ldv<T, VX>(hzm2, Hz + c - 2 * py);
-            ldv<T, VX>(hzm1, Hz + c - py);
-            ldv<T, VX>(hzp1, Hz + c + py);
-            ldv<T, VX>(hxm2, Hx + c - 2 * py);
-            ldv<T, VX>(hxm1, Hx + c - py);
-            ldv<T, VX>(hxp1, Hx + c + py);
+            ldf<T, VX, CG>(hzm2, Hz + c - 2 * py);
+            ldf<T, VX, CG>(hzm1, Hz + c - py);
+            ldf<T, VX, CG>(hzp1, Hz + c + py);
+            ldf<T, VX, CG>(hxm2, Hx + c - 2 * py);
+            ldf<T, VX, CG>(hxm1, Hx + c - py);
+            ldf<T, VX, CG>(hxp1, Hx + c + py);
         } else {
             zerov<T, VX>(hzm2); zerov<T, VX>(hzm1); zerov<T, VX>(hzp1);
             zerov<T, VX>(hxm2); zerov<T, VX>(hxm1); zerov<T, VX>(hxp1);
@@ -329,9 +347,9 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         // own cells: read once, before this thread writes them, and read by no
         // other thread in this phase, so the read-only path is valid and lets
         // the next plane's loads move above this plane's stores
-        ldv<T, VX>(ex, Ex + c);
-        ldv<T, VX>(ey, Ey + c);
-        ldv<T, VX>(ez, Ez + c);
+        ldf<T, VX, CG>(ex, Ex + c);
+        ldf<T, VX, CG>(ey, Ey + c);
+        ldf<T, VX, CG>(ez, Ez + c);
         T esh_z, ik_z;
         bool vz, kx, ky, kz;
         int lz;
@@ -364,17 +382,17 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
         if constexpr (GX) {
 #pragma unroll
             for (int v = 0; v < VX; v++) {
-                qx0[v] = (mx >> v & 1) ? __ldg(sx0 + ox + lx[v]) : T(0);
-                qx1[v] = (mx >> v & 1) ? __ldg(sx1 + ox + lx[v]) : T(0);
+                qx0[v] = (mx >> v & 1) ? ldx<T, CG>(sx0 + ox + lx[v]) : T(0);
+                qx1[v] = (mx >> v & 1) ? ldx<T, CG>(sx1 + ox + lx[v]) : T(0);
             }
         }
         if constexpr (GY) {
-            ld_psi<T, VX>(qy0, sy0, oy, my);
-            ld_psi<T, VX>(qy1, sy1, oy, my);
+            ld_psi<T, VX, CG>(qy0, sy0, oy, my);
+            ld_psi<T, VX, CG>(qy1, sy1, oy, my);
         }
         if constexpr (GZ) {
-            ld_psi<T, VX>(qz0, sz0, oz, mz);
-            ld_psi<T, VX>(qz1, sz1, oz, mz);
+            ld_psi<T, VX, CG>(qz0, sz0, oz, mz);
+            ld_psi<T, VX, CG>(qz1, sz1, oz, mz);
             be_z = __ldg(P + 18 * ps + k);
             ced_z = __ldg(P + 19 * ps + k);
         }
@@ -444,7 +462,7 @@ __device__ __forceinline__ void e_cells(const PhaseArgs<T> &a, int shot, int i0,
 }
 
 // ------------------------------------------------------------------ H phase
-template <typename T, int VX, int GM, bool ONE>
+template <typename T, int VX, int GM, bool ONE, bool CG = false>
 __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
     const long long sb = (long long)shot * a.fshot;
     const T *__restrict__ Ex = a.f[0] + sb;
@@ -536,8 +554,8 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
     for (int q = 0; q < 3; q++) {
         const int kk = kb - 1 + q;
         if (!GZ || (kk >= 0 && kk < nz)) {
-            ldv<T, VX>(wx[q], Ex + kk * pz + col);
-            ldv<T, VX>(wy[q], Ey + kk * pz + col);
+            ldf<T, VX, CG>(wx[q], Ex + kk * pz + col);
+            ldf<T, VX, CG>(wy[q], Ey + kk * pz + col);
         } else {
             zerov<T, VX>(wx[q]);
             zerov<T, VX>(wy[q]);
@@ -552,8 +570,8 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         {
             const int kk = k + 2;
             if (!GZ || kk < nz) {
-                ldv<T, VX>(wx[3], Ex + kk * pz + col);
-                ldv<T, VX>(wy[3], Ey + kk * pz + col);
+                ldf<T, VX, CG>(wx[3], Ex + kk * pz + col);
+                ldf<T, VX, CG>(wy[3], Ey + kk * pz + col);
             } else {
                 zerov<T, VX>(wx[3]);
                 zerov<T, VX>(wy[3]);
@@ -563,14 +581,14 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         T ezx[3 * VX], eyx[3 * VX];
         {
             T t[VX];
-            ldv<T, VX>(t, Ez + c);
+            ldf<T, VX, CG>(t, Ez + c);
 #pragma unroll
             for (int v = 0; v < VX; v++) { ezx[VX + v] = t[v]; eyx[VX + v] = wy[1][v]; }
             if (has_l) {
-                ldv<T, VX>(t, Ez + c - VX);
+                ldf<T, VX, CG>(t, Ez + c - VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) ezx[v] = t[v];
-                ldv<T, VX>(t, Ey + c - VX);
+                ldf<T, VX, CG>(t, Ey + c - VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) eyx[v] = t[v];
             } else {
@@ -578,10 +596,10 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
                 for (int v = 0; v < VX; v++) { ezx[v] = T(0); eyx[v] = T(0); }
             }
             if (has_r) {
-                ldv<T, VX>(t, Ez + c + VX);
+                ldf<T, VX, CG>(t, Ez + c + VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) ezx[2 * VX + v] = t[v];
-                ldv<T, VX>(t, Ey + c + VX);
+                ldf<T, VX, CG>(t, Ey + c + VX);
 #pragma unroll
                 for (int v = 0; v < VX; v++) eyx[2 * VX + v] = t[v];
             } else {
@@ -591,12 +609,12 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         }
         T ezm1[VX], ezp1[VX], ezp2[VX], exm1[VX], exp1[VX], exp2[VX];
         if (vy) {
-            ldv<T, VX>(ezm1, Ez + c - py);
-            ldv<T, VX>(ezp1, Ez + c + py);
-            ldv<T, VX>(ezp2, Ez + c + 2 * py);
-            ldv<T, VX>(exm1, Ex + c - py);
-            ldv<T, VX>(exp1, Ex + c + py);
-            ldv<T, VX>(exp2, Ex + c + 2 * py);
+            ldf<T, VX, CG>(ezm1, Ez + c - py);
+            ldf<T, VX, CG>(ezp1, Ez + c + py);
+            ldf<T, VX, CG>(ezp2, Ez + c + 2 * py);
+            ldf<T, VX, CG>(exm1, Ex + c - py);
+            ldf<T, VX, CG>(exp1, Ex + c + py);
+            ldf<T, VX, CG>(exp2, Ex + c + 2 * py);
         } else {
             zerov<T, VX>(ezm1); zerov<T, VX>(ezp1); zerov<T, VX>(ezp2);
             zerov<T, VX>(exm1); zerov<T, VX>(exp1); zerov<T, VX>(exp2);
@@ -610,9 +628,9 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
             for (int v = 0; v < VX; v++) dm[v] = a.dtmu0;
         }
         // own cells: read once before being written, by this thread only
-        ldv<T, VX>(hx, Hx + c);
-        ldv<T, VX>(hy, Hy + c);
-        ldv<T, VX>(hz, Hz + c);
+        ldf<T, VX, CG>(hx, Hx + c);
+        ldf<T, VX, CG>(hy, Hy + c);
+        ldf<T, VX, CG>(hz, Hz + c);
         T msh_z, ik_z;
         bool vz, kx, ky, kz;
         int lz;
@@ -645,17 +663,17 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
         if constexpr (GX) {
 #pragma unroll
             for (int v = 0; v < VX; v++) {
-                qx0[v] = (mx >> v & 1) ? __ldg(sx0 + ox + lx[v]) : T(0);
-                qx1[v] = (mx >> v & 1) ? __ldg(sx1 + ox + lx[v]) : T(0);
+                qx0[v] = (mx >> v & 1) ? ldx<T, CG>(sx0 + ox + lx[v]) : T(0);
+                qx1[v] = (mx >> v & 1) ? ldx<T, CG>(sx1 + ox + lx[v]) : T(0);
             }
         }
         if constexpr (GY) {
-            ld_psi<T, VX>(qy0, sy0, oy, my);
-            ld_psi<T, VX>(qy1, sy1, oy, my);
+            ld_psi<T, VX, CG>(qy0, sy0, oy, my);
+            ld_psi<T, VX, CG>(qy1, sy1, oy, my);
         }
         if constexpr (GZ) {
-            ld_psi<T, VX>(qz0, sz0, oz, mz);
-            ld_psi<T, VX>(qz1, sz1, oz, mz);
+            ld_psi<T, VX, CG>(qz0, sz0, oz, mz);
+            ld_psi<T, VX, CG>(qz1, sz1, oz, mz);
             bh_z = __ldg(P + 20 * ps + k);
             chd_z = __ldg(P + 21 * ps + k);
         }

@@ -4,14 +4,20 @@ Requests (each its own model, grid, shots, receivers and time base) arrive
 over time.  The server keeps ``n_slots`` worker slots; a waiting request is
 admitted as soon as a slot is free and its device-memory estimate fits what
 is left of the HBM budget (first come first served, but a request that does
-not fit lets later, smaller ones go ahead).  Each slot owns a solver handle,
-and with it a CUDA stream, so admitted requests run concurrently on the GPU;
-a slot keeps its handle (model, fields and psi slabs resident on the device)
-and reuses it for the next request of the same grid.  The C-ABI calls release
-the GIL, so slots are host threads.
+not fit lets later, smaller ones go ahead).  Each slot owns solver handles,
+and with them CUDA streams, so admitted requests run concurrently on the GPU.
 
-Latency = completion - arrival.  ``serial_latencies`` gives the plain path
-for comparison: one request at a time, in arrival order, on one handle.
+A slot keeps one handle per grid it has served (model, fields and psi slabs
+stay resident on the device) and reuses it for the next request of that
+grid, so switching grids never frees device memory: a freed buffer would
+synchronise the whole device and stall the other slots' streams.  The memory
+those idle handles hold counts against the budget; a request that does not
+fit otherwise evicts idle handles of free slots, least recently used first.
+The C-ABI calls release the GIL, so slots are host threads.
+
+Latency = completion - arrival.  ``serial_latencies`` gives a plain path
+for comparison from measured service times: one request at a time, in
+arrival order.
 """
 from __future__ import annotations
 
@@ -70,19 +76,22 @@ def estimate_bytes(wl, mode: str = "forward", checkpoint_every: int = 200) -> in
     return int(b)
 
 
-def run_request(solver_cache: dict, req: Request):
-    """Default executor: solve one request on a cached handle of its grid."""
-    from dataclasses import replace
+def grid_key(wl):
+    """Handles are interchangeable between requests with the same key."""
+    cp = wl.cp
+    return (cp.nx, cp.ny, cp.nz, cp.precision, cp.flavor, cp.dx, cp.dy, cp.dz, cp.dt, cp.cmax, cp.ncpml, cp.mu0,
+            cp.omega0, cp.device)
 
+
+def run_request(solver_cache: dict, req: Request):
+    """Default executor: solve one request on the cached handle of its grid
+    (created on first use; handles of other grids stay cached)."""
     from .solver import MittetSolver
 
     wl = req.workload
-    key = (wl.cp.nx, wl.cp.ny, wl.cp.nz, wl.cp.precision, wl.cp.flavor, wl.cp.dx, wl.cp.dt, wl.cp.cmax,
-           wl.cp.ncpml, wl.cp.device)
+    key = grid_key(wl)
     s = solver_cache.get(key)
     if s is None:
-        for k in list(solver_cache):
-            solver_cache.pop(k).close()
         s = MittetSolver(wl.cp)
         solver_cache[key] = s
     s.set_model(wl.sigma, wl.mu)
@@ -102,16 +111,31 @@ def run_request(solver_cache: dict, req: Request):
     return spec
 
 
+def _default_key(req):
+    try:
+        return grid_key(req.workload)
+    except AttributeError:
+        return None
+
+
 class MittetServer:
     def __init__(self, n_slots: int = 4, hbm_budget: float = 150e9,
-                 executor: Optional[Callable] = None, estimator: Optional[Callable] = None):
+                 executor: Optional[Callable] = None, estimator: Optional[Callable] = None,
+                 keyer: Optional[Callable] = None, resident_estimator: Optional[Callable] = None):
         self.n_slots = n_slots
         self.budget = float(hbm_budget)
         self.executor = executor or run_request
         self.estimator = estimator or (lambda r: estimate_bytes(r.workload, r.mode, r.checkpoint_every))
+        # the handle a request leaves cached: its forward state (gradient
+        # buffers are released at the end of a gradient request)
+        self.resident_estimator = resident_estimator or (
+            estimator if estimator is not None else (lambda r: estimate_bytes(r.workload, "forward")))
+        self.keyer = keyer or _default_key
         self._lock = threading.Condition()
         self.peak_in_use = 0.0
         self.max_concurrent = 0
+        self.evictions = 0
+        self.reuses = 0
 
     def run(self, requests: list, realtime: bool = True) -> list:
         """Serve ``requests`` (sorted by arrival); returns one Result per request."""
@@ -120,15 +144,20 @@ class MittetServer:
             if self.estimator(r) > self.budget:
                 raise ValueError(f"request {r.rid} needs more than the whole HBM budget")
         t0 = time.perf_counter()
-        now = lambda: time.perf_counter() - t0
+        now = lambda: time.perf_counter() - t0  # noqa: E731
         waiting: list = []
         results: dict = {}
         free_slots = list(range(self.n_slots))
         caches = [dict() for _ in range(self.n_slots)]
-        state = {"in_use": 0.0, "running": 0}
+        resident: dict = {}   # (slot, key) -> bytes the cached handle holds
+        last_use: dict = {}   # (slot, key) -> time of its last request
+        state = {"extra": 0.0, "running": 0}
         threads = []
 
-        def worker(slot, req, need, start):
+        def held():
+            return state["extra"] + sum(resident.values())
+
+        def worker(slot, req, key, extra, start):
             out, err = None, None
             try:
                 out = self.executor(caches[slot], req)
@@ -137,10 +166,26 @@ class MittetServer:
             done = now()
             with self._lock:
                 results[req.rid] = Result(req.rid, req.arrival, start, done, slot, out, err)
-                state["in_use"] -= need
+                state["extra"] -= extra
+                if key is not None:
+                    resident[(slot, key)] = max(resident.get((slot, key), 0.0), float(self.resident_estimator(req)))
+                    last_use[(slot, key)] = done
                 state["running"] -= 1
                 free_slots.append(slot)
                 self._lock.notify_all()
+
+        def evict_for(amount, keep):
+            """Close idle cached handles of free slots (LRU) until ``amount``
+            more bytes fit; False if they cannot."""
+            cands = sorted((k for k in resident if k[0] in free_slots and k != keep), key=lambda k: last_use.get(k, 0))
+            while held() + amount > self.budget and cands:
+                k = cands.pop(0)
+                h = caches[k[0]].pop(k[1], None)
+                if h is not None and hasattr(h, "close"):
+                    h.close()
+                resident.pop(k, None)
+                self.evictions += 1
+            return held() + amount <= self.budget
 
         pending = list(reqs)
         with self._lock:
@@ -155,19 +200,26 @@ class MittetServer:
                     for r in list(waiting):
                         if not free_slots:
                             break
-                        need = self.estimator(r)
-                        if state["in_use"] + need <= self.budget:
-                            waiting.remove(r)
-                            slot = free_slots.pop(0)
-                            state["in_use"] += need
-                            state["running"] += 1
-                            self.peak_in_use = max(self.peak_in_use, state["in_use"])
-                            self.max_concurrent = max(self.max_concurrent, state["running"])
-                            th = threading.Thread(target=worker, args=(slot, r, need, now()), daemon=True)
-                            threads.append(th)
-                            th.start()
-                            admitted = True
-                            break
+                        need = float(self.estimator(r))
+                        key = self.keyer(r)
+                        # a free slot that already holds this grid's handle first
+                        slot = next((s for s in free_slots if (s, key) in resident), free_slots[0])
+                        extra = max(0.0, need - resident.get((slot, key), 0.0))
+                        if held() + extra > self.budget and not evict_for(extra, (slot, key)):
+                            continue
+                        waiting.remove(r)
+                        free_slots.remove(slot)
+                        if (slot, key) in resident:
+                            self.reuses += 1
+                        state["extra"] += extra
+                        state["running"] += 1
+                        self.peak_in_use = max(self.peak_in_use, held())
+                        self.max_concurrent = max(self.max_concurrent, state["running"])
+                        th = threading.Thread(target=worker, args=(slot, r, key, extra, now()), daemon=True)
+                        threads.append(th)
+                        th.start()
+                        admitted = True
+                        break
                 if not pending and not waiting and state["running"] == 0:
                     break
                 timeout = None
@@ -178,7 +230,8 @@ class MittetServer:
             th.join()
         for c in caches:
             for s in c.values():
-                s.close()
+                if hasattr(s, "close"):
+                    s.close()
         return [results[r.rid] for r in reqs]
 
 

@@ -285,6 +285,16 @@ class MittetSolver:
     def launch_count(self) -> int:
         return int(self._lib.mittet_last_launch_count(self._h))
 
+    def launch_path(self) -> dict:
+        """The time loop of the last forward: {"persistent": False} for the
+        stepped graph of part kernels, else the stencil variant [VX, BX, BY,
+        ZC] of the persistent multi-shot launch and its CTAs."""
+        v, g = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.mittet_persistent_variant(self._h, ctypes.byref(v), ctypes.byref(g)))
+        if v.value < 0:
+            return {"persistent": False}
+        return {"persistent": True, "variant": stencil_variants(self.cp.precision == FP64)[v.value], "ctas": g.value}
+
 
 def stencil_variants(fp64: bool = False) -> list:
     """The stencil variants the autotuner chooses from, as [VX, BX, BY, ZC]

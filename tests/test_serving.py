@@ -68,3 +68,48 @@ def test_serial_latency_model():
     lat = serial_latencies(reqs, {0: 1.0, 1: 1.0, 2: 1.0})
     assert lat == {0: 1.0, 1: 1.5, 2: 2.4}
     assert percentile([1, 2, 3, 4], 50) == 2.5
+
+
+def test_slots_keep_handles_per_grid_within_the_budget():
+    """Idle handles of every grid a slot served stay cached and count against
+    the budget; a request of a cached grid reuses its slot's handle, and one
+    that does not fit next to the cached handles evicts idle ones (LRU)."""
+    lock = threading.Lock()
+    made = []
+
+    class Handle:
+        def __init__(self, key, size):
+            self.key, self.size, self.closed = key, size, False
+
+        def close(self):
+            self.closed = True
+
+    live = {"bytes": 0, "peak": 0}
+
+    def held_now(caches_seen):
+        return sum(h.size for h in caches_seen if not h.closed)
+
+    def execu(cache, req):
+        with lock:
+            h = cache.get(req.key)
+            if h is None:
+                h = Handle(req.key, req.size)
+                cache[req.key] = h
+                made.append(h)
+            live["peak"] = max(live["peak"], held_now(made))
+        time.sleep(0.01)
+        return req.rid
+
+    reqs = []
+    for i in range(16):
+        r = make(i, 0.02 * i, size=(40 if i % 4 == 3 else 20))
+        r.key = "big" if i % 4 == 3 else ("a" if i % 2 else "b")
+        reqs.append(r)
+    srv = MittetServer(n_slots=2, hbm_budget=100, executor=execu, estimator=lambda r: r.size,
+                       keyer=lambda r: r.key, resident_estimator=lambda r: r.size)
+    res = srv.run(reqs)
+    assert sorted(r.output for r in res) == list(range(16))
+    assert srv.peak_in_use <= 100 and live["peak"] <= 100
+    assert srv.reuses > 0
+    # fewer handles than requests were created: slots reused them
+    assert len(made) < len(reqs)
