@@ -277,6 +277,13 @@ int mittet_stencil_variants(int32_t fp64, int32_t *count, int32_t *cfg, int32_t 
  * counterpart in the reference (a tuning introspection). */
 int mittet_persistent_variant(mittet_handle *h, int32_t *variant, int32_t *grid);
 
+/* Whether each phase launches its four boundary parts (x, y, z faces and
+ * the edges) as one merged launch: the stencil variant it uses (index as in
+ * mittet_stencil_variants) for the E and H phase, -1 for four launches.
+ * Chosen by the autotuner on the whole phase.  No counterpart in the
+ * reference (a tuning introspection). */
+int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_variant);
+
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);
 

@@ -221,6 +221,150 @@ __global__ void __launch_bounds__(256, kOwnMinBlocks<T>()) adj_h_own_kernel(AdjA
     if (ch) { a.lam[3][c] = lam[0]; a.lam[4][c] = lam[1]; a.lam[5][c] = lam[2]; }
 }
 
+// h_own_cell for the cells of one box of the phase's tile map (stencil.cuh
+// TileMap): along an axis whose bit is clear in GM every cell of the box is
+// interior (no profile, no psi slab, inside every update range), so the
+// general path drops that axis's profile loads, range and slab tests at
+// compile time; GM = 0 is the interior body.  The arithmetic of every term
+// is the same as in h_own_cell, so the results are bit-identical.
+template <typename T, int GM>
+__device__ __forceinline__ bool h_own_cell_gm(const AdjArgs<T> &a, int i, int j, int k, int shot, long long c,
+                                              long long cm, T L0, T L1, T L2, T dm, T (&mu)[7], T (&lam)[3]) {
+    constexpr bool G[3] = {(GM & 1) != 0, (GM & 2) != 0, (GM & 4) != 0};
+    const T s = a.sgn;
+    lam[0] = L0; lam[1] = L1; lam[2] = L2;
+    if constexpr (GM == 0) {
+        mu[0] = -s * dm * a.ik[1] * L0;
+        mu[1] = s * dm * a.ik[2] * L0;
+        mu[2] = -s * dm * a.ik[2] * L1;
+        mu[3] = s * dm * a.ik[0] * L1;
+        mu[4] = T(0);
+        mu[5] = -s * dm * a.ik[0] * L2;
+        mu[6] = s * dm * a.ik[1] * L2;
+        return false;
+    } else {
+        const int v3[3] = {i, j, k};
+        const T m = a.m[cm];
+        T msh[3], ik[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            msh[q] = G[q] ? pget(a, q, 1, v3[q]) : T(0);
+            ik[q] = G[q] ? pget(a, q, 7, v3[q]) : a.ik[q];
+        }
+        T da[3], db[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            if (G[q] && msh[q] != T(0)) {
+                const T h = msh[q] * m;
+                const T r = rcp(T(1) + h);
+                da[q] = (T(1) - h) * r;
+                db[q] = dm * r;
+            } else {
+                da[q] = T(1);
+                db[q] = dm;
+            }
+        }
+        auto in_gm = [&](const DBox &b) {
+            bool in = true;
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                if (G[q]) in = in && v3[q] >= b.lo[q] && v3[q] < b.hi[q];
+            return in;
+        };
+        const bool in0 = in_gm(a.upd[0]), in1 = in_gm(a.upd[1]), in2 = in_gm(a.upd[2]);
+        T mu0 = in0 ? -s * db[0] * ik[1] * L0 : T(0);
+        T mu1 = in0 ? s * db[0] * ik[2] * L0 : T(0);
+        T mu2 = in1 ? -s * db[1] * ik[2] * L1 : T(0);
+        T mu3 = in1 ? s * db[1] * ik[0] * L1 : T(0);
+        T mu4 = T(0);
+        T mu5 = in2 ? -s * db[2] * ik[0] * L2 : T(0);
+        T mu6 = in2 ? s * db[2] * ik[1] * L2 : T(0);
+        if (G[0]) {
+            const int lx = slab_local(a.slab[0], i);
+            if (lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1] && k >= a.slab[0].other.lo[2] &&
+                k < a.slab[0].other.hi[2]) {
+                const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
+                const T bh = pget(a, 0, 4, i), chd = pget(a, 0, 5, i);
+                const T lzx = fma(-db[2], L2, a.lpsi[0][0][o]);
+                const T lyx = fma(db[1], L1, a.lpsi[0][1][o]);
+                a.lpsi[0][0][o] = bh * lzx;
+                a.lpsi[0][1][o] = bh * lyx;
+                mu5 = fma(chd, lzx, mu5);
+                mu4 = fma(chd, lyx, mu4);
+            }
+        }
+        if (G[1]) {
+            const int ly = slab_local(a.slab[1], j);
+            if (ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0] && k >= a.slab[1].other.lo[2] &&
+                k < a.slab[1].other.hi[2]) {
+                const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
+                const T bh = pget(a, 1, 4, j), chd = pget(a, 1, 5, j);
+                const T lxy = fma(-db[0], L0, a.lpsi[1][0][o]);
+                const T lzy = fma(db[2], L2, a.lpsi[1][1][o]);
+                a.lpsi[1][0][o] = bh * lxy;
+                a.lpsi[1][1][o] = bh * lzy;
+                mu0 = fma(chd, lxy, mu0);
+                mu6 = fma(chd, lzy, mu6);
+            }
+        }
+        if (G[2]) {
+            const int lz = slab_local(a.slab[2], k);
+            if (lz >= 0 && i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
+                j < a.slab[2].other.hi[1]) {
+                const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
+                const T bh = pget(a, 2, 4, k), chd = pget(a, 2, 5, k);
+                const T lyz = fma(-db[1], L1, a.lpsi[2][0][o]);
+                const T lxz = fma(db[0], L0, a.lpsi[2][1][o]);
+                a.lpsi[2][0][o] = bh * lyz;
+                a.lpsi[2][1][o] = bh * lxz;
+                mu2 = fma(chd, lyz, mu2);
+                mu1 = fma(chd, lxz, mu1);
+            }
+        }
+        mu[0] = mu0; mu[1] = mu1; mu[2] = mu2; mu[3] = mu3; mu[4] = mu4; mu[5] = mu5; mu[6] = mu6;
+        double gsum = 0.0;
+        const double isig = (double)m * a.inv2w0dt;
+        const bool in[3] = {in0, in1, in2};
+        const T L[3] = {L0, L1, L2};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            if (!G[q] || msh[q] == T(0)) continue;
+            const double h = (double)msh[q] * (double)m;
+            const double r = 1.0 / (1.0 + h);
+            const double dda = 2.0 * h * isig * r * r;
+            const double rdb = h * isig * r;
+            const double h0 = (double)a.H0[q][c], h1 = (double)a.H1[q][c];
+            const double d = in[q] ? fma(-(double)da[q], h0, h1) : h1 - h0;
+            gsum = fma((double)L[q], fma(rdb, d, in[q] ? dda * h0 : 0.0), gsum);
+        }
+        if (gsum != 0.0) a.grad[c] += gsum;
+        lam[0] = in0 ? da[0] * L0 : L0;
+        lam[1] = in1 ? da[1] * L1 : L1;
+        lam[2] = in2 ? da[2] * L2 : L2;
+        return true;
+    }
+}
+
+// The cells of the boxes [q0, q1) of the H phase's one-cell tile map, one
+// thread per cell (tiles [first, first + gridDim.x), blockIdx.y = shot).
+template <typename T, int GM>
+__global__ void __launch_bounds__(256, kOwnMinBlocks<T>())
+    adj_h_own_part_kernel(AdjArgs<T> a, const TileMap *__restrict__ tm, int first, int q0, int q1) {
+    int i, j, kb, ke;
+    bool inside;
+    locate<1, 32, 8>(tm, q0, q1, first + blockIdx.x, i, j, kb, ke, inside);
+    if (!inside) return;
+    const int shot = blockIdx.y, k = kb;
+    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
+    const long long c = (long long)shot * a.fshot + cm;
+    const T dm = a.dtmu ? a.dtmu[cm] : a.dtmu0;
+    T mu[7], lam[3];
+    const bool ch = h_own_cell_gm<T, GM>(a, i, j, k, shot, c, cm, a.lam[3][c], a.lam[4][c], a.lam[5][c], dm, mu, lam);
+#pragma unroll
+    for (int w = 0; w < 7; w++) a.mu[w][c] = mu[w];
+    if (ch) { a.lam[3][c] = lam[0]; a.lam[4][c] = lam[1]; a.lam[5][c] = lam[2]; }
+}
+
 // Taps [u, u-1, u-2, u+1] of one weight array along one axis (stride s).
 template <typename T>
 __device__ __forceinline__ void taps_p(const T *__restrict__ mu, long long c, long long s, int v, int n, T (&t)[4]) {
@@ -394,6 +538,151 @@ __global__ void __launch_bounds__(256, kOwnMinBlocks<T>()) adj_e_own_kernel(AdjA
     double g = a.grad[c];
     T mu[6], lam[3];
     const bool ch = e_own_cell(a, i, j, k, shot, a.m[cm], a.lam[0][c], a.lam[1][c], a.lam[2][c], e0, e1, g, mu, lam);
+    a.grad[c] = g;
+#pragma unroll
+    for (int w = 0; w < 6; w++) a.mu[w][c] = mu[w];
+    if (ch) { a.lam[0][c] = lam[0]; a.lam[1][c] = lam[1]; a.lam[2][c] = lam[2]; }
+}
+
+// e_own_cell for the cells of one box of the E phase's tile map, with the
+// axes not in GM interior at compile time (see h_own_cell_gm); GM = 0 is
+// the interior body.  Bit-identical to e_own_cell.
+template <typename T, int GM>
+__device__ __forceinline__ bool e_own_cell_gm(const AdjArgs<T> &a, int i, int j, int k, int shot, T m, T L0, T L1,
+                                              T L2, const T (&e0)[3], const T (&e1)[3], double &g, T (&mu)[6],
+                                              T (&lam)[3]) {
+    constexpr bool G[3] = {(GM & 1) != 0, (GM & 2) != 0, (GM & 4) != 0};
+    const T s = a.sgn;
+    lam[0] = L0; lam[1] = L1; lam[2] = L2;
+    const T L[3] = {L0, L1, L2};
+    const double isig = (double)m * a.inv2w0dt;
+    if constexpr (GM == 0) {
+        mu[0] = s * m * a.ik[1] * L0;
+        mu[1] = -s * m * a.ik[2] * L0;
+        mu[2] = s * m * a.ik[2] * L1;
+        mu[3] = -s * m * a.ik[0] * L1;
+        mu[4] = s * m * a.ik[0] * L2;
+        mu[5] = -s * m * a.ik[1] * L2;
+        const double rcb = -isig;
+        double gsum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; q++) gsum = fma((double)L[q], rcb * ((double)e1[q] - (double)e0[q]), gsum);
+        g += gsum;
+        return false;
+    } else {
+        const int v3[3] = {i, j, k};
+        T esh[3], ik[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            esh[q] = G[q] ? pget(a, q, 0, v3[q]) : T(0);
+            ik[q] = G[q] ? pget(a, q, 6, v3[q]) : a.ik[q];
+        }
+        T ca[3], cb[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            if (G[q] && esh[q] != T(0)) {
+                const T h = esh[q] * m;
+                const T r = rcp(T(1) + h);
+                ca[q] = (T(1) - h) * r;
+                cb[q] = m * r;
+            } else {
+                ca[q] = T(1);
+                cb[q] = m;
+            }
+        }
+        auto in_gm = [&](const DBox &b) {
+            bool in = true;
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                if (G[q]) in = in && v3[q] >= b.lo[q] && v3[q] < b.hi[q];
+            return in;
+        };
+        const bool in0 = in_gm(a.upd[0]), in1 = in_gm(a.upd[1]), in2 = in_gm(a.upd[2]);
+        T mu0 = in0 ? s * cb[0] * ik[1] * L0 : T(0);
+        T mu1 = in0 ? -s * cb[0] * ik[2] * L0 : T(0);
+        T mu2 = in1 ? s * cb[1] * ik[2] * L1 : T(0);
+        T mu3 = in1 ? -s * cb[1] * ik[0] * L1 : T(0);
+        T mu4 = in2 ? s * cb[2] * ik[0] * L2 : T(0);
+        T mu5 = in2 ? -s * cb[2] * ik[1] * L2 : T(0);
+        if (G[0]) {
+            const int lx = slab_local(a.slab[0], i);
+            if (lx >= 0 && j >= a.slab[0].other.lo[1] && j < a.slab[0].other.hi[1] && k >= a.slab[0].other.lo[2] &&
+                k < a.slab[0].other.hi[2]) {
+                const long long o = (long long)shot * a.pshot[0] + ((long long)k * a.ny + j) * a.slab[0].width + lx;
+                const T be = pget(a, 0, 2, i), ced = pget(a, 0, 3, i);
+                const T lzx = fma(cb[2], L2, a.lpsi[0][0][o]);
+                const T lyx = fma(-cb[1], L1, a.lpsi[0][1][o]);
+                a.lpsi[0][0][o] = be * lzx;
+                a.lpsi[0][1][o] = be * lyx;
+                mu4 = fma(ced, lzx, mu4);
+                mu3 = fma(ced, lyx, mu3);
+            }
+        }
+        if (G[1]) {
+            const int ly = slab_local(a.slab[1], j);
+            if (ly >= 0 && i >= a.slab[1].other.lo[0] && i < a.slab[1].other.hi[0] && k >= a.slab[1].other.lo[2] &&
+                k < a.slab[1].other.hi[2]) {
+                const long long o = (long long)shot * a.pshot[1] + ((long long)k * a.slab[1].width + ly) * a.px + i;
+                const T be = pget(a, 1, 2, j), ced = pget(a, 1, 3, j);
+                const T lxy = fma(cb[0], L0, a.lpsi[1][0][o]);
+                const T lzy = fma(-cb[2], L2, a.lpsi[1][1][o]);
+                a.lpsi[1][0][o] = be * lxy;
+                a.lpsi[1][1][o] = be * lzy;
+                mu0 = fma(ced, lxy, mu0);
+                mu5 = fma(ced, lzy, mu5);
+            }
+        }
+        if (G[2]) {
+            const int lz = slab_local(a.slab[2], k);
+            if (lz >= 0 && i >= a.slab[2].other.lo[0] && i < a.slab[2].other.hi[0] && j >= a.slab[2].other.lo[1] &&
+                j < a.slab[2].other.hi[1]) {
+                const long long o = (long long)shot * a.pshot[2] + ((long long)lz * a.ny + j) * a.px + i;
+                const T be = pget(a, 2, 2, k), ced = pget(a, 2, 3, k);
+                const T lyz = fma(cb[1], L1, a.lpsi[2][0][o]);
+                const T lxz = fma(-cb[0], L0, a.lpsi[2][1][o]);
+                a.lpsi[2][0][o] = be * lyz;
+                a.lpsi[2][1][o] = be * lxz;
+                mu2 = fma(ced, lyz, mu2);
+                mu1 = fma(ced, lxz, mu1);
+            }
+        }
+        mu[0] = mu0; mu[1] = mu1; mu[2] = mu2; mu[3] = mu3; mu[4] = mu4; mu[5] = mu5;
+        const bool in[3] = {in0, in1, in2};
+        double gsum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const bool prof = G[q] && esh[q] != T(0);
+            const double h = (double)esh[q] * (double)m;
+            const double r = prof ? 1.0 / (1.0 + h) : 1.0;
+            const double dca = prof ? 2.0 * h * isig * r * r : 0.0;
+            const double rcb = -isig * r;
+            const double x0 = (double)e0[q], x1 = (double)e1[q];
+            const double d = in[q] ? fma(-(double)ca[q], x0, x1) : x1 - x0;
+            gsum = fma((double)L[q], fma(rcb, d, in[q] ? dca * x0 : 0.0), gsum);
+        }
+        g += gsum;
+        lam[0] = in0 ? ca[0] * L0 : L0;
+        lam[1] = in1 ? ca[1] * L1 : L1;
+        lam[2] = in2 ? ca[2] * L2 : L2;
+        return true;
+    }
+}
+
+template <typename T, int GM>
+__global__ void __launch_bounds__(256, kOwnMinBlocks<T>())
+    adj_e_own_part_kernel(AdjArgs<T> a, const TileMap *__restrict__ tm, int first, int q0, int q1) {
+    int i, j, kb, ke;
+    bool inside;
+    locate<1, 32, 8>(tm, q0, q1, first + blockIdx.x, i, j, kb, ke, inside);
+    if (!inside) return;
+    const int shot = blockIdx.y, k = kb;
+    const long long cm = (long long)k * a.plane + (long long)j * a.px + i;
+    const long long c = (long long)shot * a.fshot + cm;
+    const T e0[3] = {a.E0[0][c], a.E0[1][c], a.E0[2][c]}, e1[3] = {a.E1[0][c], a.E1[1][c], a.E1[2][c]};
+    double g = a.grad[c];
+    T mu[6], lam[3];
+    const bool ch = e_own_cell_gm<T, GM>(a, i, j, k, shot, a.m[cm], a.lam[0][c], a.lam[1][c], a.lam[2][c], e0, e1, g,
+                                         mu, lam);
     a.grad[c] = g;
 #pragma unroll
     for (int w = 0; w < 6; w++) a.mu[w][c] = mu[w];

@@ -30,7 +30,7 @@ struct DBox {
     int lo[3], hi[3];
 };
 struct DSlab {
-    int nlo, nhi, flo, fhi, width;
+    int nlo, nhi, flo, fhi, width, fofs;  // see Slab (setup_host.h)
     DBox other;
 };
 
@@ -87,7 +87,7 @@ __device__ __forceinline__ bool in_box(const DBox &b, int i, int j, int k) {
 // Local index along the slab axis, or -1 if v is in neither interval.
 __device__ __forceinline__ int slab_local(const DSlab &s, int v) {
     if (v >= s.nlo && v < s.nhi) return v - s.nlo;
-    if (v >= s.flo && v < s.fhi) return (s.nhi - s.nlo) + (v - s.flo);
+    if (v >= s.flo && v < s.fhi) return s.fofs + (v - s.flo);
     return -1;
 }
 

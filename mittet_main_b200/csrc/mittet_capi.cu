@@ -87,7 +87,7 @@ DBox to_dbox(const Box &b) {
 }
 DSlab to_dslab(const Slab &s) {
     DSlab d;
-    d.nlo = s.nlo; d.nhi = s.nhi; d.flo = s.flo; d.fhi = s.fhi; d.width = s.width;
+    d.nlo = s.nlo; d.nhi = s.nhi; d.flo = s.flo; d.fhi = s.fhi; d.width = s.width; d.fofs = s.fofs;
     d.other = to_dbox(s.other);
     return d;
 }
@@ -147,8 +147,11 @@ struct mittet_handle_s {
     int ibox[2][6] = {{0}};    // interior box of each phase: lo xyz, hi xyz
     bool has_ibox[2] = {false, false};
     int ldg_int[2] = {0, 0};   // best plain-load interior variant of each phase
+    int merge_b[2] = {-1, -1}; // variant of the merged boundary launch of each phase (-1: four part launches)
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
     std::vector<TileMap> tmaps_host;
+    DevBuf adj_tmaps;          // one-cell tile maps (32 x 8 x 1) of the E and H phase: the adjoint own kernels
+    TileMap adj_tm_host[2];
     int ptile[64][kParts + 1] = {{0}};  // per (variant, phase): part p is tiles [ptile[p], ptile[p+1])
     bool tuned = false;
     DevBuf ring, acc;
@@ -444,7 +447,39 @@ int upload_tilemaps(mittet_handle *h) {
     h->tmaps_host = maps;
     CK(h->tmaps.ensure(maps.size() * sizeof(TileMap)));
     CK(cudaMemcpy(h->tmaps.p, maps.data(), maps.size() * sizeof(TileMap), cudaMemcpyHostToDevice));
+    h->adj_tm_host[0] = make_tilemap(h, true, 1, 32, 8, 1);
+    h->adj_tm_host[1] = make_tilemap(h, false, 1, 32, 8, 1);
+    CK(h->adj_tmaps.ensure(2 * sizeof(TileMap)));
+    CK(cudaMemcpy(h->adj_tmaps.p, h->adj_tm_host, 2 * sizeof(TileMap), cudaMemcpyHostToDevice));
     return MITTET_OK;
+}
+
+// The adjoint own kernels of one phase over its five parts (one-cell tiles,
+// the forward's boxes, so each part drops the CPML logic of the axes it is
+// interior along), concurrently on the part streams like a forward phase.
+template <typename T>
+void launch_adj_own(mittet_handle *h, bool e, const AdjArgs<T> &a, int nshot) {
+    using K = void (*)(AdjArgs<T>, const TileMap *, int, int, int);
+    static const K ke[kParts] = {adj_e_own_part_kernel<T, 0>, adj_e_own_part_kernel<T, 1>,
+                                 adj_e_own_part_kernel<T, 2>, adj_e_own_part_kernel<T, 4>,
+                                 adj_e_own_part_kernel<T, 7>};
+    static const K kh[kParts] = {adj_h_own_part_kernel<T, 0>, adj_h_own_part_kernel<T, 1>,
+                                 adj_h_own_part_kernel<T, 2>, adj_h_own_part_kernel<T, 4>,
+                                 adj_h_own_part_kernel<T, 7>};
+    const TileMap &tm = h->adj_tm_host[e ? 0 : 1];
+    const TileMap *dtm = h->adj_tmaps.as<TileMap>() + (e ? 0 : 1);
+    cudaEventRecord(h->ev_fork, h->st);
+    for (int p = 1; p < kParts; p++) cudaStreamWaitEvent(h->pst[p], h->ev_fork, 0);
+    for (int p = kParts - 1; p >= 0; p--) {
+        const int first = tm.start[tm.pbox[p]], last = tm.start[tm.pbox[p + 1]];
+        if (last <= first) continue;
+        cudaStream_t st = p == 0 ? h->st : h->pst[p];
+        (e ? ke : kh)[p]<<<dim3(last - first, nshot), dim3(32, 8), 0, st>>>(a, dtm, first, tm.pbox[p], tm.pbox[p + 1]);
+    }
+    for (int p = 1; p < kParts; p++) {
+        cudaEventRecord(h->ev_join[p], h->pst[p]);
+        cudaStreamWaitEvent(h->st, h->ev_join[p], 0);
+    }
 }
 
 // ------------------------------------------------- TMA-staged interior
@@ -591,6 +626,32 @@ bool tma_usable(const mittet_handle *h, const PhaseArgs<T> &a) {
            a.fo[3] == a.f[3] && a.m == h->m.as<T>();
 }
 
+template <typename T>
+using BoundaryKernel = void (*)(PhaseArgs<T>, const TileMap *, int, int, int);
+
+// The merged boundary kernels (stencil.cuh boundary_kernel), by thread shape.
+template <typename T>
+BoundaryKernel<T> boundary_kernel_for(int vx, int bx, int by, bool e) {
+    if (vx == 2 && bx == 32 && by == 4) return e ? boundary_kernel<T, 2, 32, 4, true> : boundary_kernel<T, 2, 32, 4, false>;
+    if (vx == 2 && bx == 16 && by == 8) return e ? boundary_kernel<T, 2, 16, 8, true> : boundary_kernel<T, 2, 16, 8, false>;
+    if (vx == 2 && bx == 8 && by == 16) return e ? boundary_kernel<T, 2, 8, 16, true> : boundary_kernel<T, 2, 8, 16, false>;
+    return nullptr;
+}
+
+// The four boundary parts of a phase as one launch of variant vi's tiles.
+template <typename T>
+int launch_boundary(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a, cudaStream_t st) {
+    const Variant<T> &v = variants<T>()[vi];
+    BoundaryKernel<T> k = boundary_kernel_for<T>(v.vx, v.bx, v.by, e);
+    const int slot = 2 * vi + (e ? 0 : 1);
+    const int first = h->ptile[slot][1], last = h->ptile[slot][kParts];
+    if (!k || last <= first) return 0;
+    const TileMap &th = h->tmaps_host[slot];
+    k<<<dim3(last - first, h->nshot), dim3(v.bx, v.by), 0, st>>>(a, h->tmaps.as<TileMap>() + slot, first, th.pbox[1],
+                                                                   th.pbox[kParts]);
+    return 1;
+}
+
 // One part of a phase (0 interior, 1 faces, 2 edges and corners) with
 // variant vi (vi < 0: TMA interior config -1 - vi); returns 1 if it
 // launched a kernel.
@@ -632,6 +693,16 @@ int ensure_part_streams(mittet_handle *h) {
 template <typename T>
 int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a) {
     int n = 0;
+    const int mb = h->merge_b[e ? 0 : 1];
+    if (mb >= 0 && h->ev_fork) {  // interior + one merged boundary launch
+        cudaEventRecord(h->ev_fork, h->st);
+        cudaStreamWaitEvent(h->pst[1], h->ev_fork, 0);
+        n += launch_boundary<T>(h, e, mb, a, h->pst[1]);
+        n += launch_part<T>(h, e, 0, vi[0], a, h->st);
+        cudaEventRecord(h->ev_join[1], h->pst[1]);
+        cudaStreamWaitEvent(h->st, h->ev_join[1], 0);
+        return n;
+    }
     if (!h->ev_fork || std::getenv("MITTET_SERIAL_PARTS")) {
         for (int part = 0; part < kParts; part++) n += launch_part<T>(h, e, part, vi[part], a);
         return n;
@@ -789,6 +860,18 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
             return MITTET_OK;
         }
     }
+    // The persistent launch only competes where a step holds little work
+    // (launch gaps dominate): measured on a B200 it is 1.5x slower than the
+    // stepped graph for one 64^3 shot and 4-6x slower for 32 of them, so it
+    // is timed only for steps of at most 4 M cells (or when forced), and only
+    // in the two-cell shapes with short z chunks that came closest.
+    const long long step_cells = (long long)h->nshot * h->fshot;
+    if (force != 1 && step_cells > (4LL << 20)) {
+        h->persist_vi = -1;
+        std::lock_guard<std::mutex> lk(g_persist_mu);
+        g_persist_cache[key] = -1;
+        return MITTET_OK;
+    }
     const bool log = std::getenv("MITTET_TUNE_LOG") != nullptr;
     auto capture = [&](int vi, cudaGraphExec_t *out) -> int {
         cudaGraph_t graph;
@@ -835,7 +918,9 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
     }
     const auto &vs = variants<T>();
     for (int vi = 0; vi < (int)vs.size(); vi++) {
-        if (vs[vi].bz > 0 || !persist_kernel_for<T>(vs[vi].vx, vs[vi].bx, vs[vi].by) || vs[vi].zc > 8) continue;
+        if (vs[vi].bz > 0 || !persist_kernel_for<T>(vs[vi].vx, vs[vi].bx, vs[vi].by) || vs[vi].zc > 4 ||
+            vs[vi].vx != 2)
+            continue;
         cudaGraphExec_t g;
         if (capture(vi, &g)) continue;
         CK(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->st));
@@ -873,7 +958,7 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
 // fields, so the state is untouched apart from the ring slot written by the
 // E phase).  Results are cached for the process.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 2>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 4>> g_tune_cache;
 
 template <typename T>
 int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
@@ -895,6 +980,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
         if (v >= 0 && v < nv) {
             for (int p = 0; p < kParts; p++) h->var_e[p] = h->var_h[p] = v;
             h->ldg_int[0] = h->ldg_int[1] = v;
+            h->merge_b[0] = h->merge_b[1] = -1;
             if (only_tma) h->var_e[0] = h->var_h[0] = -1;
             return MITTET_OK;
         }
@@ -911,6 +997,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             }
             h->ldg_int[0] = it->second[2 * kParts];
             h->ldg_int[1] = it->second[2 * kParts + 1];
+            h->merge_b[0] = it->second[2 * kParts + 2];
+            h->merge_b[1] = it->second[2 * kParts + 3];
             return MITTET_OK;
         }
     }
@@ -929,7 +1017,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             const std::string kt = key_text();
             while (fgets(line, sizeof(line), f)) {
                 if (strncmp(line, kt.c_str(), kt.size()) != 0 || line[kt.size()] != ':') continue;
-                std::array<int, 2 * kParts + 2> e;
+                std::array<int, 2 * kParts + 4> e;
                 int n = 0, off = (int)kt.size() + 1, used = 0;
                 while (n < (int)e.size() && sscanf(line + off, "%d%n", &e[n], &used) == 1) {
                     off += used;
@@ -942,6 +1030,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
                 }
                 h->ldg_int[0] = e[2 * kParts];
                 h->ldg_int[1] = e[2 * kParts + 1];
+                h->merge_b[0] = e[2 * kParts + 2];
+                h->merge_b[1] = e[2 * kParts + 3];
                 fclose(f);
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 g_tune_cache[key] = e;
@@ -950,6 +1040,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             fclose(f);
         }
     }
+    h->merge_b[0] = h->merge_b[1] = -1;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -995,16 +1086,85 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             }
         }
     }
+    // Refinement on the whole phase.  The per-part times above are taken with
+    // each part alone on the GPU; in a step the five parts run at once on
+    // side streams and share the SMs, so a part's best shape alone need not
+    // be its best beside the others.  Coordinate descent over the parts,
+    // timing the full phase (fork, five parts, join) for each candidate.
+    if (h->ev_fork && !only_tma && !pinned && !std::getenv("MITTET_PART_TUNE_ONLY")) {
+        for (int ph = 0; ph < 2; ph++) {
+            const PhaseArgs<T> &a = ph == 0 ? ea : ha;
+            int *var = ph == 0 ? h->var_e : h->var_h;
+            auto phase_ms = [&](float *out) -> int {
+                launch_phase<T>(h, ph == 0, var, a);  // warm-up
+                CK(cudaEventRecord(e0, h->st));
+                for (int r = 0; r < reps; r++) launch_phase<T>(h, ph == 0, var, a);
+                CK(cudaEventRecord(e1, h->st));
+                CK(cudaEventSynchronize(e1));
+                CK(cudaGetLastError());
+                CK(cudaEventElapsedTime(out, e0, e1));
+                *out /= reps;
+                return MITTET_OK;
+            };
+            float best = 0;
+            if (int rc = phase_ms(&best)) return rc;
+            for (int pass = 0; pass < 2; pass++) {
+                bool changed = false;
+                for (int part = 0; part < kParts; part++) {
+                    if (h->ptile[2 * 0 + (ph == 0 ? 0 : 1)][part + 1] <= h->ptile[2 * 0 + (ph == 0 ? 0 : 1)][part])
+                        continue;  // the part is empty
+                    const int cur = var[part];
+                    int keep = cur;
+                    const int ntma = (part == 0 && try_tma) ? (int)tma_cfgs<T>().size() : 0;
+                    for (int v = -ntma; v < nv; v++) {
+                        if (v == cur) continue;
+                        var[part] = v;
+                        float ms = 0;
+                        if (int rc = phase_ms(&ms)) return rc;
+                        if (ms < best * 0.99f) {
+                            best = ms;
+                            keep = v;
+                        }
+                    }
+                    var[part] = keep;
+                    changed |= keep != cur;
+                }
+                if (std::getenv("MITTET_TUNE_LOG"))
+                    fprintf(stderr, "autotune %s phase pass %d: %.4f ms\n", ph == 0 ? "E" : "H", pass, best);
+                if (!changed) break;
+            }
+            // the four boundary parts merged into one launch, per shape
+            int &mb = h->merge_b[ph];
+            int keep = -1;
+            for (int v = 0; v < nv; v++) {
+                const Variant<T> &vv = variants<T>()[v];
+                if (vv.bz > 0 || !boundary_kernel_for<T>(vv.vx, vv.bx, vv.by, ph == 0)) continue;
+                mb = v;
+                float ms = 0;
+                if (int rc = phase_ms(&ms)) return rc;
+                if (std::getenv("MITTET_TUNE_LOG"))
+                    fprintf(stderr, "autotune %s merged boundary vx%d %dx%dx%d: %.4f ms\n", ph == 0 ? "E" : "H", vv.vx,
+                            vv.bx, vv.by, vv.zc, ms);
+                if (ms < best * 0.99f) {
+                    best = ms;
+                    keep = v;
+                }
+            }
+            mb = keep;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    std::array<int, 2 * kParts + 2> entry;
+    std::array<int, 2 * kParts + 4> entry;
     for (int p = 0; p < kParts; p++) {
         entry[p] = h->var_e[p];
         entry[kParts + p] = h->var_h[p];
     }
     entry[2 * kParts] = h->ldg_int[0];
     entry[2 * kParts + 1] = h->ldg_int[1];
+    entry[2 * kParts + 2] = h->merge_b[0];
+    entry[2 * kParts + 3] = h->merge_b[1];
     g_tune_cache[key] = entry;
     if (tfile) {
         if (FILE *f = fopen(tfile, "a")) {
@@ -1114,6 +1274,15 @@ int run_forward(mittet_handle *h, int nt) {
         rc = ensure_state(h);  // back to zero fields and psi
         if (rc) return rc;
         h->tuned = true;
+    }
+    // MITTET_BOUNDARY=<v> forces the merged boundary launch with variant v on
+    // both phases (-1: the four part launches), e.g. to check bit-identity
+    if (const char *mbv = std::getenv("MITTET_BOUNDARY")) {
+        const int v = std::atoi(mbv);
+        const auto &vs = variants<T>();
+        const bool ok = v >= 0 && v < (int)vs.size() && vs[v].bz == 0 &&
+                        boundary_kernel_for<T>(vs[v].vx, vs[v].bx, vs[v].by, true) != nullptr;
+        h->merge_b[0] = h->merge_b[1] = ok ? v : -1;
     }
     // One graph holds G = ring_k steps; the volume flush of those steps (when
     // enabled) is launched after each replay.
@@ -1614,6 +1783,10 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         constexpr int AVX = sizeof(T) == 4 ? 4 : 2;
         const char *gmode = std::getenv("MITTET_ADJ_GATHER");
         const bool gather_cell = gmode && std::string(gmode) == "cell";
+        // own kernels per part of the forward's boxes (MITTET_ADJ_OWN=cell:
+        // one kernel over every cell with run-time CPML tests, bit-identical)
+        const char *omode = std::getenv("MITTET_ADJ_OWN");
+        const bool own_cell = omode && std::string(omode) == "cell";
         const dim3 vblk(32, 4), vgrd((h->g.nx + 32 * AVX - 1) / (32 * AVX), (h->g.ny + 3) / 4, h->g.nz * Gg);
         const T *H = hist.as<T>();
         const size_t slot = 6 * gF;
@@ -1677,14 +1850,16 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
                                                           aa.lam[5], h->rec_off.as<long long>(), h->rec_comp.as<int>(),
                                                           nrec, Gg, h->fshot, asrc, nt, n, 1);
                 if (hm) adj_src_kernel<T><<<(int)(asp.size() + 63) / 64, 64, 0, h->st>>>(ah, d_asp.as<AdjSrc>(), (int)asp.size(), h->wave.as<double>(), n, 0, s0, s1);
-                adj_h_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
+                if (own_cell) adj_h_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
+                else launch_adj_own<T>(h, false, ah, Gg);
                 if (gather_cell) adj_h_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ah);
                 else adjv_h_gather_kernel<T, AVX><<<vgrd, vblk, 0, h->st>>>(ah);
                 adj_inject_kernel<T><<<4, 256, 0, h->st>>>(aa.lam[0], aa.lam[1], aa.lam[2], aa.lam[3], aa.lam[4],
                                                           aa.lam[5], h->rec_off.as<long long>(), h->rec_comp.as<int>(),
                                                           nrec, Gg, h->fshot, asrc, nt, n, 0);
                 if (he) adj_src_kernel<T><<<(int)(asp.size() + 63) / 64, 64, 0, h->st>>>(ae, d_asp.as<AdjSrc>(), (int)asp.size(), h->wave.as<double>(), n, 1, s0, s1);
-                adj_e_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
+                if (own_cell) adj_e_own_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
+                else launch_adj_own<T>(h, true, ae, Gg);
                 if (gather_cell) adj_e_gather_kernel<T><<<agrd, ablk, 0, h->st>>>(ae);
                 else adjv_e_gather_kernel<T, AVX><<<vgrd, vblk, 0, h->st>>>(ae);
             }
@@ -2214,6 +2389,13 @@ int mittet_f_to_d(int32_t device, int32_t ntrace, int32_t nt, double dt, double 
 }
 
 int64_t mittet_last_launch_count(mittet_handle *h) { return h ? h->launches : -1; }
+
+int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_variant) {
+    if (!h || !e_variant || !h_variant) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    *e_variant = h->merge_b[0];
+    *h_variant = h->merge_b[1];
+    return MITTET_OK;
+}
 
 int mittet_persistent_variant(mittet_handle *h, int32_t *variant, int32_t *grid) {
     if (!h || !variant || !grid) return fail(MITTET_ERR_INVALID_ARG, "null argument");

@@ -302,6 +302,7 @@ extern "C" int mittet_forward_noalloc(const mittet_grid *g, const mittet_phys *p
             a.pshot[ax] = (long long)(t == 0 ? pe[ax] : ph_[ax]);
             a.slab[ax].nlo = s.nlo; a.slab[ax].nhi = s.nhi; a.slab[ax].flo = s.flo; a.slab[ax].fhi = s.fhi;
             a.slab[ax].width = s.width;
+            a.slab[ax].fofs = s.fofs;
             for (int b = 0; b < 3; b++) {
                 a.slab[ax].other.lo[b] = s.other.lo[b];
                 a.slab[ax].other.hi[b] = s.other.hi[b];

@@ -11,6 +11,7 @@
 //   SATAN_I    e/h_field_cpml42 (fwi3d_cpu_function_v1.4.c:1196-1281),
 //              xe..zh_pml4 (fwi3d_cpu_cpmlabc_v1.4.c:402-679)
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -23,9 +24,15 @@ struct Box {
 
 // A CPML slab group along one axis: a near interval [nlo,nhi) and a far
 // interval [flo,fhi) on that axis, restricted to the `other` box on the two
-// remaining axes.  width = cells of the axis that carry psi.
+// remaining axes.  Its psi are stored with `width` entries along the axis:
+// the near cells at 0.., the far cells at fofs...  Along y and z (psi rows
+// of px cells) the two intervals are packed (fofs = near cells); along x,
+// where a psi row is only the slab cells of one grid row, each interval gets
+// its own 32-byte-aligned half (fofs = width / 2, a multiple of 8 entries),
+// so the near and far sides, computed by different CTAs, never share a DRAM
+// sector.
 struct Slab {
-    int nlo, nhi, flo, fhi, width;
+    int nlo, nhi, flo, fhi, width, fofs;
     Box other;
 };
 
@@ -140,8 +147,8 @@ inline void make_ranges(int flavor, int nx, int ny, int nz, int nc, Setup &s) {
         s.upd[4] = box(1, 0, 1, nx - 2, ny, nz - 2);
         s.upd[5] = box(1, 1, 0, nx - 2, ny - 2, nz);
         for (int a = 0; a < 3; a++) {
-            s.se[a] = Slab{2, nc + 1, n3[a] - nc, n3[a] - 1, 0, box(0, 0, 0, nx, ny, nz)};
-            s.sh[a] = Slab{1, nc, n3[a] - nc - 1, n3[a] - 2, 0, box(0, 0, 0, nx, ny, nz)};
+            s.se[a] = Slab{2, nc + 1, n3[a] - nc, n3[a] - 1, 0, 0, box(0, 0, 0, nx, ny, nz)};
+            s.sh[a] = Slab{1, nc, n3[a] - nc - 1, n3[a] - 2, 0, 0, box(0, 0, 0, nx, ny, nz)};
         }
     } else {
         s.upd[0] = box(1, 2, 2, nx - 1, ny - 1, nz - 1);
@@ -151,19 +158,27 @@ inline void make_ranges(int flavor, int nx, int ny, int nz, int nc, Setup &s) {
         s.upd[4] = box(1, 1, 1, nx - 2, ny - 1, nz - 2);
         s.upd[5] = box(1, 1, 1, nx - 2, ny - 2, nz - 1);
         const Box oth = box(0, 0, 0, nx - 1, ny - 1, nz - 1);
-        s.se[0] = Slab{2, nc - 1, nx - nc + 1, nx - 2, 0, oth};
-        s.se[1] = Slab{2, nc, ny - nc + 1, ny - 2, 0, oth};
-        s.se[2] = Slab{2, nc, nz - nc + 1, nz - 2, 0, oth};
-        s.sh[0] = Slab{1, nc - 1, nx - nc, nx - 2, 0, oth};
-        s.sh[1] = Slab{1, nc - 1, ny - nc, ny - 2, 0, oth};
-        s.sh[2] = Slab{1, nc - 1, nz - nc, nz - 2, 0, oth};
+        s.se[0] = Slab{2, nc - 1, nx - nc + 1, nx - 2, 0, 0, oth};
+        s.se[1] = Slab{2, nc, ny - nc + 1, ny - 2, 0, 0, oth};
+        s.se[2] = Slab{2, nc, nz - nc + 1, nz - 2, 0, 0, oth};
+        s.sh[0] = Slab{1, nc - 1, nx - nc, nx - 2, 0, 0, oth};
+        s.sh[1] = Slab{1, nc - 1, ny - nc, ny - 2, 0, 0, oth};
+        s.sh[2] = Slab{1, nc - 1, nz - nc, nz - 2, 0, 0, oth};
     }
     for (int a = 0; a < 3; a++) {
         Slab *g[2] = {&s.se[a], &s.sh[a]};
         for (Slab *q : g) {
             if (q->nhi < q->nlo) q->nhi = q->nlo;
             if (q->fhi < q->flo) q->fhi = q->flo;
-            q->width = (q->nhi - q->nlo) + (q->fhi - q->flo);
+            const int near = q->nhi - q->nlo, far = q->fhi - q->flo;
+            if (a == 0) {
+                const int half = (std::max(near, far) + 7) / 8 * 8;
+                q->fofs = half;
+                q->width = 2 * half;
+            } else {
+                q->fofs = near;
+                q->width = near + far;
+            }
         }
     }
 }

@@ -783,6 +783,37 @@ __device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int q0, i
 MITTET_PHASE_KERNEL(e)
 MITTET_PHASE_KERNEL(h)
 
+// The four boundary parts of a phase (x, y, z faces and the edges) in one
+// launch: each CTA takes a tile of boxes [pbox[1], nbox) and runs the body of
+// its box's kind.  One launch of ~1.6 k CTAs instead of four of a few hundred
+// each gives the latency-bound boundary bodies more warps in flight beside
+// the interior; it needs the registers of the heaviest body.  Tiles
+// [first_tile, first_tile + gridDim.x).
+template <typename T, int VX, int BX, int BY, bool EPH>
+__global__ void __launch_bounds__(BX *BY, (part_min_blocks<T, VX, BX * BY, 7, 0>()))
+    boundary_kernel(const PhaseArgs<T> a, const TileMap *__restrict__ tm, int first_tile, int q0, int q1) {
+    const int b = first_tile + blockIdx.x;
+    int q = q0;
+    for (int t = q0 + 1; t < q1; t++)
+        if (b >= __ldg(&tm->start[t])) q = t;
+    int i0, j, kb, ke;
+    bool inside;
+    locate<VX, BX, BY>(tm, q, q + 1, b, i0, j, kb, ke, inside);
+    if (!inside) return;
+    const int kind = __ldg(&tm->kind[q]);
+    if constexpr (EPH) {
+        if (kind == 1) e_cells<T, VX, 1, false>(a, blockIdx.y, i0, j, kb, ke);
+        else if (kind == 2) e_cells<T, VX, 2, false>(a, blockIdx.y, i0, j, kb, ke);
+        else if (kind == 4) e_cells<T, VX, 4, false>(a, blockIdx.y, i0, j, kb, ke);
+        else e_cells<T, VX, 7, false>(a, blockIdx.y, i0, j, kb, ke);
+    } else {
+        if (kind == 1) h_cells<T, VX, 1, false>(a, blockIdx.y, i0, j, kb, ke);
+        else if (kind == 2) h_cells<T, VX, 2, false>(a, blockIdx.y, i0, j, kb, ke);
+        else if (kind == 4) h_cells<T, VX, 4, false>(a, blockIdx.y, i0, j, kb, ke);
+        else h_cells<T, VX, 7, false>(a, blockIdx.y, i0, j, kb, ke);
+    }
+}
+
 // Variants the autotuner chooses from: (VX, BX, BY, ZC, BZ) = x cells per
 // thread, thread block in x and y, z planes per tile, threads along z.
 // BZ = 0: each thread marches the tile's ZC planes; ZC is a run-time tile

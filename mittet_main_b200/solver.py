@@ -286,14 +286,20 @@ class MittetSolver:
         return int(self._lib.mittet_last_launch_count(self._h))
 
     def launch_path(self) -> dict:
-        """The time loop of the last forward: {"persistent": False} for the
-        stepped graph of part kernels, else the stencil variant [VX, BX, BY,
-        ZC] of the persistent multi-shot launch and its CTAs."""
+        """The time loop of the last forward: {"persistent": False, ...} for
+        the stepped graph of part kernels (with, per phase, the stencil
+        variant [VX, BX, BY, ZC] of its merged boundary launch, or None for
+        four boundary launches), else the variant of the persistent
+        multi-shot launch and its CTAs."""
         v, g = ctypes.c_int32(), ctypes.c_int32()
         check(self._lib.mittet_persistent_variant(self._h, ctypes.byref(v), ctypes.byref(g)))
-        if v.value < 0:
-            return {"persistent": False}
-        return {"persistent": True, "variant": stencil_variants(self.cp.precision == FP64)[v.value], "ctas": g.value}
+        vs = stencil_variants(self.cp.precision == FP64)
+        if v.value >= 0:
+            return {"persistent": True, "variant": vs[v.value], "ctas": g.value}
+        be, bh = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.mittet_boundary_variant(self._h, ctypes.byref(be), ctypes.byref(bh)))
+        return {"persistent": False, "e_boundary": vs[be.value] if be.value >= 0 else None,
+                "h_boundary": vs[bh.value] if bh.value >= 0 else None}
 
 
 def stencil_variants(fp64: bool = False) -> list:

@@ -293,3 +293,30 @@ def test_gradient_buffers_are_kept_and_released():
         J3, G3 = s.gradient(wl.nt, obs, checkpoint_every=20)
     assert J1 == pytest.approx(J2, rel=1e-13) and J1 == pytest.approx(J3, rel=1e-13)
     assert np.array_equal(G1, G2) and np.array_equal(G1, G3)
+
+
+@pytest.mark.parametrize("prec,flavor,with_mu", [(FP32, FLAVOR_NCVER0027, False), (FP64, FLAVOR_SATAN_I, False),
+                                                 (FP32, FLAVOR_SATAN_I, True)])
+def test_own_kernels_per_part_are_bit_identical(monkeypatch, prec, flavor, with_mu):
+    """The adjoint own kernels split over the forward's boxes (interior, x/y/z
+    faces, edges: the CPML logic of the axes a box is interior along dropped
+    at compile time) and the one kernel over every cell with run-time tests
+    compute the same terms, so the gradients agree bit for bit."""
+    wl = W.small_case(n=(70, 34, 30), ncpml=6, nt=60, precision=prec, flavor=flavor, magnetic=True, seed=5)
+    wl = replace(wl, shots=[wl.shots[0], Shot(points=[(30, 12, 15, "ey", SRC_ELECTRIC, 0.8)])])
+    rng = np.random.default_rng(9)
+    if with_mu:
+        wl = replace(wl, mu=wl.cp.mu0 * (1.0 + 0.2 * rng.random(wl.sigma.shape)))
+    obs = (rng.normal(size=(2, len(wl.receivers), len(wl.omega)))
+           + 1j * rng.normal(size=(2, len(wl.receivers), len(wl.omega)))) * 1e-12
+    res = {}
+    for mode in ("cell", "parts"):
+        if mode == "cell":
+            monkeypatch.setenv("MITTET_ADJ_OWN", "cell")
+        else:
+            monkeypatch.delenv("MITTET_ADJ_OWN", raising=False)
+        with W.make_solver(wl) as s:
+            res[mode] = s.gradient(wl.nt, obs, checkpoint_every=25)
+    assert res["cell"][0] == pytest.approx(res["parts"][0], rel=1e-13)
+    assert np.abs(res["cell"][1]).max() > 0
+    assert np.array_equal(res["cell"][1], res["parts"][1])
