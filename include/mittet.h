@@ -259,7 +259,9 @@ int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
 /* All chosen variants: cfg[40] = [phase E, H][launch interior, x faces,
  * y faces, z faces, edges][VX, BX, BY, ZC].  VX = 0 marks the TMA-staged
  * interior kernel, whose BX x BY is then its tile in cells.  ZC < 0 marks a
- * single-plane body: a BX x BY x (-ZC) thread block, one z plane per thread. */
+ * single-plane body: a BX x BY x (-ZC) thread block, one z plane per thread.
+ * ZC >= 1000 marks a marching body of ZC - 1000 planes whose interior part
+ * prefetches the next plane. */
 int mittet_tuned_variants(mittet_handle *h, int32_t *cfg);
 
 /* The stencil variants the autotuner chooses from for FP32 (fp64 = 0) or

@@ -918,7 +918,7 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
     }
     const auto &vs = variants<T>();
     for (int vi = 0; vi < (int)vs.size(); vi++) {
-        if (vs[vi].bz > 0 || !persist_kernel_for<T>(vs[vi].vx, vs[vi].bx, vs[vi].by) || vs[vi].zc > 4 ||
+        if (vs[vi].bz != 0 || !persist_kernel_for<T>(vs[vi].vx, vs[vi].bx, vs[vi].by) || vs[vi].zc > 4 ||
             vs[vi].vx != 2)
             continue;
         cudaGraphExec_t g;
@@ -1138,7 +1138,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             int keep = -1;
             for (int v = 0; v < nv; v++) {
                 const Variant<T> &vv = variants<T>()[v];
-                if (vv.bz > 0 || !boundary_kernel_for<T>(vv.vx, vv.bx, vv.by, ph == 0)) continue;
+                if (vv.bz != 0 || !boundary_kernel_for<T>(vv.vx, vv.bx, vv.by, ph == 0)) continue;
                 mb = v;
                 float ms = 0;
                 if (int rc = phase_ms(&ms)) return rc;
@@ -2428,7 +2428,7 @@ int mittet_tuned_variants(mittet_handle *h, int32_t *cfg) {
                     c[0] = 0; c[1] = TmaShape<T>::TX; c[2] = TmaShape<T>::TY; c[3] = tma_cfgs<T>()[-1 - vi].zc;
                 } else {
                     const auto &a = variants<T>()[vi];
-                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.bz > 0 ? -a.bz : a.zc;
+                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.bz > 0 ? -a.bz : (a.bz < 0 ? a.zc + 1000 : a.zc);
                 }
             }
     };
@@ -2443,7 +2443,8 @@ int mittet_stencil_variants(int32_t fp64, int32_t *count, int32_t *cfg, int32_t 
         *count = (int32_t)vs.size();
         for (int v = 0; v < (int)vs.size() && v < max; v++) {
             int32_t *c = cfg + 4 * v;
-            c[0] = vs[v].vx; c[1] = vs[v].bx; c[2] = vs[v].by; c[3] = vs[v].bz > 0 ? -vs[v].bz : vs[v].zc;
+            c[0] = vs[v].vx; c[1] = vs[v].bx; c[2] = vs[v].by;
+            c[3] = vs[v].bz > 0 ? -vs[v].bz : (vs[v].bz < 0 ? vs[v].zc + 1000 : vs[v].zc);
         }
     };
     if (fp64) fill(variants<double>());

@@ -180,6 +180,7 @@ template <typename T, int VX, int NT, int GM, int BZ>
 constexpr int part_min_blocks() {
     const bool narrow = sizeof(T) == 4 && VX == 2;
     if (BZ > 0) return GM == 0 ? (narrow ? 1024 : 768) / NT : (narrow ? 768 : 512) / NT;
+    if (BZ < 0 && GM == 0) return 512 / NT;  // the prefetching interior holds two planes
     return GM == 0 ? (narrow ? 768 : 512) / NT : (narrow ? 512 : 384) / NT;
 }
 
@@ -739,6 +740,208 @@ __device__ __forceinline__ void h_cells(const PhaseArgs<T> &a, int shot, int i0,
     }
 }
 
+// ------------------------------------------- interior with plane prefetch
+// The interior body (GM = 0) with a software pipeline along z: every load
+// of plane k + 1 (the x and y neighbours, the own cells, the model word and
+// the window's next plane) is issued before plane k is computed, so each
+// warp keeps two planes of loads in flight instead of one.  Two planes of
+// operands in registers restrict it to two-cell FP32 threads.  Same fma
+// forms as e_cells / h_cells: bit-identical.
+template <typename T, int VX>
+struct EPlane {
+    T hz[VX], hzl[VX], hzr[VX], hyl[VX], hyr[VX];
+    T hzm2[VX], hzm1[VX], hzp1[VX], hxm2[VX], hxm1[VX], hxp1[VX];
+    T m[VX], ex[VX], ey[VX], ez[VX], nx[VX], ny[VX];  // nx, ny: Hx, Hy of plane k + 1
+};
+
+template <typename T, int VX>
+__device__ __forceinline__ void e_plane_load(EPlane<T, VX> &p, const T *__restrict__ Hx, const T *__restrict__ Hy,
+                                             const T *__restrict__ Hz, const T *__restrict__ M,
+                                             const T *__restrict__ Ex, const T *__restrict__ Ey,
+                                             const T *__restrict__ Ez, int c, int py, int pz) {
+    ldv<T, VX>(p.hz, Hz + c);
+    ldv<T, VX>(p.hzl, Hz + c - VX);
+    ldv<T, VX>(p.hzr, Hz + c + VX);
+    ldv<T, VX>(p.hyl, Hy + c - VX);
+    ldv<T, VX>(p.hyr, Hy + c + VX);
+    ldv<T, VX>(p.hzm2, Hz + c - 2 * py);
+    ldv<T, VX>(p.hzm1, Hz + c - py);
+    ldv<T, VX>(p.hzp1, Hz + c + py);
+    ldv<T, VX>(p.hxm2, Hx + c - 2 * py);
+    ldv<T, VX>(p.hxm1, Hx + c - py);
+    ldv<T, VX>(p.hxp1, Hx + c + py);
+    ldv<T, VX>(p.m, M + c);
+    ldv<T, VX>(p.ex, Ex + c);
+    ldv<T, VX>(p.ey, Ey + c);
+    ldv<T, VX>(p.ez, Ez + c);
+    ldv<T, VX>(p.nx, Hx + c + pz);
+    ldv<T, VX>(p.ny, Hy + c + pz);
+}
+
+template <typename T, int VX>
+__device__ __forceinline__ void e_interior_pf(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
+    const long long sb = (long long)shot * a.fshot;
+    const T *__restrict__ Ex = a.f[0] + sb;
+    const T *__restrict__ Ey = a.f[1] + sb;
+    const T *__restrict__ Ez = a.f[2] + sb;
+    T *__restrict__ Exo = a.fo[0] + sb;
+    T *__restrict__ Eyo = a.fo[1] + sb;
+    T *__restrict__ Ezo = a.fo[2] + sb;
+    const T *__restrict__ Hx = a.f[3] + sb;
+    const T *__restrict__ Hy = a.f[4] + sb;
+    const T *__restrict__ Hz = a.f[5] + sb;
+    const int py = a.px, pz = (int)a.plane;
+    const T c1 = a.c1, c2 = a.c2, sg = a.sgn, ikx = a.ik[0], iky = a.ik[1], ikz = a.ik[2];
+    const int col = j * py + i0;
+    T wx[4][VX], wy[4][VX];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        ldv<T, VX>(wx[q], Hx + (kb - 2 + q) * pz + col);
+        ldv<T, VX>(wy[q], Hy + (kb - 2 + q) * pz + col);
+    }
+    const int slot = a.ring_k > 0 ? (*a.d_step) % a.ring_k : 0;
+    EPlane<T, VX> cur, nxt;
+    e_plane_load<T, VX>(cur, Hx, Hy, Hz, a.m, Ex, Ey, Ez, kb * pz + col, py, pz);
+    for (int k = kb; k < ke; k++) {
+        if (k + 1 < ke) e_plane_load<T, VX>(nxt, Hx, Hy, Hz, a.m, Ex, Ey, Ez, (k + 1) * pz + col, py, pz);
+        const int c = k * pz + col;
+#pragma unroll
+        for (int v = 0; v < VX; v++) { wx[3][v] = cur.nx[v]; wy[3][v] = cur.ny[v]; }
+        T hzx[3 * VX], hyx[3 * VX];
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            hzx[v] = cur.hzl[v]; hzx[VX + v] = cur.hz[v]; hzx[2 * VX + v] = cur.hzr[v];
+            hyx[v] = cur.hyl[v]; hyx[VX + v] = wy[2][v]; hyx[2 * VX + v] = cur.hyr[v];
+        }
+        T ex[VX], ey[VX], ez[VX];
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            const T dyHz = d4(c1, c2, hzx[VX + v], cur.hzm1[v], cur.hzp1[v], cur.hzm2[v]);
+            const T dyHx = d4(c1, c2, wx[2][v], cur.hxm1[v], cur.hxp1[v], cur.hxm2[v]);
+            const T dxHz = d4(c1, c2, hzx[VX + v], hzx[VX + v - 1], hzx[VX + v + 1], hzx[VX + v - 2]);
+            const T dxHy = d4(c1, c2, hyx[VX + v], hyx[VX + v - 1], hyx[VX + v + 1], hyx[VX + v - 2]);
+            const T dzHy = d4(c1, c2, wy[2][v], wy[1][v], wy[3][v], wy[0][v]);
+            const T dzHx = d4(c1, c2, wx[2][v], wx[1][v], wx[3][v], wx[0][v]);
+            const T mv = cur.m[v];
+            ex[v] = leap(T(1), sg * mv, curl2(dyHz, iky, dzHy, ikz), cur.ex[v]);
+            ey[v] = leap(T(1), sg * mv, curl2(dzHx, ikz, dxHz, ikx), cur.ey[v]);
+            ez[v] = leap(T(1), sg * mv, curl2(dxHy, ikx, dyHx, iky), cur.ez[v]);
+        }
+        stv<T, VX>(Exo + c, ex);
+        stv<T, VX>(Eyo + c, ey);
+        stv<T, VX>(Ezo + c, ez);
+        if (a.ring_k > 0) {
+            const long long e = sb + c;
+            if (a.vmask & 1) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 0, e, slot), ex);
+            if (a.vmask & 2) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 1, e, slot), ey);
+            if (a.vmask & 4) stv_stream<T, VX>(a.ring + ring_index(a.ring_comp, a.ring_k, 2, e, slot), ez);
+        }
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            wx[0][v] = wx[1][v]; wx[1][v] = wx[2][v]; wx[2][v] = wx[3][v];
+            wy[0][v] = wy[1][v]; wy[1][v] = wy[2][v]; wy[2][v] = wy[3][v];
+        }
+        cur = nxt;
+    }
+}
+
+template <typename T, int VX>
+struct HPlane {
+    T ez[VX], ezl[VX], ezr[VX], eyl[VX], eyr[VX];
+    T ezm1[VX], ezp1[VX], ezp2[VX], exm1[VX], exp1[VX], exp2[VX];
+    T dm[VX], hx[VX], hy[VX], hz[VX], nx[VX], ny[VX];  // nx, ny: Ex, Ey of plane k + 2
+};
+
+template <typename T, int VX>
+__device__ __forceinline__ void h_plane_load(HPlane<T, VX> &p, const T *__restrict__ Ex, const T *__restrict__ Ey,
+                                             const T *__restrict__ Ez, const T *__restrict__ DM, T dtmu0,
+                                             const T *__restrict__ Hx, const T *__restrict__ Hy,
+                                             const T *__restrict__ Hz, int c, int py, int pz) {
+    ldv<T, VX>(p.ez, Ez + c);
+    ldv<T, VX>(p.ezl, Ez + c - VX);
+    ldv<T, VX>(p.ezr, Ez + c + VX);
+    ldv<T, VX>(p.eyl, Ey + c - VX);
+    ldv<T, VX>(p.eyr, Ey + c + VX);
+    ldv<T, VX>(p.ezm1, Ez + c - py);
+    ldv<T, VX>(p.ezp1, Ez + c + py);
+    ldv<T, VX>(p.ezp2, Ez + c + 2 * py);
+    ldv<T, VX>(p.exm1, Ex + c - py);
+    ldv<T, VX>(p.exp1, Ex + c + py);
+    ldv<T, VX>(p.exp2, Ex + c + 2 * py);
+    if (DM) {
+        ldv<T, VX>(p.dm, DM + c);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VX; v++) p.dm[v] = dtmu0;
+    }
+    ldv<T, VX>(p.hx, Hx + c);
+    ldv<T, VX>(p.hy, Hy + c);
+    ldv<T, VX>(p.hz, Hz + c);
+    ldv<T, VX>(p.nx, Ex + c + 2 * pz);
+    ldv<T, VX>(p.ny, Ey + c + 2 * pz);
+}
+
+template <typename T, int VX>
+__device__ __forceinline__ void h_interior_pf(const PhaseArgs<T> &a, int shot, int i0, int j, int kb, int ke) {
+    const long long sb = (long long)shot * a.fshot;
+    const T *__restrict__ Ex = a.f[0] + sb;
+    const T *__restrict__ Ey = a.f[1] + sb;
+    const T *__restrict__ Ez = a.f[2] + sb;
+    const T *__restrict__ Hx = a.f[3] + sb;
+    const T *__restrict__ Hy = a.f[4] + sb;
+    const T *__restrict__ Hz = a.f[5] + sb;
+    T *__restrict__ Hxo = a.fo[3] + sb;
+    T *__restrict__ Hyo = a.fo[4] + sb;
+    T *__restrict__ Hzo = a.fo[5] + sb;
+    const int py = a.px, pz = (int)a.plane;
+    const T c1 = a.c1, c2 = a.c2, sg = a.sgn, ikx = a.ik[0], iky = a.ik[1], ikz = a.ik[2];
+    const int col = j * py + i0;
+    T wx[4][VX], wy[4][VX];  // planes k-1 .. k+2 of Ex and Ey
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        ldv<T, VX>(wx[q], Ex + (kb - 1 + q) * pz + col);
+        ldv<T, VX>(wy[q], Ey + (kb - 1 + q) * pz + col);
+    }
+    HPlane<T, VX> cur, nxt;
+    h_plane_load<T, VX>(cur, Ex, Ey, Ez, a.dtmu, a.dtmu0, Hx, Hy, Hz, kb * pz + col, py, pz);
+    for (int k = kb; k < ke; k++) {
+        if (k + 1 < ke) h_plane_load<T, VX>(nxt, Ex, Ey, Ez, a.dtmu, a.dtmu0, Hx, Hy, Hz, (k + 1) * pz + col, py, pz);
+        const int c = k * pz + col;
+#pragma unroll
+        for (int v = 0; v < VX; v++) { wx[3][v] = cur.nx[v]; wy[3][v] = cur.ny[v]; }
+        T ezx[3 * VX], eyx[3 * VX];
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            ezx[v] = cur.ezl[v]; ezx[VX + v] = cur.ez[v]; ezx[2 * VX + v] = cur.ezr[v];
+            eyx[v] = cur.eyl[v]; eyx[VX + v] = wy[1][v]; eyx[2 * VX + v] = cur.eyr[v];
+        }
+        T hx[VX], hy[VX], hz[VX];
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            const T ez = ezx[VX + v];
+            const T dyEz = d4(c1, c2, cur.ezp1[v], ez, cur.ezp2[v], cur.ezm1[v]);
+            const T dyEx = d4(c1, c2, cur.exp1[v], wx[1][v], cur.exp2[v], cur.exm1[v]);
+            const T dxEz = d4(c1, c2, ezx[VX + v + 1], ez, ezx[VX + v + 2], ezx[VX + v - 1]);
+            const T dxEy = d4(c1, c2, eyx[VX + v + 1], eyx[VX + v], eyx[VX + v + 2], eyx[VX + v - 1]);
+            const T dzEy = d4(c1, c2, wy[2][v], wy[1][v], wy[3][v], wy[0][v]);
+            const T dzEx = d4(c1, c2, wx[2][v], wx[1][v], wx[3][v], wx[0][v]);
+            const T dmv = cur.dm[v];
+            hx[v] = leap(T(1), -sg * dmv, curl2(dyEz, iky, dzEy, ikz), cur.hx[v]);
+            hy[v] = leap(T(1), -sg * dmv, curl2(dzEx, ikz, dxEz, ikx), cur.hy[v]);
+            hz[v] = leap(T(1), -sg * dmv, curl2(dxEy, ikx, dyEx, iky), cur.hz[v]);
+        }
+        stv<T, VX>(Hxo + c, hx);
+        stv<T, VX>(Hyo + c, hy);
+        stv<T, VX>(Hzo + c, hz);
+#pragma unroll
+        for (int v = 0; v < VX; v++) {
+            wx[0][v] = wx[1][v]; wx[1][v] = wx[2][v]; wx[2][v] = wx[3][v];
+            wy[0][v] = wy[1][v]; wy[1][v] = wy[2][v]; wy[2][v] = wy[3][v];
+        }
+        cur = nxt;
+    }
+}
+
 // Locate this CTA's box and tile (tile index b, boxes [q0, q1)): the
 // thread's first x cell i0, its row j and its z planes [kb, ke).
 template <int VX, int BX, int BY>
@@ -776,7 +979,12 @@ __device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int q0, i
             kb += (int)threadIdx.z;                                                                          \
             inside = inside && kb < ke;                                                                      \
         }                                                                                                    \
-        if (inside) PH##_cells<T, VX, GM, (BZ > 0)>(a, blockIdx.y, i0, j, kb, ke);                           \
+        if (inside) {                                                                                        \
+            if constexpr (BZ < 0 && GM == 0)                                                                 \
+                PH##_interior_pf<T, VX>(a, blockIdx.y, i0, j, kb, ke);                                       \
+            else                                                                                             \
+                PH##_cells<T, VX, GM, (BZ > 0)>(a, blockIdx.y, i0, j, kb, ke);                               \
+        }                                                                                                    \
     }
 
 // e_part_kernel and h_part_kernel.
@@ -820,8 +1028,10 @@ __global__ void __launch_bounds__(BX *BY, (part_min_blocks<T, VX, BX * BY, 7, 0>
 // parameter (the same kernel serves every ZC): short chunks give small boxes
 // enough CTAs, long ones amortise the window preload.  BZ > 0 (ZC = BZ): one
 // plane per thread (on 256^2 x 192 they lose to the marching bodies on every
-// part, by 5-20%; they stay candidates for small boxes).  The narrow blocks
-// (x tile of 8 or 16 cells) suit the thin x faces.
+// part, by 5-20%; they stay candidates for small boxes).  BZ = -1: marching,
+// with the interior part prefetching plane k + 1 (e_interior_pf; the other
+// parts march as BZ = 0).  The narrow blocks (x tile of 8 or 16 cells) suit
+// the thin x faces.
 #define MITTET_STENCIL_VARIANTS_F32(X) \
     X(2, 32, 4, 2, 0)                     \
     X(2, 32, 4, 4, 0)                     \
@@ -840,7 +1050,10 @@ __global__ void __launch_bounds__(BX *BY, (part_min_blocks<T, VX, BX * BY, 7, 0>
     X(2, 4, 32, 4, 0)                     \
     X(4, 16, 8, 2, 2)                     \
     X(2, 16, 4, 4, 4)                     \
-    X(2, 8, 8, 4, 4)
+    X(2, 8, 8, 4, 4)                      \
+    X(2, 32, 4, 8, -1)                    \
+    X(2, 16, 8, 8, -1)                    \
+    X(2, 32, 4, 16, -1)
 #define MITTET_STENCIL_VARIANTS_F64(X) \
     X(2, 32, 4, 2, 0)                     \
     X(2, 32, 4, 4, 0)                     \
