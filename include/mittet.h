@@ -260,8 +260,9 @@ int mittet_tuned_variant(mittet_handle *h, int32_t *e_cfg, int32_t *h_cfg);
  * y faces, z faces, edges][VX, BX, BY, ZC].  VX = 0 marks the TMA-staged
  * interior kernel, whose BX x BY is then its tile in cells.  ZC < 0 marks a
  * single-plane body: a BX x BY x (-ZC) thread block, one z plane per thread.
- * ZC >= 1000 marks a marching body of ZC - 1000 planes whose interior part
- * prefetches the next plane. */
+ * ZC = 1000 + z marks a marching body of z planes whose interior part
+ * prefetches the next plane, ZC = 2000 + z one whose interior body is held
+ * to 85 registers (more resident warps). */
 int mittet_tuned_variants(mittet_handle *h, int32_t *cfg);
 
 /* The stencil variants the autotuner chooses from for FP32 (fp64 = 0) or

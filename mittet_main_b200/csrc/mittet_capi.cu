@@ -374,8 +374,13 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
     // cells of x that way use multiples of 4 (every vector width divides
     // them).  Partial tiles in x and y are masked and the last z chunk of a
     // box is cut at the box edge.
+    // MITTET_X_ALIGN_MIN: the narrowest line-aligned interior kept (default 64 cells)
+    static const int align_min = [] {
+        const char *v = std::getenv("MITTET_X_ALIGN_MIN");
+        return v ? std::max(1, std::atoi(v)) : 64;
+    }();
     int X0 = (lo[0] + 31) / 32 * 32, X1 = hi[0] / 32 * 32;
-    if (X1 - X0 < 64) {
+    if (X1 - X0 < align_min) {
         X0 = (lo[0] + 3) / 4 * 4;
         X1 = hi[0] / 4 * 4;
     }
@@ -2428,7 +2433,7 @@ int mittet_tuned_variants(mittet_handle *h, int32_t *cfg) {
                     c[0] = 0; c[1] = TmaShape<T>::TX; c[2] = TmaShape<T>::TY; c[3] = tma_cfgs<T>()[-1 - vi].zc;
                 } else {
                     const auto &a = variants<T>()[vi];
-                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.bz > 0 ? -a.bz : (a.bz < 0 ? a.zc + 1000 : a.zc);
+                    c[0] = a.vx; c[1] = a.bx; c[2] = a.by; c[3] = a.bz > 0 ? -a.bz : (a.bz < 0 ? a.zc - 1000 * a.bz : a.zc);
                 }
             }
     };
@@ -2444,7 +2449,7 @@ int mittet_stencil_variants(int32_t fp64, int32_t *count, int32_t *cfg, int32_t 
         for (int v = 0; v < (int)vs.size() && v < max; v++) {
             int32_t *c = cfg + 4 * v;
             c[0] = vs[v].vx; c[1] = vs[v].bx; c[2] = vs[v].by;
-            c[3] = vs[v].bz > 0 ? -vs[v].bz : (vs[v].bz < 0 ? vs[v].zc + 1000 : vs[v].zc);
+            c[3] = vs[v].bz > 0 ? -vs[v].bz : (vs[v].bz < 0 ? vs[v].zc - 1000 * vs[v].bz : vs[v].zc);
         }
     };
     if (fp64) fill(variants<double>());

@@ -180,7 +180,8 @@ template <typename T, int VX, int NT, int GM, int BZ>
 constexpr int part_min_blocks() {
     const bool narrow = sizeof(T) == 4 && VX == 2;
     if (BZ > 0) return GM == 0 ? (narrow ? 1024 : 768) / NT : (narrow ? 768 : 512) / NT;
-    if (BZ < 0 && GM == 0) return 512 / NT;  // the prefetching interior holds two planes
+    if (BZ == -1 && GM == 0) return 512 / NT;  // the prefetching interior holds two planes
+    if (BZ == -2 && GM == 0) return 768 / NT;  // the interior held to 85 registers: 6 x 128 threads per SM
     return GM == 0 ? (narrow ? 768 : 512) / NT : (narrow ? 512 : 384) / NT;
 }
 
@@ -980,7 +981,7 @@ __device__ __forceinline__ void locate(const TileMap *__restrict__ tm, int q0, i
             inside = inside && kb < ke;                                                                      \
         }                                                                                                    \
         if (inside) {                                                                                        \
-            if constexpr (BZ < 0 && GM == 0)                                                                 \
+            if constexpr (BZ == -1 && GM == 0)                                                               \
                 PH##_interior_pf<T, VX>(a, blockIdx.y, i0, j, kb, ke);                                       \
             else                                                                                             \
                 PH##_cells<T, VX, GM, (BZ > 0)>(a, blockIdx.y, i0, j, kb, ke);                               \
@@ -1030,8 +1031,9 @@ __global__ void __launch_bounds__(BX *BY, (part_min_blocks<T, VX, BX * BY, 7, 0>
 // plane per thread (on 256^2 x 192 they lose to the marching bodies on every
 // part, by 5-20%; they stay candidates for small boxes).  BZ = -1: marching,
 // with the interior part prefetching plane k + 1 (e_interior_pf; the other
-// parts march as BZ = 0).  The narrow blocks (x tile of 8 or 16 cells) suit
-// the thin x faces.
+// parts march as BZ = 0).  BZ = -2: marching, with the interior body held to
+// 6 resident CTAs per SM (85 registers) for more warps in flight.  The
+// narrow blocks (x tile of 8 or 16 cells) suit the thin x faces.
 #define MITTET_STENCIL_VARIANTS_F32(X) \
     X(2, 32, 4, 2, 0)                     \
     X(2, 32, 4, 4, 0)                     \
@@ -1053,7 +1055,10 @@ __global__ void __launch_bounds__(BX *BY, (part_min_blocks<T, VX, BX * BY, 7, 0>
     X(2, 8, 8, 4, 4)                      \
     X(2, 32, 4, 8, -1)                    \
     X(2, 16, 8, 8, -1)                    \
-    X(2, 32, 4, 16, -1)
+    X(2, 32, 4, 16, -1)                   \
+    X(4, 16, 8, 8, -2)                    \
+    X(4, 16, 4, 8, -2)                    \
+    X(4, 16, 8, 4, -2)
 #define MITTET_STENCIL_VARIANTS_F64(X) \
     X(2, 32, 4, 2, 0)                     \
     X(2, 32, 4, 4, 0)                     \

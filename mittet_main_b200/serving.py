@@ -137,11 +137,19 @@ class MittetServer:
         self.evictions = 0
         self.reuses = 0
 
+    def need(self, req) -> float:
+        """Bytes a request is admitted for.  A gradient processes its shots in
+        groups sized to the free device memory (mittet_gradient), so one whose
+        estimate for all shots at once exceeds the budget is admitted for the
+        whole budget: it then runs with nothing else admitted beside it."""
+        b = float(self.estimator(req))
+        return min(b, self.budget) if getattr(req, "mode", "forward") == "gradient" else b
+
     def run(self, requests: list, realtime: bool = True) -> list:
         """Serve ``requests`` (sorted by arrival); returns one Result per request."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         for r in reqs:
-            if self.estimator(r) > self.budget:
+            if self.need(r) > self.budget:
                 raise ValueError(f"request {r.rid} needs more than the whole HBM budget")
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
@@ -200,7 +208,7 @@ class MittetServer:
                     for r in list(waiting):
                         if not free_slots:
                             break
-                        need = float(self.estimator(r))
+                        need = self.need(r)
                         key = self.keyer(r)
                         # a free slot that already holds this grid's handle first
                         slot = next((s for s in free_slots if (s, key) in resident), free_slots[0])

@@ -273,8 +273,9 @@ class MittetSolver:
 
     def tuned_variant(self) -> dict:
         """[VX, BX, BY, ZC] the autotuner chose per phase and launch (VX = 0:
-        the TMA-staged interior; ZC >= 1000: ZC - 1000 marching planes with a
-        prefetching interior; ZC < 0: a single-plane body with -ZC threads
+        the TMA-staged interior; ZC = 1000 + z: z marching planes with a
+        prefetching interior, 2000 + z: with the interior held to 85
+        registers; ZC < 0: a single-plane body with -ZC threads
         along z)."""
         parts = ("interior", "xfaces", "yfaces", "zfaces", "edges")
         c = (ctypes.c_int32 * (2 * len(parts) * 4))()
@@ -305,8 +306,8 @@ class MittetSolver:
 
 def stencil_variants(fp64: bool = False) -> list:
     """The stencil variants the autotuner chooses from, as [VX, BX, BY, ZC]
-    (ZC < 0: single-plane body; ZC >= 1000: prefetching interior); index v
-    is what MITTET_VARIANT=v forces."""
+    (ZC < 0: single-plane body; ZC >= 1000: marching variants of the
+    interior, see tuned_variant); index v is what MITTET_VARIANT=v forces."""
     lib = capi.load()
     n = ctypes.c_int32()
     check(lib.mittet_stencil_variants(1 if fp64 else 0, ctypes.byref(n), None, 0))

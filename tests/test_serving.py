@@ -113,3 +113,28 @@ def test_slots_keep_handles_per_grid_within_the_budget():
     assert srv.reuses > 0
     # fewer handles than requests were created: slots reused them
     assert len(made) < len(reqs)
+
+
+def test_gradient_larger_than_the_budget_runs_alone():
+    """A gradient whose all-shots estimate exceeds the budget is admitted for
+    the whole budget (its shots then run in groups that fit), alone."""
+    running = {"n": 0, "max_with_big": 0}
+    lock = threading.Lock()
+
+    def execu(cache, req):
+        with lock:
+            running["n"] += 1
+            if req.mode == "gradient":
+                running["max_with_big"] = max(running["max_with_big"], running["n"])
+        time.sleep(0.02)
+        with lock:
+            running["n"] -= 1
+        return req.rid
+
+    reqs = [make(i, 0.001 * i, 20) for i in range(6)]
+    reqs[2].mode = "gradient"
+    reqs[2].size = 500
+    srv = MittetServer(n_slots=4, hbm_budget=100, executor=execu, estimator=lambda r: r.size)
+    res = srv.run(reqs)
+    assert sorted(r.output for r in res) == list(range(6))
+    assert running["max_with_big"] == 1 and srv.peak_in_use <= 100
