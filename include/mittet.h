@@ -287,6 +287,13 @@ int mittet_persistent_variant(mittet_handle *h, int32_t *variant, int32_t *grid)
  * reference (a tuning introspection). */
 int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_variant);
 
+/* Whether each phase launches its interior and its two x faces as one band
+ * launch (tiles ordered by rows, so the CTAs in flight read whole rows): the
+ * z planes per band for the E and H phase, 0 for separate launches.  Chosen
+ * by the autotuner on the whole phase.  No counterpart in the reference (a
+ * tuning introspection). */
+int mittet_band_variant(mittet_handle *h, int32_t *e_zc, int32_t *h_zc);
+
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);
 

@@ -130,8 +130,9 @@ def serving(args):
     with dx = 6400 m / nx, 1-32 shots, Nt = 6000 nx / 256 (args.nt scales it:
     Nt x args.nt / 6000), forward:gradient = 3:1, 150 GB budget.  Three
     arms, each served in real time from the same arrival process on the same
-    GPU: the server (4 slots, continuous batching), one request at a time
-    (one slot, its shots batched) and one shot at a time (one slot, each shot
+    GPU: the server (4 slots, continuous batching, smallest estimated work
+    first with ageing), one request at a time (one slot, arrival order, its
+    shots batched) and one shot at a time (one slot, arrival order, each shot
     solved alone)."""
     from mittet_main_b200 import workloads as W
     from mittet_main_b200.serving import MittetServer, percentile, poisson_requests, run_request
@@ -165,10 +166,10 @@ def serving(args):
     out = {"report": "serving", "requests": n, "rate_per_s": args.rate, "nt_scale": scale, "shots": shots,
            "grids": sorted({f"{r.workload.cp.nx}x{r.workload.cp.ny}x{r.workload.cp.nz}" for r in reqs}),
            "modes": {m: sum(r.mode == m for r in reqs) for m in ("forward", "gradient")}}
-    arms = [("server", 4, run_request), ("one_request_at_a_time", 1, run_request),
-            ("one_shot_at_a_time", 1, one_shot_at_a_time)]
-    for name, slots, ex in arms:
-        srv = MittetServer(n_slots=slots, hbm_budget=150e9, executor=ex)
+    arms = [("server", 4, run_request, "sjf"), ("one_request_at_a_time", 1, run_request, "fcfs"),
+            ("one_shot_at_a_time", 1, one_shot_at_a_time, "fcfs")]
+    for name, slots, ex, policy in arms:
+        srv = MittetServer(n_slots=slots, hbm_budget=150e9, executor=ex, policy=policy)
         _sync()
         t0 = time.perf_counter()
         res = srv.run(reqs)
@@ -176,7 +177,7 @@ def serving(args):
         wall = time.perf_counter() - t0
         lat = [r.latency for r in res]
         errors = [r.error for r in res if r.error]
-        out[name] = {"p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
+        out[name] = {"policy": policy, "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
                      "shot_solves_per_s": shots / wall, "max_concurrent": srv.max_concurrent,
                      "peak_budget_bytes": srv.peak_in_use, "handle_reuses": srv.reuses,
                      "evictions": srv.evictions, "errors": errors[:3]}

@@ -148,6 +148,7 @@ struct mittet_handle_s {
     bool has_ibox[2] = {false, false};
     int ldg_int[2] = {0, 0};   // best plain-load interior variant of each phase
     int merge_b[2] = {-1, -1}; // variant of the merged boundary launch of each phase (-1: four part launches)
+    int band[2] = {0, 0};      // z planes per band of the interior + x-face band launch (0: part launches)
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
     std::vector<TileMap> tmaps_host;
     DevBuf adj_tmaps;          // one-cell tile maps (32 x 8 x 1) of the E and H phase: the adjoint own kernels
@@ -657,6 +658,40 @@ int launch_boundary(mittet_handle *h, bool e, int vi, const PhaseArgs<T> &a, cud
     return 1;
 }
 
+// The interior and x faces of a phase as one band launch (stencil.cuh
+// band_kernel): 128-thread CTAs, interior tiles of 64 (FP32) or 32 (FP64)
+// cells, x-face tiles of 32 cells, zc planes per band.
+template <typename T>
+struct BandShape {
+    static constexpr int VXI = sizeof(T) == 4 ? 4 : 2, VXF = 2, BX = 16, BY = 8;
+};
+
+template <typename T>
+int launch_band(mittet_handle *h, bool e, int zc, const PhaseArgs<T> &a, cudaStream_t st) {
+    using S = BandShape<T>;
+    const int p = e ? 0 : 1;
+    if (!h->has_ibox[p] || zc <= 0) return 0;
+    const int *ib = h->ibox[p];
+    BandMap bm;
+    bm.x0 = ib[0]; bm.y0 = ib[1]; bm.z0 = ib[2];
+    bm.x1 = ib[3]; bm.y1 = ib[4]; bm.z1 = ib[5];
+    bm.nx = h->g.nx;
+    bm.zc = zc;
+    const int wf = S::BX * S::VXF, wi = S::BX * S::VXI;
+    bm.ntl = (bm.x0 + wf - 1) / wf;
+    bm.nti = (bm.x1 - bm.x0 + wi - 1) / wi;
+    bm.ntr = (bm.nx - bm.x1 + wf - 1) / wf;
+    bm.nty = (bm.y1 - bm.y0 + S::BY - 1) / S::BY;
+    const int nzc = (bm.z1 - bm.z0 + zc - 1) / zc;
+    const dim3 grid((bm.ntl + bm.nti + bm.ntr) * bm.nty * nzc, h->nshot), block(S::BX, S::BY);
+    if (e)
+        band_kernel<T, S::VXI, S::VXF, S::BX, S::BY, true><<<grid, block, 0, st>>>(a, bm);
+    else
+        band_kernel<T, S::VXI, S::VXF, S::BX, S::BY, false><<<grid, block, 0, st>>>(a, bm);
+    return 1;
+}
+constexpr int kBandZc[3] = {4, 8, 16};  // band depths the autotuner tries
+
 // One part of a phase (0 interior, 1 faces, 2 edges and corners) with
 // variant vi (vi < 0: TMA interior config -1 - vi); returns 1 if it
 // launched a kernel.
@@ -706,6 +741,20 @@ int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a)
         n += launch_part<T>(h, e, 0, vi[0], a, h->st);
         cudaEventRecord(h->ev_join[1], h->pst[1]);
         cudaStreamWaitEvent(h->st, h->ev_join[1], 0);
+        return n;
+    }
+    const int bz = h->band[e ? 0 : 1];
+    if (bz > 0 && h->ev_fork && h->has_ibox[e ? 0 : 1]) {  // one band launch + y faces, z faces, edges
+        cudaEventRecord(h->ev_fork, h->st);
+        for (int p = 2; p < kParts; p++) {
+            cudaStreamWaitEvent(h->pst[p], h->ev_fork, 0);
+            n += launch_part<T>(h, e, p, vi[p], a, h->pst[p]);
+        }
+        n += launch_band<T>(h, e, bz, a, h->st);
+        for (int p = 2; p < kParts; p++) {
+            cudaEventRecord(h->ev_join[p], h->pst[p]);
+            cudaStreamWaitEvent(h->st, h->ev_join[p], 0);
+        }
         return n;
     }
     if (!h->ev_fork || std::getenv("MITTET_SERIAL_PARTS")) {
@@ -963,7 +1012,7 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
 // fields, so the state is untouched apart from the ring slot written by the
 // E phase).  Results are cached for the process.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 4>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 6>> g_tune_cache;
 
 template <typename T>
 int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
@@ -986,6 +1035,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             for (int p = 0; p < kParts; p++) h->var_e[p] = h->var_h[p] = v;
             h->ldg_int[0] = h->ldg_int[1] = v;
             h->merge_b[0] = h->merge_b[1] = -1;
+            h->band[0] = h->band[1] = 0;
             if (only_tma) h->var_e[0] = h->var_h[0] = -1;
             return MITTET_OK;
         }
@@ -1004,6 +1054,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             h->ldg_int[1] = it->second[2 * kParts + 1];
             h->merge_b[0] = it->second[2 * kParts + 2];
             h->merge_b[1] = it->second[2 * kParts + 3];
+            h->band[0] = it->second[2 * kParts + 4];
+            h->band[1] = it->second[2 * kParts + 5];
             return MITTET_OK;
         }
     }
@@ -1022,13 +1074,17 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             const std::string kt = key_text();
             while (fgets(line, sizeof(line), f)) {
                 if (strncmp(line, kt.c_str(), kt.size()) != 0 || line[kt.size()] != ':') continue;
-                std::array<int, 2 * kParts + 4> e;
+                std::array<int, 2 * kParts + 6> e;
                 int n = 0, off = (int)kt.size() + 1, used = 0;
                 while (n < (int)e.size() && sscanf(line + off, "%d%n", &e[n], &used) == 1) {
                     off += used;
                     n++;
                 }
-                if (n != (int)e.size()) continue;
+                if (n == 2 * kParts + 4) {  // a line without the band fields
+                    e[n] = e[n + 1] = 0;
+                } else if (n != (int)e.size()) {
+                    continue;
+                }
                 for (int p = 0; p < kParts; p++) {
                     h->var_e[p] = e[p];
                     h->var_h[p] = e[kParts + p];
@@ -1037,6 +1093,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
                 h->ldg_int[1] = e[2 * kParts + 1];
                 h->merge_b[0] = e[2 * kParts + 2];
                 h->merge_b[1] = e[2 * kParts + 3];
+                h->band[0] = e[2 * kParts + 4];
+                h->band[1] = e[2 * kParts + 5];
                 fclose(f);
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 g_tune_cache[key] = e;
@@ -1046,6 +1104,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
         }
     }
     h->merge_b[0] = h->merge_b[1] = -1;
+    h->band[0] = h->band[1] = 0;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1156,12 +1215,32 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
                 }
             }
             mb = keep;
+            // the interior and x faces as one band launch (no merged boundary)
+            const int mb_keep = mb;
+            int &bz = h->band[ph];
+            int bkeep = 0;
+            if (h->has_ibox[ph]) {
+                mb = -1;
+                for (int zc : kBandZc) {
+                    bz = zc;
+                    float ms = 0;
+                    if (int rc = phase_ms(&ms)) return rc;
+                    if (std::getenv("MITTET_TUNE_LOG"))
+                        fprintf(stderr, "autotune %s band launch 16x8x%d: %.4f ms\n", ph == 0 ? "E" : "H", zc, ms);
+                    if (ms < best * 0.99f) {
+                        best = ms;
+                        bkeep = zc;
+                    }
+                }
+            }
+            bz = bkeep;
+            mb = bkeep > 0 ? -1 : mb_keep;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    std::array<int, 2 * kParts + 4> entry;
+    std::array<int, 2 * kParts + 6> entry;
     for (int p = 0; p < kParts; p++) {
         entry[p] = h->var_e[p];
         entry[kParts + p] = h->var_h[p];
@@ -1170,6 +1249,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     entry[2 * kParts + 1] = h->ldg_int[1];
     entry[2 * kParts + 2] = h->merge_b[0];
     entry[2 * kParts + 3] = h->merge_b[1];
+    entry[2 * kParts + 4] = h->band[0];
+    entry[2 * kParts + 5] = h->band[1];
     g_tune_cache[key] = entry;
     if (tfile) {
         if (FILE *f = fopen(tfile, "a")) {
@@ -1288,6 +1369,14 @@ int run_forward(mittet_handle *h, int nt) {
         const bool ok = v >= 0 && v < (int)vs.size() && vs[v].bz == 0 &&
                         boundary_kernel_for<T>(vs[v].vx, vs[v].bx, vs[v].by, true) != nullptr;
         h->merge_b[0] = h->merge_b[1] = ok ? v : -1;
+        if (ok) h->band[0] = h->band[1] = 0;
+    }
+    // MITTET_BAND=<zc> forces the band launch of the interior and x faces
+    // with zc planes per band on both phases (0: the part launches)
+    if (const char *bv = std::getenv("MITTET_BAND")) {
+        const int zc = std::max(0, std::atoi(bv));
+        h->band[0] = h->band[1] = zc;
+        if (zc > 0) h->merge_b[0] = h->merge_b[1] = -1;
     }
     // One graph holds G = ring_k steps; the volume flush of those steps (when
     // enabled) is launched after each replay.
@@ -2399,6 +2488,13 @@ int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_var
     if (!h || !e_variant || !h_variant) return fail(MITTET_ERR_INVALID_ARG, "null argument");
     *e_variant = h->merge_b[0];
     *h_variant = h->merge_b[1];
+    return MITTET_OK;
+}
+
+int mittet_band_variant(mittet_handle *h, int32_t *e_zc, int32_t *h_zc) {
+    if (!h || !e_zc || !h_zc) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    *e_zc = h->has_ibox[0] ? h->band[0] : 0;
+    *h_zc = h->has_ibox[1] ? h->band[1] : 0;
     return MITTET_OK;
 }
 

@@ -1023,6 +1023,51 @@ __global__ void __launch_bounds__(BX *BY, (part_min_blocks<T, VX, BX * BY, 7, 0>
     }
 }
 
+// The interior and the two x faces of a phase in one launch, tiles in band
+// order.  A band is BY rows x ZC planes of the interior y-z box; its tiles
+// are the left x-face tiles (x-general body, VXF cells per thread), the
+// interior tiles (interior body, VXI cells per thread) and the right x-face
+// tiles, consecutive in blockIdx.x, so the CTAs in flight at any time read
+// and write whole rows (split launches read the 32-cell x-face segments of
+// a row apart from the rest of it, and row segments that short move DRAM
+// lines well below the copy rate).  The body is chosen per CTA, so no warp
+// diverges; the kernel needs the registers of the heavier body.
+struct BandMap {
+    int x0, x1, nx, y0, y1, z0, z1;  // interior box [x0, x1) x [y0, y1) x [z0, z1), row length nx
+    int zc;                          // z planes per band
+    int ntl, nti, ntr, nty;          // left-face, interior and right-face tiles per band; bands along y
+};
+
+template <typename T, int VXI, int VXF, int BX, int BY, bool EPH>
+__global__ void __launch_bounds__(BX *BY, (sizeof(T) == 4 ? 512 : 384) / (BX * BY))
+    band_kernel(const PhaseArgs<T> a, const BandMap bm) {
+    int b = blockIdx.x;
+    const int per = bm.ntl + bm.nti + bm.ntr;
+    const int t = b % per;
+    b /= per;
+    const int ty = b % bm.nty, tz = b / bm.nty;
+    const int j = bm.y0 + ty * BY + (int)threadIdx.y;
+    const int kb = bm.z0 + tz * bm.zc, ke = min(kb + bm.zc, bm.z1);
+    if (j >= bm.y1) return;
+    if (t >= bm.ntl && t < bm.ntl + bm.nti) {
+        const int i0 = bm.x0 + ((t - bm.ntl) * BX + (int)threadIdx.x) * VXI;
+        if (i0 >= bm.x1) return;
+        if constexpr (EPH)
+            e_cells<T, VXI, 0, false>(a, blockIdx.y, i0, j, kb, ke);
+        else
+            h_cells<T, VXI, 0, false>(a, blockIdx.y, i0, j, kb, ke);
+    } else {
+        const bool left = t < bm.ntl;
+        const int xe = left ? bm.x0 : bm.nx;
+        const int i0 = (left ? 0 : bm.x1) + ((left ? t : t - bm.ntl - bm.nti) * BX + (int)threadIdx.x) * VXF;
+        if (i0 >= xe) return;
+        if constexpr (EPH)
+            e_cells<T, VXF, 1, false>(a, blockIdx.y, i0, j, kb, ke);
+        else
+            h_cells<T, VXF, 1, false>(a, blockIdx.y, i0, j, kb, ke);
+    }
+}
+
 // Variants the autotuner chooses from: (VX, BX, BY, ZC, BZ) = x cells per
 // thread, thread block in x and y, z planes per tile, threads along z.
 // BZ = 0: each thread marches the tile's ZC planes; ZC is a run-time tile

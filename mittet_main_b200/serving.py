@@ -15,6 +15,14 @@ those idle handles hold counts against the budget; a request that does not
 fit otherwise evicts idle handles of free slots, least recently used first.
 The C-ABI calls release the GIL, so slots are host threads.
 
+Waiting requests are considered in arrival order (``policy="fcfs"``) or,
+with ``policy="sjf"``, smallest estimated work first (cell-updates; a
+gradient counts about four forwards), each request's estimate divided by
+1 + (time waited / ``aging_s``) so a large request is not passed over for
+ever.  Under a burst of arrivals the small requests then finish first
+instead of queueing behind large ones, which lowers the median latency at
+the same throughput.
+
 Latency = completion - arrival.  ``serial_latencies`` gives a plain path
 for comparison from measured service times: one request at a time, in
 arrival order.
@@ -111,6 +119,15 @@ def run_request(solver_cache: dict, req: Request):
     return spec
 
 
+def work_estimate(req) -> float:
+    """Cell-updates a request performs (a gradient: checkpoint pass,
+    recompute and adjoint, about 4.4 forwards)."""
+    wl = req.workload
+    cp = wl.cp
+    w = float(cp.nx * cp.ny * cp.nz) * wl.nt * len(wl.shots)
+    return w * (4.4 if req.mode == "gradient" else 1.0)
+
+
 def _default_key(req):
     try:
         return grid_key(req.workload)
@@ -121,8 +138,14 @@ def _default_key(req):
 class MittetServer:
     def __init__(self, n_slots: int = 4, hbm_budget: float = 150e9,
                  executor: Optional[Callable] = None, estimator: Optional[Callable] = None,
-                 keyer: Optional[Callable] = None, resident_estimator: Optional[Callable] = None):
+                 keyer: Optional[Callable] = None, resident_estimator: Optional[Callable] = None,
+                 policy: str = "fcfs", work: Optional[Callable] = None, aging_s: float = 30.0):
+        if policy not in ("fcfs", "sjf"):
+            raise ValueError(f"unknown admission policy {policy!r}")
         self.n_slots = n_slots
+        self.policy = policy
+        self.work = work or work_estimate
+        self.aging_s = float(aging_s)
         self.budget = float(hbm_budget)
         self.executor = executor or run_request
         self.estimator = estimator or (lambda r: estimate_bytes(r.workload, r.mode, r.checkpoint_every))
@@ -144,6 +167,11 @@ class MittetServer:
         whole budget: it then runs with nothing else admitted beside it."""
         b = float(self.estimator(req))
         return min(b, self.budget) if getattr(req, "mode", "forward") == "gradient" else b
+
+    def priority(self, req, t: float) -> float:
+        """SJF admission key at time t (smaller goes first): the estimated
+        work divided by 1 + time waited / aging_s."""
+        return float(self.work(req)) / (1.0 + max(0.0, t - req.arrival) / self.aging_s)
 
     def run(self, requests: list, realtime: bool = True) -> list:
         """Serve ``requests`` (sorted by arrival); returns one Result per request."""
@@ -201,11 +229,15 @@ class MittetServer:
                 t = now()
                 while pending and (not realtime or pending[0].arrival <= t):
                     waiting.append(pending.pop(0))
-                # admit in arrival order; a request that does not fit lets smaller ones pass
+                # admit in policy order; a request that does not fit lets later ones pass
                 admitted = True
                 while admitted:
                     admitted = False
-                    for r in list(waiting):
+                    order = list(waiting)
+                    if self.policy == "sjf":
+                        tnow = now()
+                        order.sort(key=lambda q: self.priority(q, tnow))
+                    for r in order:
                         if not free_slots:
                             break
                         need = self.need(r)

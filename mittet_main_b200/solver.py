@@ -291,8 +291,9 @@ class MittetSolver:
         """The time loop of the last forward: {"persistent": False, ...} for
         the stepped graph of part kernels (with, per phase, the stencil
         variant [VX, BX, BY, ZC] of its merged boundary launch, or None for
-        four boundary launches), else the variant of the persistent
-        multi-shot launch and its CTAs."""
+        four boundary launches, and the z planes per band of its interior +
+        x-face band launch, 0 for separate launches), else the variant of
+        the persistent multi-shot launch and its CTAs."""
         v, g = ctypes.c_int32(), ctypes.c_int32()
         check(self._lib.mittet_persistent_variant(self._h, ctypes.byref(v), ctypes.byref(g)))
         vs = stencil_variants(self.cp.precision == FP64)
@@ -300,8 +301,10 @@ class MittetSolver:
             return {"persistent": True, "variant": vs[v.value], "ctas": g.value}
         be, bh = ctypes.c_int32(), ctypes.c_int32()
         check(self._lib.mittet_boundary_variant(self._h, ctypes.byref(be), ctypes.byref(bh)))
+        ze, zh = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.mittet_band_variant(self._h, ctypes.byref(ze), ctypes.byref(zh)))
         return {"persistent": False, "e_boundary": vs[be.value] if be.value >= 0 else None,
-                "h_boundary": vs[bh.value] if bh.value >= 0 else None}
+                "h_boundary": vs[bh.value] if bh.value >= 0 else None, "e_band": ze.value, "h_band": zh.value}
 
 
 def stencil_variants(fp64: bool = False) -> list:

@@ -138,3 +138,52 @@ def test_gradient_larger_than_the_budget_runs_alone():
     res = srv.run(reqs)
     assert sorted(r.output for r in res) == list(range(6))
     assert running["max_with_big"] == 1 and srv.peak_in_use <= 100
+
+
+def test_sjf_admits_the_smallest_waiting_request_first():
+    """With one slot and a burst of arrivals, policy="sjf" runs the waiting
+    requests in order of estimated work; "fcfs" in arrival order."""
+    def run(policy):
+        order = []
+
+        def execu(cache, req):
+            order.append(req.rid)
+            time.sleep(0.02)
+            return None
+
+        # request 0 occupies the slot while 1..4 arrive
+        reqs = [make(0, 0.0, 5), make(1, 0.001, 40), make(2, 0.002, 10), make(3, 0.003, 30), make(4, 0.004, 20)]
+        srv = MittetServer(n_slots=1, hbm_budget=100, executor=execu, estimator=lambda r: r.size,
+                           policy=policy, work=lambda r: r.size, aging_s=1e6)
+        srv.run(reqs)
+        return order
+
+    assert run("fcfs") == [0, 1, 2, 3, 4]
+    assert run("sjf") == [0, 2, 4, 3, 1]
+
+
+def test_sjf_ageing_lets_a_long_waiting_request_through():
+    """The SJF key divides the work by 1 + waited / aging_s: a large request
+    that has waited many ageing periods goes before a small new one."""
+    srv = MittetServer(n_slots=1, hbm_budget=100, estimator=lambda r: r.size, policy="sjf",
+                       work=lambda r: r.size, aging_s=1.0)
+    big, small = make(0, 0.0, 50), make(1, 9.0, 2)
+    assert srv.priority(big, 9.0) > srv.priority(small, 9.0)     # 50 / 10 = 5 > 2 / 1
+    late = make(2, 29.9, 2)
+    assert srv.priority(big, 30.0) < srv.priority(late, 30.0)    # 50 / 31 = 1.61 < 2 / 1.1 = 1.82
+
+
+def test_unknown_policy_is_rejected():
+    with pytest.raises(ValueError):
+        MittetServer(policy="lifo")
+
+
+def test_work_estimate_counts_cell_updates():
+    from mittet_main_b200 import workloads as W
+    from mittet_main_b200.serving import work_estimate
+
+    wl = W.serving_case(32, 32, 32, 3, 100)
+    fwd = Request(0, 0.0, wl)
+    grad = Request(1, 0.0, wl, mode="gradient")
+    assert work_estimate(fwd) == 32 ** 3 * 100 * 3
+    assert work_estimate(grad) == 4.4 * work_estimate(fwd)
