@@ -398,7 +398,7 @@ def roofline(wl, esz, kt, peak, peak_kind):
     alg_reads = stencil_read_bytes(wl, esz) / cells
     prof = e_phase_profile(esz, wl.volume_dft)
     r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-         "kernel": "E phase (e_part_kernel parts / interior_tma_kernel)", "alg_bytes_per_launch": ebytes,
+         "kernel": "E phase (band_kernel / e_part_kernel parts / interior_tma_kernel)", "alg_bytes_per_launch": ebytes,
          "alg_read_bytes_per_cell": alg_reads, "peak_source": peak_kind, "traffic": None}
     if prof:
         r["read_bytes_per_cell"] = prof["read"]
