@@ -156,6 +156,7 @@ struct mittet_handle_s {
     int ptile[64][kParts + 1] = {{0}};  // per (variant, phase): part p is tiles [ptile[p], ptile[p+1])
     bool tuned = false;
     DevBuf ring, acc;
+    DevBuf stage_sigma, stage_mu;  // host model uploads (kept: a freed buffer would synchronise the device)
     std::vector<double> wt_host;  // volume-DFT weights [n][f] (re, im)
     // Work buffers of mittet_gradient, kept for the next call on this handle
     // (an FWI loop calls it once per iteration; allocating and freeing ~100
@@ -163,10 +164,10 @@ struct mittet_handle_s {
     // frees them.
     struct GradBufs {
         DevBuf obs, R, mis, asrc, asp, fl[6], pe[3][2], pH[3][2], hist, ck, lam[6], lpe[3][2], lph[3][2], mu[7],
-            gacc, gred;
+            gacc, gred, gpts;
         template <typename F>
         void each(F f) {
-            for (DevBuf *b : {&obs, &R, &mis, &asrc, &asp, &hist, &ck, &gacc, &gred}) f(*b);
+            for (DevBuf *b : {&obs, &R, &mis, &asrc, &asp, &hist, &ck, &gacc, &gred, &gpts}) f(*b);
             for (int c = 0; c < 6; c++) { f(fl[c]); f(lam[c]); }
             for (int c = 0; c < 7; c++) f(mu[c]);
             for (int a = 0; a < 3; a++)
@@ -1718,7 +1719,7 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
             sp.g = asp[q].g;
             gp.push_back(sp);
         }
-        DevBuf d_gp;
+        DevBuf &d_gp = h->gb.gpts;  // kept: a freed buffer would synchronise the device
         CK(d_gp.ensure(std::max<size_t>(gp.size(), 1) * sizeof(SrcPoint)));
         CK(cudaMemcpyAsync(d_gp.p, gp.data(), gp.size() * sizeof(SrcPoint), cudaMemcpyHostToDevice, h->st));
         PhaseArgs<T> ea = phase_args<T>(h, true), ha = phase_args<T>(h, false);
@@ -2187,7 +2188,7 @@ int mittet_set_model(mittet_handle *h, const double *sigma, const double *mu) {
                 return fail(MITTET_ERR_INVALID_ARG, "mu[%zu] = %g is not positive and finite", q, mu[q]);
     h->sigma_h.assign(sigma, sigma + n);
     if (mu) h->mu_h.assign(mu, mu + n); else h->mu_h.clear();
-    DevBuf ds, dm;
+    DevBuf &ds = h->stage_sigma, &dm = h->stage_mu;
     CK(ds.ensure(n * 8));
     CK(cudaMemcpyAsync(ds.p, sigma, n * 8, cudaMemcpyHostToDevice, h->st));
     if (mu) {

@@ -73,7 +73,7 @@ def estimate_bytes(wl, mode: str = "forward", checkpoint_every: int = 200) -> in
     ns = len(wl.shots)
     nc = cp.ncpml
     slab = 2 * (nc * cp.ny * cp.nz + cp.nz * nc * px + nc * cp.ny * px)  # both slab groups, rough
-    b = ns * (6 * fshot + 4 * slab) * esz + 2 * fshot * esz
+    b = ns * (6 * fshot + 4 * slab) * esz + 2 * fshot * esz + cp.nx * cp.ny * cp.nz * 8  # + FP64 model upload stage
     b += ns * len(wl.receivers) * wl.nt * esz + ns * len(wl.receivers) * len(wl.omega) * 16
     if wl.volume_dft:
         b += 64 * 3 * ns * fshot * esz + ns * 3 * len(wl.omega) * fshot * 16
