@@ -239,7 +239,12 @@ int mittet_satan_gamma(int32_t device, const mittet_grid *grid, int32_t nrec, co
  * PyTorch front end).  Pointers are device pointers of the handle's device;
  * stream is the caller's cudaStream_t (NULL = the legacy default stream): the
  * solve starts after the work already queued there and the stream waits for
- * the solve, so events recorded on it bracket the whole solve. */
+ * the solve, so events recorded on it bracket the whole solve.
+ * mittet_set_model_device: sigma (and mu, or NULL) are [nz][ny][nx] arrays of
+ * double (is_fp64 = 1) or float (0), whatever the handle's precision; the
+ * model stays on the device (checked there: MITTET_ERR_INVALID_ARG for a
+ * value that is not positive and finite), and m = 2 w0 dt / sigma is formed
+ * in FP64 from the given values as mittet_set_model does. */
 int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu, int32_t is_fp64);
 int mittet_forward_device(mittet_handle *h, int32_t nt, void *rec_fd_dev, void *stream);
 

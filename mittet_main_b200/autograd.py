@@ -4,7 +4,9 @@ forward(sigma) runs the batched forward solve and the discrete adjoint on the
 GPU (mittet_gradient: checkpointed forward, recomputation, adjoint sweep) and
 returns the misfit 0.5 sum |S - obs|^2 over shots, receivers and frequencies;
 backward multiplies the stored gradient d(misfit)/d(sigma) (satan_i layout:
-[nz, ny, nx], zero in the CPML frame) by the incoming gradient.
+[nz, ny, nx], zero in the CPML frame) by the incoming gradient.  A CUDA sigma
+goes to the solver from device memory (mittet_set_model_device), without a
+host round trip.
 """
 from __future__ import annotations
 
@@ -18,8 +20,10 @@ class MisfitFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, sigma: torch.Tensor, solver: MittetSolver, obs: np.ndarray, nt: int,
                 checkpoint_every: int = 200):
-        s = sigma.detach().to(torch.float64).cpu().numpy()
-        solver.set_model(s)
+        if sigma.is_cuda:
+            solver.set_model_device(sigma.detach().to(torch.float64).contiguous())
+        else:
+            solver.set_model(sigma.detach().to(torch.float64).numpy())
         misfit, grad = solver.gradient(nt, obs, checkpoint_every)
         ctx.save_for_backward(torch.from_numpy(grad).to(device=sigma.device, dtype=sigma.dtype))
         return sigma.new_tensor(misfit)

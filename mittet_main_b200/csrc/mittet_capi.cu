@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <array>
 #include <map>
 #include <mutex>
@@ -156,7 +157,8 @@ struct mittet_handle_s {
     int ptile[64][kParts + 1] = {{0}};  // per (variant, phase): part p is tiles [ptile[p], ptile[p+1])
     bool tuned = false;
     DevBuf ring, acc;
-    DevBuf stage_sigma, stage_mu;  // host model uploads (kept: a freed buffer would synchronise the device)
+    DevBuf stage_sigma, stage_mu;  // FP64 model stage of uploads (kept: a freed buffer would synchronise the device)
+    bool model_dev = false;        // the model came from device memory: sigma_h / mu_h are empty, the stage holds it
     std::vector<double> wt_host;  // volume-DFT weights [n][f] (re, im)
     // Work buffers of mittet_gradient, kept for the next call on this handle
     // (an FWI loop calls it once per iteration; allocating and freeing ~100
@@ -1555,6 +1557,8 @@ int validate_ready(mittet_handle *h, int nt) {
 // The captured step graph reads the points from d_pts at run time, so it
 // stays valid unless the buffer moves or the number or kinds of points
 // change (those are baked into the graph's launches).
+double model_value(mittet_handle *h, int which, size_t c0);
+
 int upload_sources(mittet_handle *h) {
     if (!h->has_model || h->pts.empty()) return MITTET_OK;
     std::vector<SrcPoint> dp(h->pts.size());
@@ -1571,11 +1575,11 @@ int upload_sources(mittet_handle *h) {
         dp[q].comp = p.comp;
         dp[q].kind = p.kind;
         if (p.kind == MITTET_SRC_MAGNETIC) {
-            const double mu = h->mu_h.empty() ? h->ph.mu0 : h->mu_h[c0];
+            const double mu = h->has_mu ? model_value(h, 1, c0) : h->ph.mu0;
             dp[q].g = p.amp * h->ph.dt / mu / vol;
             h->has_mag = true;
         } else {
-            dp[q].g = p.amp * h->ph.dt * 2.0 * h->ph.omega0 / h->sigma_h[c0] / vol;
+            dp[q].g = p.amp * h->ph.dt * 2.0 * h->ph.omega0 / model_value(h, 0, c0) / vol;
             h->has_ele = true;
         }
     }
@@ -1658,8 +1662,8 @@ int run_gradient(mittet_handle *h, int nt, const double *obs_host, int K, double
         a.moff = a.off;
         a.shot = p.shot; a.comp = p.comp; a.kind = p.kind;
         a.i = p.ix - 1; a.j = p.iy - 1; a.k = p.iz - 1;
-        a.g = p.kind == MITTET_SRC_MAGNETIC ? p.amp * h->ph.dt / (h->mu_h.empty() ? h->ph.mu0 : h->mu_h[c0]) / vol
-                                            : p.amp * h->ph.dt * 2.0 * h->ph.omega0 / h->sigma_h[c0] / vol;
+        a.g = p.kind == MITTET_SRC_MAGNETIC ? p.amp * h->ph.dt / (h->has_mu ? model_value(h, 1, c0) : h->ph.mu0) / vol
+                                            : p.amp * h->ph.dt * 2.0 * h->ph.omega0 / model_value(h, 0, c0) / vol;
     }
     DevBuf &d_asp = B.asp;
     CK(d_asp.ensure(std::max<size_t>(asp.size(), 1) * sizeof(AdjSrc)));
@@ -2002,8 +2006,8 @@ __global__ void model_kernel(const double *__restrict__ sig, const double *__res
     }
 }
 
-template <typename T>
-__global__ void model_kernel_dev(const T *__restrict__ sig, const T *__restrict__ mu, int nx, int ny, int nz, int px,
+template <typename S, typename T>
+__global__ void model_kernel_dev(const S *__restrict__ sig, const S *__restrict__ mu, int nx, int ny, int nz, int px,
                                  double two_w0_dt, double dt, T *__restrict__ m, T *__restrict__ dtmu) {
     const long long n = (long long)nx * ny * nz;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
@@ -2013,6 +2017,38 @@ __global__ void model_kernel_dev(const T *__restrict__ sig, const T *__restrict_
         m[o] = (T)(two_w0_dt / (double)sig[e]);
         if (mu) dtmu[o] = (T)(dt / (double)mu[e]);
     }
+}
+
+// A device model's check (sig64 == nullptr: bit 0 of *bad when a
+// conductivity, bit 1 when a permeability is not positive and finite) or its
+// FP64 copy for the source gains.
+template <typename T>
+__global__ void model_stage_kernel(const T *__restrict__ sig, const T *__restrict__ mu, long long n,
+                                   double *__restrict__ sig64, double *__restrict__ mu64, int *bad) {
+    int b = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double s = (double)sig[e];
+        const double u = mu ? (double)mu[e] : 1.0;
+        if (sig64) {
+            sig64[e] = s;
+            if (mu) mu64[e] = u;
+        } else {
+            b |= (!(s > 0.0) || !isfinite(s)) | ((!(u > 0.0) || !isfinite(u)) << 1);
+        }
+    }
+    if (b) atomicOr(bad, b);
+}
+
+// sigma (which 0) or mu (which 1) at model cell c0 (x fastest, no padding):
+// from the host copy of a host-set model, else from the device stage of a
+// device-set one (one 8-byte read, for the few source cells).
+double model_value(mittet_handle *h, int which, size_t c0) {
+    const std::vector<double> &hv = which ? h->mu_h : h->sigma_h;
+    if (!h->model_dev) return hv[c0];
+    double v = 0.0;
+    const DevBuf &d = which ? h->stage_mu : h->stage_sigma;
+    cudaMemcpy(&v, d.as<double>() + c0, 8, cudaMemcpyDeviceToHost);
+    return v;
 }
 
 }  // namespace
@@ -2188,6 +2224,7 @@ int mittet_set_model(mittet_handle *h, const double *sigma, const double *mu) {
                 return fail(MITTET_ERR_INVALID_ARG, "mu[%zu] = %g is not positive and finite", q, mu[q]);
     h->sigma_h.assign(sigma, sigma + n);
     if (mu) h->mu_h.assign(mu, mu + n); else h->mu_h.clear();
+    h->model_dev = false;
     DevBuf &ds = h->stage_sigma, &dm = h->stage_mu;
     CK(ds.ensure(n * 8));
     CK(cudaMemcpyAsync(ds.p, sigma, n * 8, cudaMemcpyHostToDevice, h->st));
@@ -2227,30 +2264,33 @@ int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu,
     int rc = set_device(h);
     if (rc) return rc;
     const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
-    // a host copy is kept for the electric source gains
-    h->sigma_h.resize(n);
-    if (is_fp64) {
-        CK(cudaMemcpy(h->sigma_h.data(), sigma, n * 8, cudaMemcpyDeviceToHost));
-    } else {
-        std::vector<float> tmp(n);
-        CK(cudaMemcpy(tmp.data(), sigma, n * 4, cudaMemcpyDeviceToHost));
-        for (size_t q = 0; q < n; q++) h->sigma_h[q] = tmp[q];
-    }
-    for (size_t q = 0; q < n; q++)
-        if (!(h->sigma_h[q] > 0) || !std::isfinite(h->sigma_h[q]))
-            return fail(MITTET_ERR_INVALID_ARG, "sigma[%zu] is not a positive finite conductivity", q);
-    if (mu) {
-        h->mu_h.resize(n);
-        if (is_fp64) {
-            CK(cudaMemcpy(h->mu_h.data(), mu, n * 8, cudaMemcpyDeviceToHost));
-        } else {
-            std::vector<float> tmp(n);
-            CK(cudaMemcpy(tmp.data(), mu, n * 4, cudaMemcpyDeviceToHost));
-            for (size_t q = 0; q < n; q++) h->mu_h[q] = tmp[q];
-        }
-    } else {
-        h->mu_h.clear();
-    }
+    // the model stays on the device: a device-side check (a rejected model
+    // leaves the handle's model as it was), then an FP64 stage that the
+    // source gains read their few cells from; no host round trip
+    CK(h->d_flag.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->st));
+    auto stage = [&](double *s64, double *m64) {
+        if (is_fp64)
+            model_stage_kernel<double><<<1024, 256, 0, h->st>>>((const double *)sigma, (const double *)mu, (long long)n,
+                                                                s64, m64, h->d_flag.as<int>());
+        else
+            model_stage_kernel<float><<<1024, 256, 0, h->st>>>((const float *)sigma, (const float *)mu, (long long)n,
+                                                               s64, m64, h->d_flag.as<int>());
+    };
+    stage(nullptr, nullptr);
+    CK(cudaGetLastError());
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (bad & 1) return fail(MITTET_ERR_INVALID_ARG, "sigma holds a conductivity that is not positive and finite");
+    if (bad & 2) return fail(MITTET_ERR_INVALID_ARG, "mu holds a permeability that is not positive and finite");
+    CK(h->stage_sigma.ensure(n * 8));
+    if (mu) CK(h->stage_mu.ensure(n * 8));
+    stage(h->stage_sigma.as<double>(), mu ? h->stage_mu.as<double>() : nullptr);
+    CK(cudaGetLastError());
+    h->sigma_h.clear();
+    h->mu_h.clear();
+    h->model_dev = true;
     const size_t cb = (size_t)h->fshot * h->esz;
     const void *m0 = h->m.p, *dm0 = h->dtmu.p;
     CK(h->m.ensure(cb));
@@ -2261,16 +2301,20 @@ int mittet_set_model_device(mittet_handle *h, const void *sigma, const void *mu,
     }
     if (h->m.p != m0 || h->dtmu.p != dm0 || h->has_mu != (mu != nullptr) || !h->has_model) drop_graph(h);
     const double k = 2.0 * h->ph.omega0 * h->ph.dt;
-    if (h->fp64 && is_fp64)
-        model_kernel_dev<double><<<1024, 256, 0, h->st>>>((const double *)sigma, (const double *)mu, h->g.nx, h->g.ny,
-                                                          h->g.nz, h->px, k, h->ph.dt, h->m.as<double>(),
-                                                          mu ? h->dtmu.as<double>() : nullptr);
-    else if (!h->fp64 && !is_fp64)
-        model_kernel_dev<float><<<1024, 256, 0, h->st>>>((const float *)sigma, (const float *)mu, h->g.nx, h->g.ny,
-                                                         h->g.nz, h->px, k, h->ph.dt, h->m.as<float>(),
-                                                         mu ? h->dtmu.as<float>() : nullptr);
+    // m = 2 w0 dt / sigma formed in FP64 from the given values, as set_model does
+    auto launch = [&](auto *sg, auto *mg) {
+        using S = std::remove_const_t<std::remove_pointer_t<decltype(sg)>>;
+        if (h->fp64)
+            model_kernel_dev<S, double><<<1024, 256, 0, h->st>>>(sg, mg, h->g.nx, h->g.ny, h->g.nz, h->px, k, h->ph.dt,
+                                                                 h->m.as<double>(), mu ? h->dtmu.as<double>() : nullptr);
+        else
+            model_kernel_dev<S, float><<<1024, 256, 0, h->st>>>(sg, mg, h->g.nx, h->g.ny, h->g.nz, h->px, k, h->ph.dt,
+                                                                h->m.as<float>(), mu ? h->dtmu.as<float>() : nullptr);
+    };
+    if (is_fp64)
+        launch((const double *)sigma, (const double *)mu);
     else
-        return fail(MITTET_ERR_INVALID_ARG, "model dtype must match the handle precision");
+        launch((const float *)sigma, (const float *)mu);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
     h->has_model = true;
@@ -2620,7 +2664,11 @@ int mittet_fwi_update(mittet_handle *h, int32_t nt, const double *obs, const dou
     for (size_t q = 0; q < n; q++) sig2[q] = sigma[q] - scaler * grad[q];
     // trial forward of every shot (media_coeff_sig_tmp + fwdpropagation + laplaceToFreq_3)
     std::vector<double> mu_keep = h->mu_h;
-    const double *mu = mu_keep.empty() ? nullptr : mu_keep.data();
+    if (h->model_dev && h->has_mu) {  // a device-set permeability: bring it to the host once
+        mu_keep.resize(n);
+        CK(cudaMemcpy(mu_keep.data(), h->stage_mu.p, n * 8, cudaMemcpyDeviceToHost));
+    }
+    const double *mu = (h->has_mu && !mu_keep.empty()) ? mu_keep.data() : nullptr;
     rc = mittet_set_model(h, sig2.data(), mu);
     if (rc) return rc;
     const int nf = (int)h->omega.size();

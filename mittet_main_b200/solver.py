@@ -162,11 +162,21 @@ class MittetSolver:
         check(self._lib.mittet_set_model(self._h, _dptr(s), _dptr(m) if m is not None else None))
 
     def set_model_device(self, sigma, mu=None):
-        """sigma/mu as CUDA torch tensors of the handle's precision."""
-        fp64 = self.cp.precision == FP64
+        """sigma/mu as contiguous [nz, ny, nx] CUDA torch tensors (float64 or
+        float32, both the same) on the handle's device; the model stays on the
+        device."""
+        import torch
+
+        if sigma.dtype not in (torch.float64, torch.float32) or not sigma.is_cuda or not sigma.is_contiguous():
+            raise ValueError("sigma must be a contiguous float64 or float32 CUDA tensor")
+        if sigma.numel() != self.cp.nx * self.cp.ny * self.cp.nz:
+            raise ValueError("sigma has the wrong number of cells")
+        if mu is not None and (mu.dtype != sigma.dtype or mu.shape != sigma.shape or not mu.is_cuda
+                               or not mu.is_contiguous()):
+            raise ValueError("mu must be a contiguous CUDA tensor of sigma's dtype and shape")
         check(self._lib.mittet_set_model_device(self._h, ctypes.c_void_p(sigma.data_ptr()),
                                                 ctypes.c_void_p(mu.data_ptr()) if mu is not None else None,
-                                                1 if fp64 else 0))
+                                                1 if sigma.dtype == torch.float64 else 0))
 
     def set_shots(self, shots: Sequence[Shot]):
         pts = []

@@ -124,6 +124,26 @@ def test_autograd_function_returns_the_gradient():
     assert np.array_equal(sig.grad.numpy(), G)
 
 
+def test_autograd_takes_a_cuda_sigma_from_device_memory():
+    """A CUDA sigma reaches the solver through mittet_set_model_device (no
+    host round trip) and gives the misfit and gradient of the host path bit
+    for bit; the gradient comes back on sigma's device."""
+    import torch
+    from mittet_main_b200.autograd import fwi_misfit
+
+    wl, obs = case(FP64, nt=60)
+    with W.make_solver(wl) as s:
+        sig = torch.tensor(wl.sigma, dtype=torch.float64, requires_grad=True)
+        f = fwi_misfit(sig, s, obs, wl.nt, 20)
+        f.backward()
+        sig_d = torch.tensor(wl.sigma, dtype=torch.float64, device="cuda", requires_grad=True)
+        f_d = fwi_misfit(sig_d, s, obs, wl.nt, 20)
+        f_d.backward()
+    assert sig_d.grad.is_cuda
+    assert float(f_d.detach()) == pytest.approx(float(f.detach()), rel=1e-13)
+    assert np.array_equal(sig_d.grad.cpu().numpy(), sig.grad.numpy())
+
+
 def test_fwi_update_is_the_satan_i_step():
     """mittet_fwi_update = calc_phi, a forward on the trial model, calc_alpha
     and update_para2, restated in oracle.calc_phi / oracle.update_para2."""

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from mittet_main_b200 import workloads as W
-from mittet_main_b200.capi import FLAVOR_NCVER0027, FLAVOR_SATAN_I, FP32, FP64, SRC_ELECTRIC
+from mittet_main_b200.capi import FLAVOR_NCVER0027, FLAVOR_SATAN_I, FP32, FP64, SRC_ELECTRIC, MittetError
 from mittet_main_b200.solver import ConstPara, MittetSolver, Shot, f_to_d
 from oracle import oracle as O
 from tests.conftest import rel_l2
@@ -423,3 +423,33 @@ def test_band_launch_is_bit_identical(monkeypatch, prec, n):
             assert np.array_equal(va, vb), zc
         for fa, fb in zip(fields, base[3]):
             assert np.array_equal(fa, fb), zc
+
+
+@pytest.mark.parametrize("prec", [FP32, FP64])
+def test_device_model_equals_host_model(prec):
+    """mittet_set_model_device (float64 or float32 CUDA arrays, with mu and
+    with electric and magnetic sources) forms the same model words and
+    source gains as mittet_set_model given the same values: bit-identical
+    spectra and traces.  A zero conductivity is rejected on the device."""
+    import torch
+
+    wl = W.small_case(n=(40, 36, 32), ncpml=6, nt=60, precision=prec, magnetic=True)
+    wl = replace(wl, shots=[wl.shots[0], Shot(points=[(12, 20, 14, "ey", SRC_ELECTRIC, 0.8)])])
+    rng = np.random.default_rng(4)
+    mu = wl.cp.mu0 * (1.0 + 0.2 * rng.random(wl.sigma.shape))
+    for dt in (torch.float64, torch.float32):
+        # the host path gets the values the device path is given
+        sig_h = torch.tensor(wl.sigma, dtype=dt).to(torch.float64).numpy()
+        mu_h = torch.tensor(mu, dtype=dt).to(torch.float64).numpy()
+        with W.make_solver(replace(wl, sigma=sig_h, mu=mu_h)) as s:
+            ref_spec, ref_td = s.forward(wl.nt, want_traces=True)
+            s.set_model_device(torch.tensor(sig_h, dtype=dt, device="cuda"), torch.tensor(mu_h, dtype=dt, device="cuda"))
+            spec, td = s.forward(wl.nt, want_traces=True)
+            assert np.array_equal(spec, ref_spec) and np.array_equal(td, ref_td), dt
+            bad = torch.tensor(sig_h, dtype=dt, device="cuda")
+            bad[3, 4, 5] = 0.0
+            with pytest.raises(MittetError):
+                s.set_model_device(bad)
+            s.set_model_device(torch.tensor(sig_h, dtype=dt, device="cuda"), torch.tensor(mu_h, dtype=dt, device="cuda"))
+            again, _ = s.forward(wl.nt)
+            assert np.array_equal(again, ref_spec), dt
