@@ -257,7 +257,7 @@ def main():
     gpu_launches = launches0 * args.steps
 
     # per-kernel device times (CUDA events on the launching stream) for the roofline
-    kt = solver.time_kernels(min(64, wl.nt))
+    kt = solver.time_kernels(min(128, wl.nt))  # one ring period: the flush runs once
     esz = 8 if prec == FP64 else 4
     peak, peak_kind = peaks()
     roof = roofline(wl, esz, kt, peak, peak_kind)
@@ -307,7 +307,7 @@ def main():
             out64 = torch.zeros_like(out)
             st64, sw64 = max(1, min(args.steps, 2)), 1
             t64, l64, c64 = timed_solves(s64, wl64, st64, sw64, None, dev, out64, stream)
-            kt64 = s64.time_kernels(min(64, wl.nt))
+            kt64 = s64.time_kernels(min(128, wl.nt))
             s64.close()
             extras["fp64"] = {"value": cells * st64 / (t64 / 1e3) / 1e9, "unit": "Gcell/s", "steps": st64,
                               "warmup": sw64, "ms_per_step": t64 / st64, "kernel_ms": kt64,

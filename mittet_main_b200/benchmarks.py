@@ -1,7 +1,7 @@
 """Reports of the batching, gradient and serving workloads (``bench.py --mode``).
 
 batching: 64 shots of one 192x192x128 model in one batched solve (one CUDA
-  graph per 64 steps, all shots in every launch) against the same 64 shots
+  graph per 128 steps, all shots in every launch) against the same 64 shots
   solved one at a time on the same GPU; shot-solves/s of both and the ratio.
 gradient: FWI gradient of the 128x128x96 model, 16 shots, Ex/Ey at 3
   frequencies, checkpoints every 200 steps; seconds per gradient and Gcell/s

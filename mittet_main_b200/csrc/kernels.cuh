@@ -9,7 +9,7 @@
 //   H phase: h_part_kernel x 5 / interior_tma_kernel
 //                   H update + CPML psi_H        cpu_eh_field_cpml42.f90:210-253, cpu_cpml4.f90:384-474
 //   sample_kernel   receiver gather + step++     cpu_output.f90:20-30
-// and every 64 steps volume_dft_kernel folds the E ring into the spectra.
+// and every 128 steps volume_dft_kernel folds the E ring into the spectra.
 // The step index lives in device memory (d_step) so a block of steps can be
 // captured once in a CUDA graph and replayed.
 //
@@ -240,20 +240,23 @@ __global__ void trace_dft_kernel(const T *__restrict__ x, int ntrace, int nt, co
 
 // ---------------------------------------------------- full-volume f_to_d
 //
-// Every ring_k (= 64) steps the E phase has left the last values of each
+// Every ring_k (= 128) steps the E phase has left the last values of each
 // selected E component in the ring; this kernel folds them into the FP64
 // accumulators:
 //   acc[shot][vc][f][cell] += sum_{s<cnt} wt[n0+s][f] * ring(vc, shot*fshot + cell, s),
 //   wt[n][f] = dt exp((i-1) sqrt(w0 w_f) n dt)  (cpu_f_to_d_e.f90:140-142).
-// Grid (cells, component, shot), one thread per cell.  A thread issues its
-// 64 ring loads (one 128-byte line per warp each) before any arithmetic and
-// forms every product and partial sum in FP64 (the ring samples are exact in
-// FP64, the weights are FP64), so the whole transform is accumulated in FP64
-// whatever the field precision: the FP32 path's only DFT error is the
-// rounding of the field samples themselves.  The weights of one group of up
-// to four frequencies are a by-value kernel parameter (zero for s >= cnt), so
-// every multiply reads its weight from the constant bank.
-constexpr int kFlushRing = 64;
+// Grid (cells, component, shot), one thread per cell.  A thread issues the
+// ring loads of a chunk of 64 (FP32) or 32 (FP64) steps (one 128-byte line
+// per warp each) before that chunk's arithmetic and forms every product and
+// partial sum in FP64 (the ring samples are exact in FP64, the weights are
+// FP64), so the whole
+// transform is accumulated in FP64 whatever the field precision: the FP32
+// path's only DFT error is the rounding of the field samples themselves.  The
+// weights of one group of up to four frequencies are a by-value kernel
+// parameter (8 KB; zero for s >= cnt), so every multiply reads its weight
+// from the constant bank.  A ring of 128 steps reads and writes the
+// accumulators half as often as one of 64, for twice the ring memory.
+constexpr int kFlushRing = 128;
 constexpr int kFlushFreqs = 4;
 struct FlushWeights {
     double wr[kFlushRing][kFlushFreqs];
@@ -271,19 +274,24 @@ __global__ void __launch_bounds__(256) volume_dft_kernel(const T *__restrict__ r
     const int vc = vi == 0 ? vcs.x : (vi == 1 ? vcs.y : vcs.z);
     const long long e = (long long)shot * fshot + cell;
     const T *__restrict__ rp = ring + ring_index(ring_comp, ring_k, vc, e, 0);
-    T xs[kFlushRing];
-#pragma unroll
-    for (int s = 0; s < kFlushRing; s++) xs[s] = s < cnt ? __ldcs(rp + s * kRingTile) : T(0);
+    constexpr int kFlushChunk = sizeof(T) == 4 ? 64 : 32;  // ring loads in flight per thread
     double pr[kFlushFreqs], pi[kFlushFreqs];
 #pragma unroll
     for (int f = 0; f < kFlushFreqs; f++) { pr[f] = 0.0; pi[f] = 0.0; }
 #pragma unroll
-    for (int s = 0; s < kFlushRing; s++) {
-        const double x = (double)xs[s];
+    for (int s0 = 0; s0 < kFlushRing; s0 += kFlushChunk) {
+        if (s0 >= cnt) break;
+        T xs[kFlushChunk];
 #pragma unroll
-        for (int f = 0; f < kFlushFreqs; f++) {
-            pr[f] = fma(w.wr[s][f], x, pr[f]);
-            pi[f] = fma(w.wi[s][f], x, pi[f]);
+        for (int s = 0; s < kFlushChunk; s++) xs[s] = s0 + s < cnt ? __ldcs(rp + (s0 + s) * kRingTile) : T(0);
+#pragma unroll
+        for (int s = 0; s < kFlushChunk; s++) {
+            const double x = (double)xs[s];
+#pragma unroll
+            for (int f = 0; f < kFlushFreqs; f++) {
+                pr[f] = fma(w.wr[s0 + s][f], x, pr[f]);
+                pi[f] = fma(w.wi[s0 + s][f], x, pi[f]);
+            }
         }
     }
     double2 *__restrict__ ap = acc + (((long long)shot * 3 + vc) * nf + f0) * fshot + cell;

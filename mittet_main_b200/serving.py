@@ -76,7 +76,7 @@ def estimate_bytes(wl, mode: str = "forward", checkpoint_every: int = 200) -> in
     b = ns * (6 * fshot + 4 * slab) * esz + 2 * fshot * esz + cp.nx * cp.ny * cp.nz * 8  # + FP64 model upload stage
     b += ns * len(wl.receivers) * wl.nt * esz + ns * len(wl.receivers) * len(wl.omega) * 16
     if wl.volume_dft:
-        b += 64 * 3 * ns * fshot * esz + ns * 3 * len(wl.omega) * fshot * 16
+        b += 128 * 3 * ns * fshot * esz + ns * 3 * len(wl.omega) * fshot * 16  # 128-step ring, FP64 accumulators
     if mode == "gradient":
         K = checkpoint_every
         ncheck = -(-wl.nt // K)

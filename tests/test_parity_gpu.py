@@ -189,12 +189,12 @@ def test_volume_dft_with_ring_remainder():
 
 
 def test_volume_dft_matches_receiver_spectra():
-    """Nt = 277 runs four 64-step ring blocks, each folded into the
+    """Nt = 533 runs four 128-step ring blocks, each folded into the
     accumulators before the ring is rewritten, and a remainder.  The volume
     spectra at 80 random cells (all three components) equal the spectra of
     receivers sampled there, an independent path (traces, then the trace
     DFT), to FP64 rounding, and the oracle at three of them."""
-    wl = W.small_case(nt=277, precision=FP64)
+    wl = W.small_case(nt=533, precision=FP64)
     rng = np.random.default_rng(17)
     cells = [(int(rng.integers(1, wl.cp.nx + 1)), int(rng.integers(1, wl.cp.ny + 1)),
               int(rng.integers(1, wl.cp.nz + 1))) for _ in range(80)]

@@ -1,10 +1,10 @@
-"""The persistent multi-shot launch (one cooperative launch per block of 64
+"""The persistent multi-shot launch (one cooperative launch per block of 128
 steps, persistent.cuh) against the stepped graph of part kernels.
 
 Both run the same cell bodies with the same fma forms, so traces, final
 fields and full-volume spectra must be bit-identical, for a batch of shots
 with electric and magnetic sources, in FP32 and FP64, with a remainder block
-shorter than 64 steps.  A grid barrier that cannot complete (it waits for
+shorter than 128 steps.  A grid barrier that cannot complete (it waits for
 one CTA more than the grid has) gives up after its time limit and the solve
 reports MITTET_ERR_DEVICE_TIMEOUT; a new handle then solves normally.
 """
@@ -54,7 +54,7 @@ def test_persistent_launch_is_bit_identical_to_stepped(monkeypatch, prec):
 
 
 def test_persistent_barrier_timeout_reports_and_recovers(monkeypatch):
-    wl = _batch(FP32, nt=70)
+    wl = _batch(FP32, nt=150)
     monkeypatch.setenv("MITTET_PERSIST", "1")
     monkeypatch.setenv("MITTET_PERSIST_STALL", "1")
     monkeypatch.setenv("MITTET_PERSIST_WAIT_MS", "20")
