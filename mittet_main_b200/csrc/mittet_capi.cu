@@ -308,6 +308,12 @@ struct Variant {
 template <typename T>
 const std::vector<Variant<T>> &variants();
 
+// the handle's ptile table holds 64 (variant, phase) slots
+#define MITTET_COUNT(vx, bx, by, zc, bz) +1
+static_assert(0 MITTET_STENCIL_VARIANTS_F32(MITTET_COUNT) <= 32 && 0 MITTET_STENCIL_VARIANTS_F64(MITTET_COUNT) <= 32,
+              "more stencil variants than the ptile table holds");
+#undef MITTET_COUNT
+
 template <>
 const std::vector<Variant<float>> &variants<float>() {
     static const std::vector<Variant<float>> v = {
