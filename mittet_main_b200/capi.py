@@ -114,6 +114,7 @@ SIGNATURES = {
     "mittet_persistent_variant": (ctypes.c_int, [_VP, _P(_I), _P(_I)]),
     "mittet_boundary_variant": (ctypes.c_int, [_VP, _P(_I), _P(_I)]),
     "mittet_band_variant": (ctypes.c_int, [_VP, _P(_I), _P(_I)]),
+    "mittet_layout_variant": (ctypes.c_int, [_VP, _P(_I), _P(_I)]),
     "mittet_forward_noalloc": (ctypes.c_int, [_P(Grid), _P(Phys), _VP, _I, _P(PointSource), _I, _VP, _I,
                                                _P(Receiver), _I, _P(_D), _I, _VP, _VP]),
     "mittet_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),

@@ -150,6 +150,8 @@ struct mittet_handle_s {
     int ldg_int[2] = {0, 0};   // best plain-load interior variant of each phase
     int merge_b[2] = {-1, -1}; // variant of the merged boundary launch of each phase (-1: four part launches)
     int band[2] = {0, 0};      // z planes per band of the interior + x-face band launch (0: part launches)
+    bool one_box[2] = {false, false};     // the phase's forward tiles cover the grid as one general box
+    bool tm_one_box[2] = {false, false};  // the layout the uploaded tile maps have
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
     std::vector<TileMap> tmaps_host;
     DevBuf adj_tmaps;          // one-cell tile maps (32 x 8 x 1) of the E and H phase: the adjoint own kernels
@@ -366,7 +368,7 @@ void interior_box(const mittet_handle *h, bool e, int lo[3], int hi[3]) {
     }
 }
 
-TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int zc) {
+TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int zc, bool one_box = false) {
     TileMap t;
     memset(&t, 0, sizeof(t));
     t.zc = zc;
@@ -407,7 +409,9 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
         const int nzt = (z1 - z0 + zc - 1) / zc;
         t.start[q + 1] = t.start[q] + t.ntx[q] * t.nty[q] * nzt;
     };
-    if (X1 > X0 && Y1 > Y0 && Z1 > Z0) {
+    // one_box: the whole grid as one general box (part 4), the layout the
+    // autotuner may choose for grids that are mostly CPML slab
+    if (X1 > X0 && Y1 > Y0 && Z1 > Z0 && !one_box) {
         t.pbox[0] = t.nbox;
         add(0, X0, Y0, Z0, X1, Y1, Z1);
         t.pbox[1] = t.nbox;
@@ -444,15 +448,17 @@ int upload_tilemaps(mittet_handle *h) {
     const auto &vs = variants<T>();
     std::vector<TileMap> maps(2 * vs.size());
     for (size_t v = 0; v < vs.size(); v++) {
-        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc);
-        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc);
+        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc, h->one_box[0]);
+        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc, h->one_box[1]);
         for (int p = 0; p < 2; p++) {
             const TileMap &t = maps[2 * v + p];
             for (int q = 0; q <= kParts; q++) h->ptile[2 * v + p][q] = t.start[t.pbox[q]];
         }
     }
-    for (int p = 0; p < 2; p++) {  // the interior box (identical in every variant's map)
-        const TileMap &t = maps[p];
+    h->tm_one_box[0] = h->one_box[0];
+    h->tm_one_box[1] = h->one_box[1];
+    for (int p = 0; p < 2; p++) {  // the interior box of the partitioned layout (the adjoint's boxes too)
+        const TileMap t = make_tilemap(h, p == 0, vs[0].vx, vs[0].bx, vs[0].by, vs[0].zc);
         h->has_ibox[p] = t.pbox[1] > t.pbox[0];
         for (int q = 0; q < 3; q++) {
             h->ibox[p][q] = t.lo[0][q];
@@ -462,6 +468,7 @@ int upload_tilemaps(mittet_handle *h) {
     h->tmaps_host = maps;
     CK(h->tmaps.ensure(maps.size() * sizeof(TileMap)));
     CK(cudaMemcpy(h->tmaps.p, maps.data(), maps.size() * sizeof(TileMap), cudaMemcpyHostToDevice));
+    drop_graph(h);
     h->adj_tm_host[0] = make_tilemap(h, true, 1, 32, 8, 1);
     h->adj_tm_host[1] = make_tilemap(h, false, 1, 32, 8, 1);
     CK(h->adj_tmaps.ensure(2 * sizeof(TileMap)));
@@ -616,7 +623,7 @@ template <typename T>
 int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a, cudaStream_t st) {
     using S = TmaShape<T>;
     const int p = e ? 0 : 1;
-    if (!h->has_ibox[p]) return 0;
+    if (!h->has_ibox[p] || h->one_box[p]) return 0;
     const TmaCfg<T> &c = tma_cfgs<T>()[ci];
     const int *ib = h->ibox[p];
     TmaTiling tl;
@@ -679,7 +686,7 @@ template <typename T>
 int launch_band(mittet_handle *h, bool e, int zc, const PhaseArgs<T> &a, cudaStream_t st) {
     using S = BandShape<T>;
     const int p = e ? 0 : 1;
-    if (!h->has_ibox[p] || zc <= 0) return 0;
+    if (!h->has_ibox[p] || h->one_box[p] || zc <= 0) return 0;
     const int *ib = h->ibox[p];
     BandMap bm;
     bm.x0 = ib[0]; bm.y0 = ib[1]; bm.z0 = ib[2];
@@ -753,7 +760,7 @@ int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a)
         return n;
     }
     const int bz = h->band[e ? 0 : 1];
-    if (bz > 0 && h->ev_fork && h->has_ibox[e ? 0 : 1]) {  // one band launch + y faces, z faces, edges
+    if (bz > 0 && h->ev_fork && h->has_ibox[e ? 0 : 1] && !h->one_box[e ? 0 : 1]) {  // band + y, z faces, edges
         cudaEventRecord(h->ev_fork, h->st);
         for (int p = 2; p < kParts; p++) {
             cudaStreamWaitEvent(h->pst[p], h->ev_fork, 0);
@@ -1020,8 +1027,22 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
 // precision by timing each candidate on the handle's own buffers (zero
 // fields, so the state is untouched apart from the ring slot written by the
 // E phase).  Results are cached for the process.
+// Sets the forward layout of each phase (partitioned, or the whole grid as
+// one general box) and re-uploads the tile maps when it changed.
+template <typename T>
+int sync_layout(mittet_handle *h, bool e_one, bool h_one) {
+    h->one_box[0] = e_one;
+    h->one_box[1] = h_one;
+    if (h->tm_one_box[0] == e_one && h->tm_one_box[1] == h_one) return MITTET_OK;
+    return upload_tilemaps<T>(h);
+}
+template <typename T>
+int sync_layout(mittet_handle *h, bool both) {
+    return sync_layout<T>(h, both, both);
+}
+
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 6>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int, int, int>, std::array<int, 2 * kParts + 8>> g_tune_cache;
 
 template <typename T>
 int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
@@ -1046,7 +1067,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             h->merge_b[0] = h->merge_b[1] = -1;
             h->band[0] = h->band[1] = 0;
             if (only_tma) h->var_e[0] = h->var_h[0] = -1;
-            return MITTET_OK;
+            return sync_layout<T>(h, false);
         }
     }
     const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0,
@@ -1065,7 +1086,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             h->merge_b[1] = it->second[2 * kParts + 3];
             h->band[0] = it->second[2 * kParts + 4];
             h->band[1] = it->second[2 * kParts + 5];
-            return MITTET_OK;
+            return sync_layout<T>(h, it->second[2 * kParts + 6], it->second[2 * kParts + 7]);
         }
     }
     // A tune file (MITTET_TUNE_CACHE) carries choices across processes, e.g. so
@@ -1083,14 +1104,14 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             const std::string kt = key_text();
             while (fgets(line, sizeof(line), f)) {
                 if (strncmp(line, kt.c_str(), kt.size()) != 0 || line[kt.size()] != ':') continue;
-                std::array<int, 2 * kParts + 6> e;
+                std::array<int, 2 * kParts + 8> e;
                 int n = 0, off = (int)kt.size() + 1, used = 0;
                 while (n < (int)e.size() && sscanf(line + off, "%d%n", &e[n], &used) == 1) {
                     off += used;
                     n++;
                 }
-                if (n == 2 * kParts + 4) {  // a line without the band fields
-                    e[n] = e[n + 1] = 0;
+                if (n == 2 * kParts + 4 || n == 2 * kParts + 6) {  // a line without (some) later fields
+                    for (int q = n; q < (int)e.size(); q++) e[q] = 0;
                 } else if (n != (int)e.size()) {
                     continue;
                 }
@@ -1105,15 +1126,18 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
                 h->band[0] = e[2 * kParts + 4];
                 h->band[1] = e[2 * kParts + 5];
                 fclose(f);
-                std::lock_guard<std::mutex> lk(g_tune_mu);
-                g_tune_cache[key] = e;
-                return MITTET_OK;
+                {
+                    std::lock_guard<std::mutex> lk(g_tune_mu);
+                    g_tune_cache[key] = e;
+                }
+                return sync_layout<T>(h, e[2 * kParts + 6], e[2 * kParts + 7]);
             }
             fclose(f);
         }
     }
     h->merge_b[0] = h->merge_b[1] = -1;
     h->band[0] = h->band[1] = 0;
+    if (int rc = sync_layout<T>(h, false)) return rc;  // tune the partitioned layout first
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1244,12 +1268,44 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             }
             bz = bkeep;
             mb = bkeep > 0 ? -1 : mb_keep;
+            // the whole grid as one general box (wins where most cells are
+            // CPML slab): every variant on it, kept if the phase is faster
+            if (h->has_ibox[ph] && !std::getenv("MITTET_PARTS_ONLY")) {
+                const int keep_v = var[4], keep_mb = mb, keep_bz = bz;
+                h->one_box[ph] = true;
+                if (int rc = sync_layout<T>(h, h->one_box[0], h->one_box[1])) return rc;
+                mb = -1;
+                bz = 0;
+                int obv = -1;
+                for (int v = 0; v < nv; v++) {
+                    var[4] = v;
+                    float ms = 0;
+                    if (int rc = phase_ms(&ms)) return rc;
+                    if (std::getenv("MITTET_TUNE_LOG"))
+                        fprintf(stderr, "autotune %s one box vx%d %dx%dx%d%s: %.4f ms\n", ph == 0 ? "E" : "H",
+                                variants<T>()[v].vx, variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].zc,
+                                variants<T>()[v].bz > 0 ? " one-plane" : "", ms);
+                    if (ms < best * 0.99f) {
+                        best = ms;
+                        obv = v;
+                    }
+                }
+                if (obv >= 0) {
+                    var[4] = obv;
+                } else {
+                    var[4] = keep_v;
+                    mb = keep_mb;
+                    bz = keep_bz;
+                    h->one_box[ph] = false;
+                    if (int rc = sync_layout<T>(h, h->one_box[0], h->one_box[1])) return rc;
+                }
+            }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    std::array<int, 2 * kParts + 6> entry;
+    std::array<int, 2 * kParts + 8> entry;
     for (int p = 0; p < kParts; p++) {
         entry[p] = h->var_e[p];
         entry[kParts + p] = h->var_h[p];
@@ -1260,6 +1316,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     entry[2 * kParts + 3] = h->merge_b[1];
     entry[2 * kParts + 4] = h->band[0];
     entry[2 * kParts + 5] = h->band[1];
+    entry[2 * kParts + 6] = h->one_box[0] ? 1 : 0;
+    entry[2 * kParts + 7] = h->one_box[1] ? 1 : 0;
     g_tune_cache[key] = entry;
     if (tfile) {
         if (FILE *f = fopen(tfile, "a")) {
@@ -1386,6 +1444,17 @@ int run_forward(mittet_handle *h, int nt) {
         const int zc = std::max(0, std::atoi(bv));
         h->band[0] = h->band[1] = zc;
         if (zc > 0) h->merge_b[0] = h->merge_b[1] = -1;
+    }
+    // MITTET_ONE_BOX=1 / 0 forces the whole grid as one general box on both
+    // phases (with the edge part's variant) / the partitioned layout
+    if (const char *ob = std::getenv("MITTET_ONE_BOX")) {
+        const bool on = std::atoi(ob) != 0;
+        if (on) {
+            h->band[0] = h->band[1] = 0;
+            h->merge_b[0] = h->merge_b[1] = -1;
+        }
+        rc = sync_layout<T>(h, on, on);
+        if (rc) return rc;
     }
     // One graph holds G = ring_k steps; the volume flush of those steps (when
     // enabled) is launched after each replay.
@@ -2539,6 +2608,13 @@ int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_var
     if (!h || !e_variant || !h_variant) return fail(MITTET_ERR_INVALID_ARG, "null argument");
     *e_variant = h->merge_b[0];
     *h_variant = h->merge_b[1];
+    return MITTET_OK;
+}
+
+int mittet_layout_variant(mittet_handle *h, int32_t *e_one_box, int32_t *h_one_box) {
+    if (!h || !e_one_box || !h_one_box) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    *e_one_box = h->one_box[0] ? 1 : 0;
+    *h_one_box = h->one_box[1] ? 1 : 0;
     return MITTET_OK;
 }
 
