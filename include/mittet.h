@@ -299,12 +299,13 @@ int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_var
  * tuning introspection). */
 int mittet_band_variant(mittet_handle *h, int32_t *e_zc, int32_t *h_zc);
 
-/* Whether the forward tiles of each phase cover the grid as one box with
- * the general (CPML on every axis) body: 1 for the E / H phase when so, 0
- * when the phase is split into interior, faces and edges.  Chosen by the
- * autotuner per grid and batch (one box wins on grids that are mostly CPML
- * slab).  No counterpart in the reference (a tuning introspection). */
-int mittet_layout_variant(mittet_handle *h, int32_t *e_one_box, int32_t *h_one_box);
+/* How the forward tiles of the E / H phase cover the grid: 0 split into
+ * interior, faces and edges; 1 the whole grid as one box with the general
+ * (CPML on every axis) body; 2 the interior and x faces as in 0 and the y-
+ * and z-slab rows whole, in general boxes.  Chosen by the autotuner per grid
+ * and batch (1 wins on grids that are mostly CPML slab).  No counterpart in
+ * the reference (a tuning introspection). */
+int mittet_layout_variant(mittet_handle *h, int32_t *e_layout, int32_t *h_layout);
 
 /* Number of kernels the last forward launched (for launch accounting). */
 int64_t mittet_last_launch_count(mittet_handle *h);

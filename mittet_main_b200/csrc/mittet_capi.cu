@@ -150,8 +150,11 @@ struct mittet_handle_s {
     int ldg_int[2] = {0, 0};   // best plain-load interior variant of each phase
     int merge_b[2] = {-1, -1}; // variant of the merged boundary launch of each phase (-1: four part launches)
     int band[2] = {0, 0};      // z planes per band of the interior + x-face band launch (0: part launches)
-    bool one_box[2] = {false, false};     // the phase's forward tiles cover the grid as one general box
-    bool tm_one_box[2] = {false, false};  // the layout the uploaded tile maps have
+    // forward layout of each phase: kLayoutParts, kLayoutOneBox (the grid as
+    // one general box) or kLayoutCoreRows (interior and x faces as parts, the
+    // y- and z-slab rows whole as general boxes)
+    int layout[2] = {0, 0};
+    int tm_layout[2] = {0, 0};  // the layout the uploaded tile maps have
     DevBuf tmaps;              // TileMap per (variant, phase), device copy
     std::vector<TileMap> tmaps_host;
     DevBuf adj_tmaps;          // one-cell tile maps (32 x 8 x 1) of the E and H phase: the adjoint own kernels
@@ -368,7 +371,9 @@ void interior_box(const mittet_handle *h, bool e, int lo[3], int hi[3]) {
     }
 }
 
-TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int zc, bool one_box = false) {
+enum Layout { kLayoutParts = 0, kLayoutOneBox = 1, kLayoutCoreRows = 2 };
+
+TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int zc, int layout = kLayoutParts) {
     TileMap t;
     memset(&t, 0, sizeof(t));
     t.zc = zc;
@@ -409,9 +414,20 @@ TileMap make_tilemap(const mittet_handle *h, bool e, int vx, int bx, int by, int
         const int nzt = (z1 - z0 + zc - 1) / zc;
         t.start[q + 1] = t.start[q] + t.ntx[q] * t.nty[q] * nzt;
     };
-    // one_box: the whole grid as one general box (part 4), the layout the
-    // autotuner may choose for grids that are mostly CPML slab
-    if (X1 > X0 && Y1 > Y0 && Z1 > Z0 && !one_box) {
+    // kLayoutOneBox: the whole grid as one general box (part 4), the layout
+    // the autotuner may choose for grids that are mostly CPML slab
+    if (X1 > X0 && Y1 > Y0 && Z1 > Z0 && layout == kLayoutCoreRows) {
+        t.pbox[0] = t.nbox;
+        add(0, X0, Y0, Z0, X1, Y1, Z1);
+        t.pbox[1] = t.nbox;
+        add(1, 0, Y0, Z0, X0, Y1, Z1);   // x faces
+        add(1, X1, Y0, Z0, nx, Y1, Z1);
+        t.pbox[2] = t.pbox[3] = t.pbox[4] = t.nbox;
+        add(7, 0, 0, 0, nx, ny, Z0);     // z-slab planes, whole
+        add(7, 0, 0, Z1, nx, ny, nz);
+        add(7, 0, 0, Z0, nx, Y0, Z1);    // y-slab rows of the interior z range, whole
+        add(7, 0, Y1, Z0, nx, ny, Z1);
+    } else if (X1 > X0 && Y1 > Y0 && Z1 > Z0 && layout != kLayoutOneBox) {
         t.pbox[0] = t.nbox;
         add(0, X0, Y0, Z0, X1, Y1, Z1);
         t.pbox[1] = t.nbox;
@@ -448,15 +464,15 @@ int upload_tilemaps(mittet_handle *h) {
     const auto &vs = variants<T>();
     std::vector<TileMap> maps(2 * vs.size());
     for (size_t v = 0; v < vs.size(); v++) {
-        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc, h->one_box[0]);
-        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc, h->one_box[1]);
+        maps[2 * v] = make_tilemap(h, true, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc, h->layout[0]);
+        maps[2 * v + 1] = make_tilemap(h, false, vs[v].vx, vs[v].bx, vs[v].by, vs[v].zc, h->layout[1]);
         for (int p = 0; p < 2; p++) {
             const TileMap &t = maps[2 * v + p];
             for (int q = 0; q <= kParts; q++) h->ptile[2 * v + p][q] = t.start[t.pbox[q]];
         }
     }
-    h->tm_one_box[0] = h->one_box[0];
-    h->tm_one_box[1] = h->one_box[1];
+    h->tm_layout[0] = h->layout[0];
+    h->tm_layout[1] = h->layout[1];
     for (int p = 0; p < 2; p++) {  // the interior box of the partitioned layout (the adjoint's boxes too)
         const TileMap t = make_tilemap(h, p == 0, vs[0].vx, vs[0].bx, vs[0].by, vs[0].zc);
         h->has_ibox[p] = t.pbox[1] > t.pbox[0];
@@ -623,7 +639,7 @@ template <typename T>
 int launch_tma(mittet_handle *h, bool e, int ci, const PhaseArgs<T> &a, cudaStream_t st) {
     using S = TmaShape<T>;
     const int p = e ? 0 : 1;
-    if (!h->has_ibox[p] || h->one_box[p]) return 0;
+    if (!h->has_ibox[p] || h->layout[p] == kLayoutOneBox) return 0;
     const TmaCfg<T> &c = tma_cfgs<T>()[ci];
     const int *ib = h->ibox[p];
     TmaTiling tl;
@@ -686,7 +702,7 @@ template <typename T>
 int launch_band(mittet_handle *h, bool e, int zc, const PhaseArgs<T> &a, cudaStream_t st) {
     using S = BandShape<T>;
     const int p = e ? 0 : 1;
-    if (!h->has_ibox[p] || h->one_box[p] || zc <= 0) return 0;
+    if (!h->has_ibox[p] || h->layout[p] == kLayoutOneBox || zc <= 0) return 0;
     const int *ib = h->ibox[p];
     BandMap bm;
     bm.x0 = ib[0]; bm.y0 = ib[1]; bm.z0 = ib[2];
@@ -760,7 +776,7 @@ int launch_phase(mittet_handle *h, bool e, const int *vi, const PhaseArgs<T> &a)
         return n;
     }
     const int bz = h->band[e ? 0 : 1];
-    if (bz > 0 && h->ev_fork && h->has_ibox[e ? 0 : 1] && !h->one_box[e ? 0 : 1]) {  // band + y, z faces, edges
+    if (bz > 0 && h->ev_fork && h->has_ibox[e ? 0 : 1] && h->layout[e ? 0 : 1] != kLayoutOneBox) {  // band + rest
         cudaEventRecord(h->ev_fork, h->st);
         for (int p = 2; p < kParts; p++) {
             cudaStreamWaitEvent(h->pst[p], h->ev_fork, 0);
@@ -1030,15 +1046,11 @@ int decide_persistent(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<
 // Sets the forward layout of each phase (partitioned, or the whole grid as
 // one general box) and re-uploads the tile maps when it changed.
 template <typename T>
-int sync_layout(mittet_handle *h, bool e_one, bool h_one) {
-    h->one_box[0] = e_one;
-    h->one_box[1] = h_one;
-    if (h->tm_one_box[0] == e_one && h->tm_one_box[1] == h_one) return MITTET_OK;
+int sync_layout(mittet_handle *h, int e_layout, int h_layout) {
+    h->layout[0] = e_layout;
+    h->layout[1] = h_layout;
+    if (h->tm_layout[0] == e_layout && h->tm_layout[1] == h_layout) return MITTET_OK;
     return upload_tilemaps<T>(h);
-}
-template <typename T>
-int sync_layout(mittet_handle *h, bool both) {
-    return sync_layout<T>(h, both, both);
 }
 
 std::mutex g_tune_mu;
@@ -1067,7 +1079,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             h->merge_b[0] = h->merge_b[1] = -1;
             h->band[0] = h->band[1] = 0;
             if (only_tma) h->var_e[0] = h->var_h[0] = -1;
-            return sync_layout<T>(h, false);
+            return sync_layout<T>(h, kLayoutParts, kLayoutParts);
         }
     }
     const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz, h->nshot, (int)h->fp64, ea.ring_k > 0 ? 1 : 0,
@@ -1137,7 +1149,7 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     }
     h->merge_b[0] = h->merge_b[1] = -1;
     h->band[0] = h->band[1] = 0;
-    if (int rc = sync_layout<T>(h, false)) return rc;  // tune the partitioned layout first
+    if (int rc = sync_layout<T>(h, kLayoutParts, kLayoutParts)) return rc;  // tune the partitioned layout first
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1268,37 +1280,38 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
             }
             bz = bkeep;
             mb = bkeep > 0 ? -1 : mb_keep;
-            // the whole grid as one general box (wins where most cells are
-            // CPML slab): every variant on it, kept if the phase is faster
+            // other layouts: the whole grid as one general box (wins where
+            // most cells are CPML slab), and the interior and x faces as
+            // before with the y- and z-slab rows whole in general boxes;
+            // every variant on the general boxes, kept if the phase is faster
             if (h->has_ibox[ph] && !std::getenv("MITTET_PARTS_ONLY")) {
                 const int keep_v = var[4], keep_mb = mb, keep_bz = bz;
-                h->one_box[ph] = true;
-                if (int rc = sync_layout<T>(h, h->one_box[0], h->one_box[1])) return rc;
-                mb = -1;
-                bz = 0;
-                int obv = -1;
-                for (int v = 0; v < nv; v++) {
-                    var[4] = v;
-                    float ms = 0;
-                    if (int rc = phase_ms(&ms)) return rc;
-                    if (std::getenv("MITTET_TUNE_LOG"))
-                        fprintf(stderr, "autotune %s one box vx%d %dx%dx%d%s: %.4f ms\n", ph == 0 ? "E" : "H",
-                                variants<T>()[v].vx, variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].zc,
-                                variants<T>()[v].bz > 0 ? " one-plane" : "", ms);
-                    if (ms < best * 0.99f) {
-                        best = ms;
-                        obv = v;
+                int win_layout = kLayoutParts, win_v = keep_v;
+                for (int lay : {kLayoutOneBox, kLayoutCoreRows}) {
+                    h->layout[ph] = lay;
+                    if (int rc = sync_layout<T>(h, h->layout[0], h->layout[1])) return rc;
+                    mb = lay == kLayoutOneBox ? -1 : keep_mb;
+                    bz = lay == kLayoutOneBox ? 0 : keep_bz;
+                    for (int v = 0; v < nv; v++) {
+                        var[4] = v;
+                        float ms = 0;
+                        if (int rc = phase_ms(&ms)) return rc;
+                        if (std::getenv("MITTET_TUNE_LOG"))
+                            fprintf(stderr, "autotune %s layout %d vx%d %dx%dx%d%s: %.4f ms\n", ph == 0 ? "E" : "H", lay,
+                                    variants<T>()[v].vx, variants<T>()[v].bx, variants<T>()[v].by, variants<T>()[v].zc,
+                                    variants<T>()[v].bz > 0 ? " one-plane" : "", ms);
+                        if (ms < best * 0.99f) {
+                            best = ms;
+                            win_layout = lay;
+                            win_v = v;
+                        }
                     }
                 }
-                if (obv >= 0) {
-                    var[4] = obv;
-                } else {
-                    var[4] = keep_v;
-                    mb = keep_mb;
-                    bz = keep_bz;
-                    h->one_box[ph] = false;
-                    if (int rc = sync_layout<T>(h, h->one_box[0], h->one_box[1])) return rc;
-                }
+                h->layout[ph] = win_layout;
+                var[4] = win_v;
+                mb = win_layout == kLayoutOneBox ? -1 : keep_mb;
+                bz = win_layout == kLayoutOneBox ? 0 : keep_bz;
+                if (int rc = sync_layout<T>(h, h->layout[0], h->layout[1])) return rc;
             }
         }
     }
@@ -1316,8 +1329,8 @@ int autotune(mittet_handle *h, const PhaseArgs<T> &ea, const PhaseArgs<T> &ha) {
     entry[2 * kParts + 3] = h->merge_b[1];
     entry[2 * kParts + 4] = h->band[0];
     entry[2 * kParts + 5] = h->band[1];
-    entry[2 * kParts + 6] = h->one_box[0] ? 1 : 0;
-    entry[2 * kParts + 7] = h->one_box[1] ? 1 : 0;
+    entry[2 * kParts + 6] = h->layout[0];
+    entry[2 * kParts + 7] = h->layout[1];
     g_tune_cache[key] = entry;
     if (tfile) {
         if (FILE *f = fopen(tfile, "a")) {
@@ -1445,15 +1458,16 @@ int run_forward(mittet_handle *h, int nt) {
         h->band[0] = h->band[1] = zc;
         if (zc > 0) h->merge_b[0] = h->merge_b[1] = -1;
     }
-    // MITTET_ONE_BOX=1 / 0 forces the whole grid as one general box on both
-    // phases (with the edge part's variant) / the partitioned layout
-    if (const char *ob = std::getenv("MITTET_ONE_BOX")) {
-        const bool on = std::atoi(ob) != 0;
-        if (on) {
+    // MITTET_LAYOUT=0 / 1 / 2 forces on both phases the partitioned layout /
+    // the whole grid as one general box / the interior and x faces as parts
+    // with the slab rows whole (the general boxes run the edge part's variant)
+    if (const char *ob = std::getenv("MITTET_LAYOUT")) {
+        const int lay = std::min(2, std::max(0, std::atoi(ob)));
+        if (lay == kLayoutOneBox) {
             h->band[0] = h->band[1] = 0;
             h->merge_b[0] = h->merge_b[1] = -1;
         }
-        rc = sync_layout<T>(h, on, on);
+        rc = sync_layout<T>(h, lay, lay);
         if (rc) return rc;
     }
     // One graph holds G = ring_k steps; the volume flush of those steps (when
@@ -2611,10 +2625,10 @@ int mittet_boundary_variant(mittet_handle *h, int32_t *e_variant, int32_t *h_var
     return MITTET_OK;
 }
 
-int mittet_layout_variant(mittet_handle *h, int32_t *e_one_box, int32_t *h_one_box) {
-    if (!h || !e_one_box || !h_one_box) return fail(MITTET_ERR_INVALID_ARG, "null argument");
-    *e_one_box = h->one_box[0] ? 1 : 0;
-    *h_one_box = h->one_box[1] ? 1 : 0;
+int mittet_layout_variant(mittet_handle *h, int32_t *e_layout, int32_t *h_layout) {
+    if (!h || !e_layout || !h_layout) return fail(MITTET_ERR_INVALID_ARG, "null argument");
+    *e_layout = h->layout[0];
+    *h_layout = h->layout[1];
     return MITTET_OK;
 }
 

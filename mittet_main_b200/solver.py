@@ -302,9 +302,10 @@ class MittetSolver:
         the stepped graph of part kernels (with, per phase, the stencil
         variant [VX, BX, BY, ZC] of its merged boundary launch, or None for
         four boundary launches, the z planes per band of its interior +
-        x-face band launch, 0 for separate launches, and whether the phase
-        runs the grid as one general box), else the variant of the
-        persistent multi-shot launch and its CTAs."""
+        x-face band launch, 0 for separate launches, and its layout: 0
+        parts, 1 the grid as one general box, 2 parts with the slab rows
+        whole), else the variant of the persistent multi-shot launch and its
+        CTAs."""
         v, g = ctypes.c_int32(), ctypes.c_int32()
         check(self._lib.mittet_persistent_variant(self._h, ctypes.byref(v), ctypes.byref(g)))
         vs = stencil_variants(self.cp.precision == FP64)
@@ -318,7 +319,7 @@ class MittetSolver:
         check(self._lib.mittet_layout_variant(self._h, ctypes.byref(oe), ctypes.byref(oh)))
         return {"persistent": False, "e_boundary": vs[be.value] if be.value >= 0 else None,
                 "h_boundary": vs[bh.value] if bh.value >= 0 else None, "e_band": ze.value, "h_band": zh.value,
-                "e_one_box": bool(oe.value), "h_one_box": bool(oh.value)}
+                "e_layout": oe.value, "h_layout": oh.value}
 
 
 def stencil_variants(fp64: bool = False) -> list:

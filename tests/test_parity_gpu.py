@@ -456,11 +456,12 @@ def test_device_model_equals_host_model(prec):
 
 
 @pytest.mark.parametrize("prec", [FP32, FP64])
-def test_one_box_layout_is_bit_identical(monkeypatch, prec):
-    """The whole grid as one box with the general body (the layout the
-    autotuner may pick for grids that are mostly CPML slab) gives the
-    fields, traces and volume spectra of the partitioned layout bit for bit,
-    and the gradient (whose adjoint keeps the partitioned boxes) too."""
+def test_layouts_are_bit_identical(monkeypatch, prec):
+    """The whole grid as one box with the general body, and the interior and
+    x faces as parts with the slab rows whole (the layouts the autotuner may
+    pick besides the partitioned one) give the fields, traces and volume
+    spectra of the partitioned layout bit for bit, and the gradient (whose
+    adjoint keeps the partitioned boxes) too."""
     monkeypatch.setenv("MITTET_PERSIST", "0")
     wl = W.small_case(n=(70, 44, 40), ncpml=8, nt=70, precision=prec, magnetic=True)
     second = Shot(points=[(20, 30, 12, "ez", SRC_ELECTRIC, 0.7)])
@@ -469,20 +470,22 @@ def test_one_box_layout_is_bit_identical(monkeypatch, prec):
     obs = (rng.normal(size=(2, len(wl.receivers), len(wl.omega)))
            + 1j * rng.normal(size=(2, len(wl.receivers), len(wl.omega)))) * 1e-12
     out = {}
-    for one in ("0", "1"):
-        monkeypatch.setenv("MITTET_ONE_BOX", one)
+    for lay in ("0", "1", "2"):
+        monkeypatch.setenv("MITTET_LAYOUT", lay)
         with W.make_solver(wl) as s:
             spec, td = s.forward(wl.nt, want_traces=True)
             path = s.launch_path()
             vols = [s.volume_dft(k, c) for k in (0, 1) for c in ("ex", "ey", "ez")]
             fields = [s.fields(k) for k in (0, 1)]
             grad = s.gradient(wl.nt, obs, checkpoint_every=25)
-        assert path["e_one_box"] == (one == "1") and path["h_one_box"] == (one == "1"), path
-        out[one] = (spec, td, vols, fields, grad)
-    a, b = out["0"], out["1"]
-    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-    for va, vb in zip(a[2], b[2]):
-        assert np.array_equal(va, vb)
-    for fa, fb in zip(a[3], b[3]):
-        assert np.array_equal(fa, fb)
-    assert a[4][0] == pytest.approx(b[4][0], rel=1e-13) and np.array_equal(a[4][1], b[4][1])
+        assert path["e_layout"] == int(lay) and path["h_layout"] == int(lay), path
+        out[lay] = (spec, td, vols, fields, grad)
+    a = out["0"]
+    for lay in ("1", "2"):
+        b = out[lay]
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), lay
+        for va, vb in zip(a[2], b[2]):
+            assert np.array_equal(va, vb), lay
+        for fa, fb in zip(a[3], b[3]):
+            assert np.array_equal(fa, fb), lay
+        assert a[4][0] == pytest.approx(b[4][0], rel=1e-13) and np.array_equal(a[4][1], b[4][1]), lay
